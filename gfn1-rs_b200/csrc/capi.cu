@@ -1,0 +1,851 @@
+// Host side of the engine: table loading, per-element device tables, batch
+// layout and the C ABI declared in include/gfn1_b200.h.
+//
+// Element preparation follows gfn1-rs BasisSet::build (src/basis.rs:121-233):
+// STO-nG expansion with normalised primitives (src/sto.rs:790-881), the GFN1
+// primitive-count rule (src/basis.rs:251-279), same-centre orthogonalisation of
+// a second shell of the same angular momentum (src/basis.rs:318-344), the CN
+// shift (src/basis.rs:281-293) and the legacy eV->Eh factor (src/basis.rs:18).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/gfn1_b200.h"
+#include "common.cuh"
+#include "model.cuh"
+
+namespace gfn1 {
+__global__ void setup_kernel(Batch B, Model M, int enable_dispersion, int max_nsh);
+__global__ void scc_kernel(Batch B, Model M, SccOptions opt, int max_nsh, int max_n);
+__global__ void grad_kernel(Batch B, Model M);
+long long scc_workspace_doubles(int maxn, int maxnsh, int cap, int maxnat);
+}  // namespace gfn1
+
+using namespace gfn1;
+
+namespace {
+
+const double kEvToHartreeModel = 1.0 / 27.21138505;  // src/basis.rs:18
+const double kAngstromToBohr = 1.8897261246257702;   // src/constants.rs:27
+const double kPiHost = 3.14159265358979323846;
+
+thread_local std::string t_error;
+
+struct Tables {
+  std::map<std::string, std::vector<double>> kv;
+  bool has(const std::string& k) const { return kv.count(k) != 0; }
+  const std::vector<double>* get(const std::string& k) const {
+    auto it = kv.find(k);
+    return it == kv.end() ? nullptr : &it->second;
+  }
+  double scalar(const std::string& k, double d) const {
+    auto p = get(k);
+    return p && !p->empty() ? (*p)[0] : d;
+  }
+};
+
+// C stdio on purpose: the host process may already hold a different libstdc++.
+bool load_tables(const char* path, Tables& t, std::string& err) {
+  FILE* fp = std::fopen(path, "rb");
+  if (!fp) {
+    err = std::string("cannot open tables file ") + path;
+    return false;
+  }
+  std::string text;
+  char buf[1 << 16];
+  size_t got;
+  while ((got = std::fread(buf, 1, sizeof buf, fp)) > 0) text.append(buf, got);
+  std::fclose(fp);
+  size_t pos = 0;
+  while (pos < text.size()) {
+    size_t eol = text.find('\n', pos);
+    if (eol == std::string::npos) eol = text.size();
+    std::string line = text.substr(pos, eol - pos);
+    pos = eol + 1;
+    if (line.empty() || line[0] == '#') continue;
+    const char* c = line.c_str();
+    while (*c == ' ') ++c;
+    const char* ks = c;
+    while (*c && *c != ' ') ++c;
+    std::string key(ks, c - ks);
+    char* end = nullptr;
+    long n = std::strtol(c, &end, 10);
+    if (end == c || n < 0) {
+      err = "bad table line for `" + key + "`";
+      return false;
+    }
+    c = end;
+    std::vector<double> v((size_t)n);
+    for (long i = 0; i < n; ++i) {
+      v[i] = std::strtod(c, &end);
+      if (end == c) {
+        err = "bad table value for `" + key + "`";
+        return false;
+      }
+      c = end;
+    }
+    t.kv[key] = std::move(v);
+  }
+  return true;
+}
+
+struct Prim {
+  double a, c;
+};
+
+// src/sto.rs:790-881
+bool sto_ng(const Tables& t, int ng, int n, int l, double zeta, std::vector<Prim>& out) {
+  bool special = (n == 6 && ng == 6 && l <= 1);
+  if (ng < 1 || ng > 6 || ((n > 5 || n <= l) && !special) || zeta <= 0) return false;
+  std::vector<double> alpha(ng), coeff(ng);
+  if (special) {
+    auto a = t.get(l == 0 ? "sto.alpha6s" : "sto.alpha6p");
+    auto c = t.get(l == 0 ? "sto.coeff6s" : "sto.coeff6p");
+    if (!a || !c) return false;
+    for (int i = 0; i < 6; ++i) {
+      alpha[i] = (*a)[i];
+      coeff[i] = (*c)[i];
+    }
+  } else {
+    int ityp1 = (l == 0) ? n : (l == 1 ? 4 + n : (l == 2 ? 7 + n : (l == 3 ? 9 + n : 10 + n)));
+    if (ityp1 < 1 || ityp1 > 15) return false;
+    auto a = t.get("sto.alpha." + std::to_string(ng));
+    auto c = t.get("sto.coeff." + std::to_string(ng));
+    if (!a || !c) return false;
+    for (int i = 0; i < ng; ++i) {
+      alpha[i] = (*a)[(ityp1 - 1) * ng + i];
+      coeff[i] = (*c)[(ityp1 - 1) * ng + i];
+    }
+  }
+  static const double dfact[8] = {1.0, 1.0, 3.0, 15.0, 105.0, 945.0, 10395.0, 135135.0};
+  out.resize(ng);
+  for (int i = 0; i < ng; ++i) {
+    const double al = alpha[i] * zeta * zeta;
+    out[i].a = al;
+    out[i].c = coeff[i] * std::pow(2.0 / kPiHost * al, 0.75) * std::pow(std::sqrt(4.0 * al), l) / std::sqrt(dfact[l]);
+  }
+  return true;
+}
+
+// src/basis.rs:318-344
+void orthogonalize(const std::vector<Prim>& ref, std::vector<Prim>& sh) {
+  double ov = 0.0;
+  for (auto& a : ref)
+    for (auto& b : sh) ov += a.c * b.c * std::pow(std::sqrt(kPiHost / (a.a + b.a)), 3);
+  for (auto& a : ref) sh.push_back({a.a, -ov * a.c});
+  double nrm = 0.0;
+  for (auto& a : sh)
+    for (auto& b : sh) nrm += a.c * b.c * std::pow(std::sqrt(kPiHost / (a.a + b.a)), 3);
+  const double sc = 1.0 / std::sqrt(nrm);
+  for (auto& p : sh) p.c *= sc;
+}
+
+int gfn1_kind(int z) {  // src/basis.rs:295-302
+  if (z == 1 || z == 2 || (z >= 6 && z <= 10) || (z >= 14 && z <= 18) || (z >= 32 && z <= 36) ||
+      (z >= 50 && z <= 54) || (z >= 82 && z <= 86))
+    return 1;
+  if (z >= 21 && z <= 24) return 2;
+  return 0;
+}
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  bool ensure(size_t count) {
+    if (count <= n && p) return true;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    size_t want = std::max<size_t>(count, 1);
+    if (cudaMalloc(&p, want * sizeof(T)) != cudaSuccess) return false;
+    n = want;
+    return true;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+}  // namespace
+
+struct gfn1_engine {
+  int device = 0;
+  int num_sms = 148;
+  std::string error;
+  ElemTable elem[kNZ];
+  bool device_ok[kNZ];
+  double refocc_total[kNZ];
+  Globals glob;
+  std::vector<double> pair_scaling, c6ref;
+  ElemTable* d_elem = nullptr;
+  double* d_pair = nullptr;
+  double* d_c6 = nullptr;
+  cudaStream_t stream = nullptr;
+  Model model() const {
+    Model m;
+    m.elem = d_elem;
+    m.pair_scaling = d_pair;
+    m.c6ref = d_c6;
+    m.g = glob;
+    return m;
+  }
+};
+
+struct gfn1_batch {
+  gfn1_engine* eng = nullptr;
+  int nmol = 0;
+  long long natoms = 0, nshells = 0, naos = 0, mat_total = 0, gam_total = 0, pair_total = 0;
+  int max_nat = 0, max_nsh = 0, max_n = 0, cap = 0, n_cta = 0;
+  long long ws_stride = 0;
+  gfn1_options opt;
+  std::vector<int> h_status;
+  std::vector<int> h_atom_off;
+  std::vector<int> h_shell_off;
+  bool has_init_q = false;
+  DevBuf<int> atom_off, shell_off, ao_off, order, z, status, iterations, queue;
+  DevBuf<long long> mat_off, gam_off, pair_off;
+  DevBuf<double> xyz, charge, init_q, S, H0, P, W, ws, gam, pairbuf, cn, shell_q, shell_pot, atom_q, se, terms,
+      grad, grad_classic, dipole, fermi;
+  Batch dev() const {
+    Batch B;
+    std::memset(&B, 0, sizeof B);
+    B.nmol = nmol;
+    B.max_nat = max_nat;
+    B.atom_off = atom_off.p;
+    B.shell_off = shell_off.p;
+    B.ao_off = ao_off.p;
+    B.mat_off = mat_off.p;
+    B.gam_off = gam_off.p;
+    B.pair_off = pair_off.p;
+    B.order = order.p;
+    B.z = z.p;
+    B.xyz = xyz.p;
+    B.charge = charge.p;
+    B.init_q = has_init_q ? init_q.p : nullptr;
+    B.S = S.p;
+    B.H0 = H0.p;
+    B.P = P.p;
+    B.W = W.p;
+    B.ws = ws.p;
+    B.ws_stride = ws_stride;
+    B.ws_maxn = max_n;
+    B.ws_maxnsh = max_nsh;
+    B.ws_cap = cap;
+    B.gam = gam.p;
+    B.pairbuf = pairbuf.p;
+    B.cn = cn.p;
+    B.shell_q = shell_q.p;
+    B.shell_pot = shell_pot.p;
+    B.atom_q = atom_q.p;
+    B.se = se.p;
+    B.terms = terms.p;
+    B.grad = grad.p;
+    B.grad_classic = grad_classic.p;
+    B.dipole = dipole.p;
+    B.fermi = fermi.p;
+    B.iterations = iterations.p;
+    B.status = status.p;
+    B.queue = queue.p;
+    return B;
+  }
+};
+
+namespace {
+
+int fail(const gfn1_engine* eng, int code, const std::string& msg) {
+  t_error = msg;
+  if (eng) const_cast<gfn1_engine*>(eng)->error = msg;
+  return code;
+}
+
+int cuda_fail(const gfn1_engine* eng, cudaError_t e, const char* what) {
+  return fail(eng, GFN1_E_DEVICE, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+std::string default_tables_path() {
+  // <package>/data/gfn1_tables.txt next to <package>/lib/libgfn1_b200.so is
+  // resolved by the Python layer; the C ABI accepts an explicit path or the
+  // GFN1_B200_TABLES environment variable.
+  const char* envp = std::getenv("GFN1_B200_TABLES");
+  if (envp && *envp) return envp;
+  return "gfn1_tables.txt";
+}
+
+bool build_elements(gfn1_engine* eng, const Tables& t, std::string& err) {
+  Globals& g = eng->glob;
+  g.ks = t.scalar("glob.ks", 1.85);
+  g.kp = t.scalar("glob.kp", 2.25);
+  g.kd = t.scalar("glob.kd", 2.00);
+  g.ksp = t.scalar("glob.ksp", 2.08);
+  g.kdiff = t.scalar("glob.kdiff", 2.85);
+  g.enscale = t.scalar("glob.enscale", -0.7);
+  g.kexp = t.scalar("glob.kexp", 1.5);
+  g.kexplight = t.scalar("glob.kexplight", g.kexp);
+  g.s6 = t.scalar("glob.s6", 1.0);
+  for (const char* k : {"glob.a1", "glob.a2", "glob.s8", "glob.s9"}) {
+    if (!t.has(k)) {
+      err = std::string("missing required $globpar entry `") + (k + 5) + "`";
+      return false;
+    }
+  }
+  g.a1 = t.scalar("glob.a1", 0);
+  g.a2 = t.scalar("glob.a2", 0);
+  g.s8 = t.scalar("glob.s8", 0);
+  if (std::fabs(t.scalar("glob.s9", 0.0)) > 1e-15) {
+    err = "D3 three-body term (s9 != 0) is outside the device path";
+    return false;
+  }
+  const double cns = t.scalar("glob.cns", 0.6), cnp = t.scalar("glob.cnp", -0.3);
+  auto refocc = t.get("refocc");
+  auto radius = t.get("atomic_radius_ang");
+  auto covrad = t.get("covrad_ang");
+  auto en = t.get("pauling_en");
+  auto nref = t.get("d3.nref");
+  auto r4r2 = t.get("d3.r4r2");
+  if (!refocc || !radius || !covrad || !en || !nref || !r4r2) {
+    err = "tables file lacks element data";
+    return false;
+  }
+  for (int z = 0; z < kNZ; ++z) {
+    std::memset(&eng->elem[z], 0, sizeof(ElemTable));
+    eng->device_ok[z] = false;
+    eng->refocc_total[z] = 0.0;
+  }
+  for (int z = 1; z <= kMaxZ; ++z) {
+    const std::string p = "elem." + std::to_string(z) + ".";
+    auto ao = t.get(p + "ao");
+    auto lev = t.get(p + "lev");
+    auto ex = t.get(p + "exp");
+    if (!ao || !lev || !ex) continue;
+    const int nsh = (int)ao->size() / 2;
+    bool ok = nsh <= kMaxShAtom;
+    for (int k = 0; k < nsh && ok; ++k)
+      if ((int)(*ao)[2 * k + 1] > 1) ok = false;  // device path: s and p shells
+    if (!ok) continue;
+    ElemTable& e = eng->elem[z];
+    e.nsh = nsh;
+    const double gam = t.scalar(p + "gam", 0.0);
+    const double lpar[2] = {t.scalar(p + "lpars", 0.0), t.scalar(p + "lparp", 0.0)};
+    const double poly[2] = {t.scalar(p + "polys", 0.0), t.scalar(p + "polyp", 0.0)};
+    bool seen[2] = {false, false};
+    std::vector<Prim> ref[2];
+    int nao = 0;
+    for (int k = 0; k < nsh; ++k) {
+      const int n = (int)(*ao)[2 * k], l = (int)(*ao)[2 * k + 1];
+      const bool valence = !seen[l];
+      const int np = (z <= 2) ? (l == 0 ? (n == 1 ? 4 : 3) : 3) : 6;
+      std::vector<Prim> prims;
+      if (!sto_ng(t, np, n, l, (*ex)[k], prims)) {
+        ok = false;
+        break;
+      }
+      if (seen[l]) orthogonalize(ref[l], prims);
+      else ref[l] = prims;
+      seen[l] = true;
+      if ((int)prims.size() > kMaxPrim) {
+        ok = false;
+        break;
+      }
+      e.l[k] = l;
+      e.nprim[k] = (int)prims.size();
+      e.valence[k] = valence ? 1 : 0;
+      e.ao_first[k] = nao;
+      nao += 2 * l + 1;
+      for (size_t i = 0; i < prims.size(); ++i) {
+        e.alpha[k][i] = prims[i].a;
+        e.coef[k][i] = prims[i].c;
+      }
+      e.hdiag[k] = (*lev)[k] * kEvToHartreeModel;
+      const int kind = gfn1_kind(z);
+      const double f = kind == 0 ? 0.0 : (l == 0 ? cns : cnp);
+      e.kcn[k] = -(*lev)[k] * kEvToHartreeModel * f * 0.01;
+      e.poly[k] = poly[l] * 0.01;
+      e.refocc[k] = valence ? (*refocc)[3 * z + l] : 0.0;
+      e.hard[k] = gam * (1.0 + 0.1 * lpar[l]);  // src/params.rs:152-161
+      eng->refocc_total[z] += e.refocc[k];
+    }
+    if (!ok) {
+      std::memset(&e, 0, sizeof(ElemTable));
+      eng->refocc_total[z] = 0.0;
+      continue;
+    }
+    e.nao = nao;
+    e.gam3 = 0.1 * t.scalar(p + "gam3", 0.0);
+    e.repa = t.scalar(p + "repa", 0.0);
+    e.repb = t.scalar(p + "repb", 0.0);
+    e.en = (*en)[z];
+    e.rad = (*radius)[z] * kAngstromToBohr;
+    e.rcov = (4.0 / 3.0) * (*covrad)[z] * kAngstromToBohr;
+    e.r4r2 = std::sqrt(0.5 * (*r4r2)[z - 1] * std::sqrt((double)z));
+    e.d3_nref = (int)(*nref)[z - 1];
+    auto cref = t.get("d3.cnref." + std::to_string(z));
+    if (!cref || e.d3_nref > kMaxRef || e.d3_nref < 1 || e.rad <= 0 || e.rcov <= 0) {
+      std::memset(&e, 0, sizeof(ElemTable));
+      eng->refocc_total[z] = 0.0;
+      continue;
+    }
+    for (int r = 0; r < e.d3_nref; ++r) e.d3_cnref[r] = (*cref)[r];
+    eng->device_ok[z] = true;
+  }
+  // pair scaling (src/params.rs:361-367, :694-710)
+  eng->pair_scaling.assign(kNZ * kNZ, 1.0);
+  for (int a = 1; a <= kMaxZ; ++a)
+    for (int b = 1; b <= kMaxZ; ++b) {
+      auto drow = [](int zz) {
+        if (zz >= 21 && zz < 30) return 1.1;
+        if (zz >= 39 && zz < 48) return 1.2;
+        if (zz >= 57 && zz < 80) return 1.2;
+        return -1.0;
+      };
+      double v = (drow(a) > 0 && drow(b) > 0) ? 0.5 * (drow(a) + drow(b)) : 1.0;
+      const std::string key = "pair." + std::to_string(std::min(a, b)) + "." + std::to_string(std::max(a, b));
+      if (t.has(key)) v = t.scalar(key, v);
+      eng->pair_scaling[a * kNZ + b] = v;
+    }
+  // D3 reference C6, stored for both element orders (src/dispersion.rs:3145-3164)
+  eng->c6ref.assign((size_t)kNZ * kNZ * kMaxRef * kMaxRef, 0.0);
+  for (int a = 1; a <= kMaxZ; ++a)
+    for (int b = 1; b <= kMaxZ; ++b) {
+      if (!eng->device_ok[a] || !eng->device_ok[b]) continue;
+      const int hi = std::max(a, b), lo = std::min(a, b);
+      auto blk = t.get("d3.c6." + std::to_string(hi) + "." + std::to_string(lo));
+      if (!blk) continue;
+      const int nhi = eng->elem[hi].d3_nref, nlo = eng->elem[lo].d3_nref;
+      for (int ra = 0; ra < eng->elem[a].d3_nref; ++ra)
+        for (int rb = 0; rb < eng->elem[b].d3_nref; ++rb) {
+          // lookup rule of D3Reference::c6: the larger element's reference first
+          int ia, ib;
+          if (a > b) {
+            ia = ra;
+            ib = rb;
+          } else {
+            ia = rb;
+            ib = ra;
+          }
+          (void)nhi;
+          eng->c6ref[((size_t)(a * kNZ + b)) * kMaxRef * kMaxRef + ra * kMaxRef + rb] = (*blk)[ia * nlo + ib];
+        }
+    }
+  return true;
+}
+
+void fill_default(gfn1_options* o) {
+  o->max_scc = 250;
+  o->energy_tolerance = 1e-6;
+  o->charge_tolerance = 2e-5;
+  o->mixing = 0.4;
+  o->scc_broyden = 1;
+  o->scc_broyden_size = 250;
+  o->electronic_temperature = 300.0;
+  o->enable_dispersion = 1;
+  o->compute_gradient = 1;
+}
+
+template <class T>
+int upload(gfn1_engine* eng, DevBuf<T>& buf, const T* host, size_t n, cudaStream_t s) {
+  if (!buf.ensure(n)) return fail(eng, GFN1_E_DEVICE, "device allocation failed");
+  if (n == 0) return GFN1_OK;
+  cudaError_t e = cudaMemcpyAsync(buf.p, host, n * sizeof(T), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return cuda_fail(eng, e, "host to device copy");
+  return GFN1_OK;
+}
+
+}  // namespace
+
+// ============================================================== C ABI
+extern "C" {
+
+void gfn1_default_options(gfn1_options* opt) {
+  if (opt) fill_default(opt);
+}
+
+const char* gfn1_last_error(const gfn1_engine* eng) {
+  (void)eng;
+  return t_error.c_str();
+}
+
+int gfn1_engine_create(const char* param_spec, int device, gfn1_engine** out) {
+  if (!out) return fail(nullptr, GFN1_E_INVALID_INPUT, "null output handle");
+  *out = nullptr;
+  std::string path;
+  if (!param_spec || !*param_spec || std::strcmp(param_spec, "builtin") == 0 || std::strcmp(param_spec, "builtin:gfn1") == 0)
+    path = default_tables_path();
+  else
+    path = param_spec;
+  Tables t;
+  std::string err;
+  if (!load_tables(path.c_str(), t, err)) return fail(nullptr, GFN1_E_IO, err);
+  gfn1_engine* eng = new gfn1_engine();
+  eng->device = device;
+  if (!build_elements(eng, t, err)) {
+    delete eng;
+    return fail(nullptr, GFN1_E_MISSING_GLOBAL, err);
+  }
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) {
+    delete eng;
+    return cuda_fail(nullptr, e, "cudaSetDevice");
+  }
+  cudaDeviceGetAttribute(&eng->num_sms, cudaDevAttrMultiProcessorCount, device);
+  if ((e = cudaMalloc(&eng->d_elem, sizeof(ElemTable) * kNZ)) != cudaSuccess ||
+      (e = cudaMalloc(&eng->d_pair, sizeof(double) * eng->pair_scaling.size())) != cudaSuccess ||
+      (e = cudaMalloc(&eng->d_c6, sizeof(double) * eng->c6ref.size())) != cudaSuccess ||
+      (e = cudaStreamCreateWithFlags(&eng->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+    gfn1_engine_destroy(eng);
+    return cuda_fail(nullptr, e, "engine allocation");
+  }
+  cudaMemcpy(eng->d_elem, eng->elem, sizeof(ElemTable) * kNZ, cudaMemcpyHostToDevice);
+  cudaMemcpy(eng->d_pair, eng->pair_scaling.data(), sizeof(double) * eng->pair_scaling.size(), cudaMemcpyHostToDevice);
+  e = cudaMemcpy(eng->d_c6, eng->c6ref.data(), sizeof(double) * eng->c6ref.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    gfn1_engine_destroy(eng);
+    return cuda_fail(nullptr, e, "engine table upload");
+  }
+  *out = eng;
+  return GFN1_OK;
+}
+
+void gfn1_engine_destroy(gfn1_engine* eng) {
+  if (!eng) return;
+  if (eng->d_elem) cudaFree(eng->d_elem);
+  if (eng->d_pair) cudaFree(eng->d_pair);
+  if (eng->d_c6) cudaFree(eng->d_c6);
+  if (eng->stream) cudaStreamDestroy(eng->stream);
+  delete eng;
+}
+
+int gfn1_basis_size(const gfn1_engine* eng, int nat, const uint8_t* z, int32_t* nao, int32_t* nshells) {
+  if (!eng || nat < 0 || (nat > 0 && !z)) return fail(eng, GFN1_E_INVALID_INPUT, "invalid arguments");
+  int n = 0, s = 0;
+  for (int a = 0; a < nat; ++a) {
+    const int zz = z[a];
+    if (zz < 1 || zz > kMaxZ) return fail(eng, GFN1_E_MISSING_ELEMENT, "missing GFN1 parameter block for Z=" + std::to_string(zz));
+    if (!eng->device_ok[zz])
+      return fail(eng, GFN1_E_UNSUPPORTED, "element Z=" + std::to_string(zz) + " has d/f shells; outside the device path");
+    n += eng->elem[zz].nao;
+    s += eng->elem[zz].nsh;
+  }
+  if (nao) *nao = n;
+  if (nshells) *nshells = s;
+  return GFN1_OK;
+}
+
+int gfn1_batch_create(gfn1_engine* eng, int nmol, const int32_t* atom_offsets, const uint8_t* z, const double* charge,
+                      const gfn1_options* opt, gfn1_batch** out) {
+  if (!eng || !out || nmol < 1 || !atom_offsets || !z) return fail(eng, GFN1_E_INVALID_INPUT, "invalid batch arguments");
+  *out = nullptr;
+  gfn1_options o;
+  if (opt) o = *opt;
+  else fill_default(&o);
+  if (o.max_scc < 1) return fail(eng, GFN1_E_INVALID_INPUT, "max_scc must be at least 1");
+  cudaSetDevice(eng->device);
+  gfn1_batch* b = new gfn1_batch();
+  b->eng = eng;
+  b->nmol = nmol;
+  b->opt = o;
+  const long long natoms = atom_offsets[nmol];
+  b->natoms = natoms;
+  std::vector<int> shell_off(nmol + 1, 0), ao_off(nmol + 1, 0);
+  std::vector<long long> mat_off(nmol + 1, 0), gam_off(nmol + 1, 0), pair_off(nmol + 1, 0);
+  std::vector<int> status(nmol, GFN1_OK), zi(std::max<long long>(natoms, 1));
+  std::vector<double> ch(nmol, 0.0);
+  std::string first_err;
+  int worst = GFN1_OK;
+  for (int m = 0; m < nmol; ++m) {
+    const int a0 = atom_offsets[m], a1 = atom_offsets[m + 1];
+    int n = 0, s = 0, st = GFN1_OK;
+    double nref = 0.0;
+    if (a1 <= a0) {
+      st = GFN1_E_INVALID_INPUT;
+      if (first_err.empty()) first_err = "molecule " + std::to_string(m) + ": cannot run GFN1 SCC for an empty basis";
+    }
+    for (int a = a0; a < a1; ++a) {
+      const int zz = z[a];
+      zi[a] = zz;
+      if (zz < 1 || zz > kMaxZ) {
+        st = GFN1_E_MISSING_ELEMENT;
+        if (first_err.empty()) first_err = "missing GFN1 parameter block for Z=" + std::to_string(zz);
+        zi[a] = 1;
+        continue;
+      }
+      if (!eng->device_ok[zz]) {
+        st = GFN1_E_UNSUPPORTED;
+        if (first_err.empty()) first_err = "element Z=" + std::to_string(zz) + " has d/f shells; outside the device path";
+        zi[a] = 1;
+        continue;
+      }
+      n += eng->elem[zz].nao;
+      s += eng->elem[zz].nsh;
+      nref += eng->refocc_total[zz];
+    }
+    ch[m] = charge ? charge[m] : 0.0;
+    const double nelec = nref - ch[m];  // src/electronic.rs:491-510
+    if (st == GFN1_OK && (!std::isfinite(nelec) || nelec < -1e-8 || nelec > 2.0 * n + 1e-8)) {
+      st = GFN1_E_INVALID_INPUT;
+      if (first_err.empty()) first_err = "molecule " + std::to_string(m) + ": invalid electron count";
+    }
+    status[m] = st;
+    worst = std::max(worst, st);
+    shell_off[m + 1] = shell_off[m] + s;
+    ao_off[m + 1] = ao_off[m] + n;
+    mat_off[m + 1] = mat_off[m] + (((long long)n * n + 31) / 32) * 32;
+    gam_off[m + 1] = gam_off[m] + (long long)s * s;
+    pair_off[m + 1] = pair_off[m] + (long long)(a1 - a0) * (a1 - a0 - 1) / 2;
+    b->max_nat = std::max(b->max_nat, a1 - a0);
+    b->max_nsh = std::max(b->max_nsh, s);
+    b->max_n = std::max(b->max_n, n);
+  }
+  b->nshells = shell_off[nmol];
+  b->naos = ao_off[nmol];
+  b->mat_total = mat_off[nmol];
+  b->gam_total = gam_off[nmol];
+  b->pair_total = pair_off[nmol];
+  b->h_status = status;
+  b->h_atom_off.assign(atom_offsets, atom_offsets + nmol + 1);
+  b->h_shell_off = shell_off;
+  b->cap = std::max(1, std::min(std::max(o.scc_broyden_size, 2), o.max_scc));
+  b->ws_stride = scc_workspace_doubles(b->max_n, b->max_nsh, b->cap, b->max_nat);
+  // most expensive molecules first (cost ~ N^3)
+  std::vector<int> order(nmol);
+  for (int m = 0; m < nmol; ++m) order[m] = m;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    return (ao_off[x + 1] - ao_off[x]) > (ao_off[y + 1] - ao_off[y]);
+  });
+  const int per_sm = 2;
+  b->n_cta = std::max(1, std::min(nmol, per_sm * eng->num_sms));
+  cudaStream_t st = eng->stream;
+  int rc;
+  if ((rc = upload(eng, b->atom_off, atom_offsets, nmol + 1, st)) ||
+      (rc = upload(eng, b->shell_off, shell_off.data(), nmol + 1, st)) ||
+      (rc = upload(eng, b->ao_off, ao_off.data(), nmol + 1, st)) ||
+      (rc = upload(eng, b->mat_off, mat_off.data(), nmol + 1, st)) ||
+      (rc = upload(eng, b->gam_off, gam_off.data(), nmol + 1, st)) ||
+      (rc = upload(eng, b->pair_off, pair_off.data(), nmol + 1, st)) ||
+      (rc = upload(eng, b->order, order.data(), nmol, st)) ||
+      (rc = upload(eng, b->z, zi.data(), (size_t)natoms, st)) || (rc = upload(eng, b->charge, ch.data(), nmol, st))) {
+    gfn1_batch_destroy(b);
+    return rc;
+  }
+  bool ok = b->xyz.ensure(3 * natoms) && b->status.ensure(nmol) && b->iterations.ensure(nmol) && b->queue.ensure(4) &&
+            b->S.ensure(b->mat_total) && b->H0.ensure(b->mat_total) && b->P.ensure(b->mat_total) &&
+            b->W.ensure(b->mat_total) && b->ws.ensure((size_t)b->ws_stride * b->n_cta) && b->gam.ensure(b->gam_total) &&
+            b->pairbuf.ensure(8 * std::max<long long>(b->pair_total, 1)) && b->cn.ensure(natoms) &&
+            b->shell_q.ensure(b->nshells) && b->shell_pot.ensure(b->nshells) && b->atom_q.ensure(natoms) &&
+            b->se.ensure(b->nshells) && b->terms.ensure((size_t)kTerms * nmol) && b->grad.ensure(3 * natoms) &&
+            b->grad_classic.ensure(3 * natoms) && b->dipole.ensure(3 * nmol) && b->fermi.ensure(nmol);
+  if (!ok) {
+    gfn1_batch_destroy(b);
+    return fail(eng, GFN1_E_DEVICE, "device allocation failed for the batch workspace");
+  }
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    gfn1_batch_destroy(b);
+    return cuda_fail(eng, e, "batch upload");
+  }
+  *out = b;
+  if (worst != GFN1_OK) fail(eng, worst, first_err);
+  return GFN1_OK;
+}
+
+void gfn1_batch_destroy(gfn1_batch* b) {
+  if (!b) return;
+  b->atom_off.release();
+  b->shell_off.release();
+  b->ao_off.release();
+  b->order.release();
+  b->z.release();
+  b->status.release();
+  b->iterations.release();
+  b->queue.release();
+  b->mat_off.release();
+  b->gam_off.release();
+  b->pair_off.release();
+  for (DevBuf<double>* d : {&b->xyz, &b->charge, &b->init_q, &b->S, &b->H0, &b->P, &b->W, &b->ws, &b->gam,
+                            &b->pairbuf, &b->cn, &b->shell_q, &b->shell_pot, &b->atom_q, &b->se, &b->terms, &b->grad,
+                            &b->grad_classic, &b->dipole, &b->fermi})
+    d->release();
+  delete b;
+}
+
+int gfn1_batch_set_positions(gfn1_batch* b, const double* xyz, int on_device) {
+  if (!b || !xyz) return fail(b ? b->eng : nullptr, GFN1_E_INVALID_INPUT, "invalid arguments");
+  cudaError_t e = cudaMemcpyAsync(b->xyz.p, xyz, sizeof(double) * 3 * b->natoms,
+                                  on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, b->eng->stream);
+  if (e != cudaSuccess) return cuda_fail(b->eng, e, "set positions");
+  return GFN1_OK;
+}
+
+int gfn1_batch_set_initial_charges(gfn1_batch* b, const double* q, int on_device) {
+  if (!b) return fail(nullptr, GFN1_E_INVALID_INPUT, "invalid arguments");
+  if (!q) {
+    b->has_init_q = false;
+    return GFN1_OK;
+  }
+  if (!b->init_q.ensure(b->nshells)) return fail(b->eng, GFN1_E_DEVICE, "device allocation failed");
+  cudaError_t e = cudaMemcpyAsync(b->init_q.p, q, sizeof(double) * b->nshells,
+                                  on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, b->eng->stream);
+  if (e != cudaSuccess) return cuda_fail(b->eng, e, "set initial charges");
+  b->has_init_q = true;
+  return GFN1_OK;
+}
+
+int gfn1_batch_launch(gfn1_batch* b, void* stream) {
+  if (!b) return fail(nullptr, GFN1_E_INVALID_INPUT, "null batch");
+  gfn1_engine* eng = b->eng;
+  cudaStream_t st = stream ? (cudaStream_t)stream : eng->stream;
+  if (stream) {  // order the engine-stream uploads before work on the caller's stream
+    cudaEvent_t ev;
+    cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    cudaEventRecord(ev, eng->stream);
+    cudaStreamWaitEvent(st, ev, 0);
+    cudaEventDestroy(ev);
+  }
+  const Batch B = b->dev();
+  const Model M = eng->model();
+  cudaError_t e;
+  if ((e = cudaMemcpyAsync(b->status.p, b->h_status.data(), sizeof(int) * b->nmol, cudaMemcpyHostToDevice, st)) !=
+          cudaSuccess ||
+      (e = cudaMemsetAsync(b->queue.p, 0, sizeof(int) * 4, st)) != cudaSuccess)
+    return cuda_fail(eng, e, "batch reset");
+  const int nt = 256;
+  const size_t smem_setup = sizeof(double) * (16 * (size_t)b->max_nat + 32) +
+                            sizeof(int) * (3 * (size_t)b->max_nat + 2 + 2 * (size_t)b->max_nsh);
+  const size_t smem_scc = sizeof(int) * (3 * (size_t)b->max_nsh + b->max_n + b->max_nat + 1);
+  const size_t smem_grad = sizeof(double) * 7 * (size_t)b->max_nat + sizeof(int) * (3 * (size_t)b->max_nat + 2);
+  if (smem_setup > 48 * 1024) cudaFuncSetAttribute(setup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_setup);
+  if (smem_scc > 48 * 1024) cudaFuncSetAttribute(scc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_scc);
+  if (smem_grad > 48 * 1024) cudaFuncSetAttribute(grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_grad);
+  setup_kernel<<<b->nmol, nt, smem_setup, st>>>(B, M, b->opt.enable_dispersion, b->max_nsh);
+  SccOptions so;
+  so.max_scc = b->opt.max_scc;
+  so.broyden = b->opt.scc_broyden;
+  so.broyden_size = b->opt.scc_broyden_size;
+  so.enable_dispersion = b->opt.enable_dispersion;
+  so.energy_tol = b->opt.energy_tolerance;
+  so.charge_tol = b->opt.charge_tolerance;
+  so.mixing = b->opt.mixing;
+  so.etemp = b->opt.electronic_temperature;
+  scc_kernel<<<b->n_cta, nt, smem_scc, st>>>(B, M, so, b->max_nsh, b->max_n);
+  if (b->opt.compute_gradient) grad_kernel<<<b->nmol, nt, smem_grad, st>>>(B, M);
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(eng, e, "kernel launch");
+  if (stream) {  // later engine-stream copies wait for the caller's stream
+    cudaEvent_t ev;
+    cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    cudaEventRecord(ev, st);
+    cudaStreamWaitEvent(eng->stream, ev, 0);
+    cudaEventDestroy(ev);
+  }
+  return GFN1_OK;
+}
+
+int gfn1_batch_info(const gfn1_batch* b, int64_t* natoms, int64_t* nshells, int64_t* naos, int32_t* launches) {
+  if (!b) return fail(nullptr, GFN1_E_INVALID_INPUT, "null batch");
+  if (natoms) *natoms = b->natoms;
+  if (nshells) *nshells = b->nshells;
+  if (naos) *naos = b->naos;
+  if (launches) *launches = b->opt.compute_gradient ? 3 : 2;
+  return GFN1_OK;
+}
+
+int gfn1_batch_outputs_device(gfn1_batch* b, gfn1_outputs* out) {
+  if (!b || !out) return fail(nullptr, GFN1_E_INVALID_INPUT, "invalid arguments");
+  out->energy = nullptr;  // total_free is terms[m*15 + 0]
+  out->terms = b->terms.p;
+  out->gradient = b->grad.p;
+  out->shell_charges = b->shell_q.p;
+  out->atomic_charges = b->atom_q.p;
+  out->dipole = b->dipole.p;
+  out->fermi_level = b->fermi.p;
+  out->iterations = b->iterations.p;
+  out->status = b->status.p;
+  return GFN1_OK;
+}
+
+int gfn1_batch_download(gfn1_batch* b, const gfn1_outputs* out) {
+  if (!b) return fail(nullptr, GFN1_E_INVALID_INPUT, "null batch");
+  gfn1_engine* eng = b->eng;
+  cudaStream_t st = eng->stream;
+  std::vector<double> terms((size_t)kTerms * b->nmol);
+  std::vector<int> status(b->nmol);
+  cudaError_t e;
+  if ((e = cudaMemcpyAsync(terms.data(), b->terms.p, sizeof(double) * terms.size(), cudaMemcpyDeviceToHost, st)) !=
+          cudaSuccess ||
+      (e = cudaMemcpyAsync(status.data(), b->status.p, sizeof(int) * b->nmol, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+    return cuda_fail(eng, e, "device to host copy");
+  if (out) {
+    auto cp = [&](void* dst, const void* src, size_t bytes) {
+      if (dst && bytes && e == cudaSuccess) e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st);
+    };
+    if (b->opt.compute_gradient) cp(out->gradient, b->grad.p, sizeof(double) * 3 * b->natoms);
+    cp(out->shell_charges, b->shell_q.p, sizeof(double) * b->nshells);
+    cp(out->atomic_charges, b->atom_q.p, sizeof(double) * b->natoms);
+    cp(out->dipole, b->dipole.p, sizeof(double) * 3 * b->nmol);
+    cp(out->fermi_level, b->fermi.p, sizeof(double) * b->nmol);
+    cp(out->iterations, b->iterations.p, sizeof(int) * b->nmol);
+    if (e != cudaSuccess) return cuda_fail(eng, e, "device to host copy");
+  }
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(eng, e, "batch execution");
+  int worst = GFN1_OK, first = -1;
+  for (int m = 0; m < b->nmol; ++m) {
+    if (status[m] > worst) worst = status[m];
+    if (status[m] != GFN1_OK && first < 0) first = m;
+  }
+  if (out) {
+    if (out->energy)
+      for (int m = 0; m < b->nmol; ++m) out->energy[m] = terms[(size_t)kTerms * m];
+    if (out->terms) std::memcpy(out->terms, terms.data(), sizeof(double) * terms.size());
+    if (out->status) std::memcpy(out->status, status.data(), sizeof(int) * b->nmol);
+  }
+  if (worst != GFN1_OK) {
+    std::string msg = "molecule " + std::to_string(first) + ": ";
+    switch (status[first]) {
+      case GFN1_E_SCC_NOT_CONVERGED: msg += "GFN1 SCC did not converge"; break;
+      case GFN1_E_INVALID_INPUT: msg += "invalid input (empty molecule, electron count or non-positive-definite overlap)"; break;
+      case GFN1_E_UNSUPPORTED: msg += "element outside the device path"; break;
+      case GFN1_E_MISSING_ELEMENT: msg += "missing GFN1 parameter block"; break;
+      default: msg += "error " + std::to_string(status[first]);
+    }
+    return fail(eng, worst, msg);
+  }
+  return GFN1_OK;
+}
+
+int gfn1_batch_energy_gradient(gfn1_engine* eng, int nmol, const int32_t* atom_offsets, const uint8_t* z,
+                               const double* xyz_bohr, const double* charge, const double* init_shell_q,
+                               const gfn1_options* opt, const gfn1_outputs* out) {
+  if (!xyz_bohr) return fail(eng, GFN1_E_INVALID_INPUT, "null coordinates");
+  gfn1_batch* b = nullptr;
+  int rc = gfn1_batch_create(eng, nmol, atom_offsets, z, charge, opt, &b);
+  if (rc != GFN1_OK) return rc;
+  for (long long i = 0; i < 3 * b->natoms; ++i)
+    if (!std::isfinite(xyz_bohr[i])) {
+      gfn1_batch_destroy(b);
+      return fail(eng, GFN1_E_NAN, "non-finite coordinate");
+    }
+  if ((rc = gfn1_batch_set_positions(b, xyz_bohr, 0)) != GFN1_OK ||
+      (rc = gfn1_batch_set_initial_charges(b, init_shell_q, 0)) != GFN1_OK || (rc = gfn1_batch_launch(b, nullptr)) != GFN1_OK) {
+    gfn1_batch_destroy(b);
+    return rc;
+  }
+  rc = gfn1_batch_download(b, out);
+  gfn1_batch_destroy(b);
+  return rc;
+}
+
+int gfn1_run(gfn1_engine* eng, int nat, const uint8_t* z, const double* xyz_bohr, double charge,
+             const double* init_shell_q, const gfn1_options* opt, const gfn1_outputs* out) {
+  int32_t off[2] = {0, nat};
+  return gfn1_batch_energy_gradient(eng, 1, off, z, xyz_bohr, &charge, init_shell_q, opt, out);
+}
+
+}  // extern "C"

@@ -1,0 +1,112 @@
+// Contracted STO-nG overlap blocks and their centre derivatives for s and p
+// shells, evaluated primitive pair by primitive pair in registers.
+//
+// Follows the integrals of gfn1-rs src/integrals.rs: the contracted overlap
+// `contracted_pair` (:290-360, index 0 of the ten moments) and its bra/ket
+// derivatives `contracted_pair_with_derivatives` (:481-537, :782-868), including
+// the primitive-pair screening bound `primitive_pair_bound` (:30-45) with its
+// 1e-13 threshold (:17).  The 1D Gaussian moments are generated by the
+// Obara-Saika recurrence E(i+1,j) = PA E(i,j) + (i E(i-1,j) + j E(i,j-1)) / 2p,
+// which equals the reference's binomial expansion (`moment_1d_no_kab`, :895-920).
+#pragma once
+
+#include "common.cuh"
+
+namespace gfn1 {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kPrimScreen = 1.0e-13;
+
+// Cartesian component of AO k of a shell with angular momentum l (s: (0,0,0);
+// p: x, y, z in that order, src/basis.rs:390-405).
+__device__ __forceinline__ void ao_powers(int l, int k, int& px, int& py, int& pz) {
+  px = (l == 1 && k == 0);
+  py = (l == 1 && k == 1);
+  pz = (l == 1 && k == 2);
+}
+
+// 1D moments E[i][j], i,j <= 2 (normalised so E[0][0] = 1) along one axis.
+__device__ __forceinline__ void moments1d(double pa, double pb, double inv2p, double E[3][3]) {
+  E[0][0] = 1.0;
+  E[1][0] = pa;
+  E[0][1] = pb;
+  E[1][1] = pa * pb + inv2p;
+  E[2][0] = pa * pa + inv2p;
+  E[0][2] = pb * pb + inv2p;
+  E[2][1] = pa * E[1][1] + inv2p * (E[0][1] + E[1][0]);
+  E[1][2] = pb * E[1][1] + inv2p * (E[1][0] + E[0][1]);
+  E[2][2] = pa * E[1][2] + inv2p * (E[0][2] + 2.0 * E[1][1]);
+}
+
+__device__ __forceinline__ double ipow(double x, int n) {
+  double r = 1.0;
+  for (int i = 0; i < n; ++i) r *= x;
+  return r;
+}
+
+// Overlap block S[ka][kb] between shell (la, prims a) at A and shell (lb, prims b)
+// at B; nao = 2l+1 for l <= 1.  `order_extra` is the screening order offset
+// (+2 for the integral build, +3 for the gradient, src/integrals.rs:313-316, :498-501).
+// When `want_deriv`, dA[ka][kb][3] receives dS/dA (bra centre) and dB the ket
+// centre derivative.
+template <bool WantDeriv>
+__device__ void overlap_block(int la, int na, const double* alpha_a, const double* coef_a, const double* A, int lb,
+                              int nb, const double* alpha_b, const double* coef_b, const double* B, int order_extra,
+                              double S[3][3], double dA[3][3][3], double dB[3][3][3]) {
+  const int nao_a = 2 * la + 1, nao_b = 2 * lb + 1;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      S[i][j] = 0.0;
+      if (WantDeriv)
+        for (int k = 0; k < 3; ++k) dA[i][j][k] = dB[i][j][k] = 0.0;
+    }
+  const double d[3] = {A[0] - B[0], A[1] - B[1], A[2] - B[2]};
+  const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+  const double r = sqrt(r2);
+  const int order = la + lb + order_extra;
+  for (int ia = 0; ia < na; ++ia) {
+    const double al = alpha_a[ia];
+    for (int ib = 0; ib < nb; ++ib) {
+      const double be = alpha_b[ib];
+      const double p = al + be;
+      const double ip = 1.0 / p;
+      const double kab = exp(-al * be * ip * r2);
+      const double gpre = (kPi * ip) * sqrt(kPi * ip);
+      const double pref = coef_a[ia] * coef_b[ib];
+      // src/integrals.rs:30-45 (component scale is 1 for s and p AOs)
+      const double bound = fabs(pref) * kab * gpre * ipow(1.0 + r + sqrt(ip), order);
+      if (bound < kPrimScreen) continue;
+      const double c = pref * kab * gpre;
+      const double inv2p = 0.5 * ip;
+      double E[3][3][3];
+#pragma unroll
+      for (int x = 0; x < 3; ++x) {
+        const double P = (al * A[x] + be * B[x]) * ip;
+        moments1d(P - A[x], P - B[x], inv2p, E[x]);
+      }
+      for (int ka = 0; ka < nao_a; ++ka) {
+        int a[3];
+        ao_powers(la, ka, a[0], a[1], a[2]);
+        for (int kb = 0; kb < nao_b; ++kb) {
+          int b[3];
+          ao_powers(lb, kb, b[0], b[1], b[2]);
+          const double ex = E[0][a[0]][b[0]], ey = E[1][a[1]][b[1]], ez = E[2][a[2]][b[2]];
+          S[ka][kb] += c * ex * ey * ez;
+          if (WantDeriv) {
+            const double e1[3] = {ex, ey, ez};
+#pragma unroll
+            for (int x = 0; x < 3; ++x) {
+              const double o = e1[(x + 1) % 3] * e1[(x + 2) % 3];
+              const double da = 2.0 * al * E[x][a[x] + 1][b[x]] - (a[x] ? E[x][a[x] - 1][b[x]] : 0.0);
+              const double db = 2.0 * be * E[x][a[x]][b[x] + 1] - (b[x] ? E[x][a[x]][b[x] - 1] : 0.0);
+              dA[ka][kb][x] += c * da * o;
+              dB[ka][kb][x] += c * db * o;
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
+}  // namespace gfn1

@@ -1,0 +1,305 @@
+// Per-molecule setup kernel: one CTA per molecule builds everything that depends
+// on the geometry only.
+//
+//  * coordination numbers with the exponential count, k = 16, cutoff 30 bohr for
+//    H0 and 25 bohr for D3 (src/coordination.rs:51-106, src/dispersion.rs:1245-1251);
+//  * self energies se = h - kcn*CN (src/hamiltonian.rs:98-104);
+//  * the overlap S and H0 = S * 1/2 (se_i + se_j) * hscale * Pi(R) for every shell
+//    pair inside the 30 bohr integral cutoff (src/integrals.rs:133-243,
+//    src/hamiltonian.rs:91-134).  Each unordered shell pair is evaluated once and
+//    mirrored, where the reference evaluates both directed atom pairs;
+//  * the shell-resolved Klopman-Ohno matrix (src/coulomb.rs:82-107);
+//  * repulsion energy and gradient (src/repulsion.rs:39-59, :139-159);
+//  * D3(BJ) two-body energy and gradient with its CN chain
+//    (src/dispersion.rs:1232-1360, :1629-1692, :1753-1787).
+//
+// Per-atom sums run one thread per atom over all partners in a fixed order, so
+// the results are bitwise reproducible (no floating-point atomics).
+#include "common.cuh"
+#include "model.cuh"
+#include "overlap.cuh"
+
+namespace gfn1 {
+
+__device__ __forceinline__ void tri_inverse(long long w, int& i, int& j) {
+  long long ii = (long long)((sqrt(8.0 * (double)w + 1.0) - 1.0) * 0.5);
+  while (ii * (ii + 1) / 2 > w) --ii;
+  while ((ii + 1) * (ii + 2) / 2 <= w) ++ii;
+  i = (int)ii;
+  j = (int)(w - ii * (ii + 1) / 2);
+}
+
+__global__ void __launch_bounds__(256) setup_kernel(Batch B, Model M, int enable_dispersion, int max_nsh) {
+  extern __shared__ double smem[];
+  const int m = blockIdx.x;
+  if (B.status[m] != kOk) return;  // rejected by the host-side validation
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int a0 = B.atom_off[m], nat = B.atom_off[m + 1] - a0;
+  const int sh0 = B.shell_off[m], nsh = B.shell_off[m + 1] - sh0;
+  const int N = B.ao_off[m + 1] - B.ao_off[m];
+  const int maxn = B.max_nat;
+  double* xyz = smem;                 // 3*maxn
+  double* cn = xyz + 3 * maxn;        // maxn
+  double* cnd = cn + maxn;            // maxn
+  double* dedcn = cnd + maxn;         // maxn
+  double* gw = dedcn + maxn;          // kMaxRef*maxn
+  double* dgw = gw + kMaxRef * maxn;  // kMaxRef*maxn
+  double* red = dgw + kMaxRef * maxn; // 32
+  int* zs = (int*)(red + 32);         // maxn
+  int* atom_sh = zs + maxn;           // maxn+1
+  int* atom_ao = atom_sh + maxn + 1;  // maxn+1
+  int* sh_atom = atom_ao + maxn + 1;  // max_nsh
+  int* sh_k = sh_atom + max_nsh;      // max_nsh
+
+  for (int i = tid; i < nat; i += nt) {
+    zs[i] = B.z[a0 + i];
+    xyz[3 * i] = B.xyz[3 * (a0 + i)];
+    xyz[3 * i + 1] = B.xyz[3 * (a0 + i) + 1];
+    xyz[3 * i + 2] = B.xyz[3 * (a0 + i) + 2];
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int s = 0, o = 0;
+    for (int a = 0; a < nat; ++a) {
+      const ElemTable& e = M.elem[zs[a]];
+      atom_sh[a] = s;
+      atom_ao[a] = o;
+      for (int k = 0; k < e.nsh; ++k) {
+        sh_atom[s + k] = a;
+        sh_k[s + k] = k;
+      }
+      s += e.nsh;
+      o += e.nao;
+    }
+    atom_sh[nat] = s;
+    atom_ao[nat] = o;
+  }
+  // coordination numbers (both cutoffs), one thread per atom
+  for (int i = tid; i < nat; i += nt) {
+    const double ri = M.elem[zs[i]].rcov;
+    double c30 = 0.0, c25 = 0.0;
+    for (int j = 0; j < nat; ++j) {
+      if (j == i) continue;
+      const double dx = xyz[3 * j] - xyz[3 * i], dy = xyz[3 * j + 1] - xyz[3 * i + 1], dz = xyz[3 * j + 2] - xyz[3 * i + 2];
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      if (r2 <= 1e-24 || r2 > 900.0) continue;
+      const double rc = ri + M.elem[zs[j]].rcov;
+      double v, dv;
+      exp_count(sqrt(r2), rc, v, dv);
+      c30 += v;
+      if (r2 <= 625.0) c25 += v;
+    }
+    cn[i] = c30;
+    cnd[i] = c25;
+    B.cn[a0 + i] = c30;
+  }
+  __syncthreads();
+  for (int s = tid; s < nsh; s += nt) {
+    const int a = sh_atom[s], k = sh_k[s];
+    const ElemTable& e = M.elem[zs[a]];
+    B.se[sh0 + s] = e.hdiag[k] - e.kcn[k] * cn[a];
+  }
+  __syncthreads();
+
+  // ---- S and H0, one work item per unordered shell pair
+  double* S = B.S + B.mat_off[m];
+  double* H0 = B.H0 + B.mat_off[m];
+  const long long npairs = (long long)nsh * (nsh + 1) / 2;
+  for (long long w = tid; w < npairs; w += nt) {
+    int si, sj;
+    tri_inverse(w, si, sj);
+    const int a = sh_atom[si], b = sh_atom[sj];
+    const int za = zs[a], zb = zs[b];
+    const int ka = sh_k[si], kb = sh_k[sj];
+    const ElemTable& ea = M.elem[za];
+    const ElemTable& eb = M.elem[zb];
+    const int la = ea.l[ka], lb = eb.l[kb];
+    const int mu0 = atom_ao[a] + ea.ao_first[ka], nu0 = atom_ao[b] + eb.ao_first[kb];
+    const int na = 2 * la + 1, nb = 2 * lb + 1;
+    const double sei = B.se[sh0 + si], sej = B.se[sh0 + sj];
+    double Sb[3][3];
+    double hij;
+    bool zero = false;
+    if (a == b) {
+      overlap_block<false>(la, ea.nprim[ka], ea.alpha[ka], ea.coef[ka], &xyz[3 * a], lb, eb.nprim[kb], eb.alpha[kb],
+                           eb.coef[kb], &xyz[3 * b], 2, Sb, nullptr, nullptr);
+      hij = 0.5 * (sei + sej);
+    } else {
+      const double dx = xyz[3 * a] - xyz[3 * b], dy = xyz[3 * a + 1] - xyz[3 * b + 1], dz = xyz[3 * a + 2] - xyz[3 * b + 2];
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      if (r2 <= 1e-24 || r2 > 900.0) {
+        zero = true;
+        hij = 0.0;
+      } else {
+        overlap_block<false>(la, ea.nprim[ka], ea.alpha[ka], ea.coef[ka], &xyz[3 * a], lb, eb.nprim[kb], eb.alpha[kb],
+                             eb.coef[kb], &xyz[3 * b], 2, Sb, nullptr, nullptr);
+        const double rr = sqrt(sqrt(r2) / (ea.rad + eb.rad));
+        const double poly = (1.0 + ea.poly[ka] * rr) * (1.0 + eb.poly[kb] * rr);
+        hij = 0.5 * (sei + sej) * hscale(M, za, ka, zb, kb) * poly;
+      }
+    }
+    for (int x = 0; x < na; ++x)
+      for (int y = 0; y < nb; ++y) {
+        const double s = zero ? 0.0 : Sb[x][y];
+        const long long i1 = (long long)(mu0 + x) * N + (nu0 + y);
+        const long long i2 = (long long)(nu0 + y) * N + (mu0 + x);
+        S[i1] = s;
+        S[i2] = s;
+        H0[i1] = s * hij;
+        H0[i2] = s * hij;
+      }
+  }
+
+  // ---- Klopman-Ohno matrix
+  double* G = B.gam + B.gam_off[m];
+  for (long long w = tid; w < (long long)nsh * nsh; w += nt) {
+    const int i = (int)(w / nsh), j = (int)(w % nsh);
+    const int a = sh_atom[i], b = sh_atom[j];
+    const double g = harmonic_avg(M.elem[zs[a]].hard[sh_k[i]], M.elem[zs[b]].hard[sh_k[j]]);
+    double v;
+    if (a == b) v = g;
+    else {
+      const double dx = xyz[3 * a] - xyz[3 * b], dy = xyz[3 * a + 1] - xyz[3 * b + 1], dz = xyz[3 * a + 2] - xyz[3 * b + 2];
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      v = 1.0 / sqrt(r2 + 1.0 / (g * g));
+    }
+    G[w] = v;
+  }
+
+  // ---- repulsion (pairs within 25 bohr), one thread per atom
+  double erep = 0.0;
+  for (int i = tid; i < nat; i += nt) {
+    const ElemTable& ei = M.elem[zs[i]];
+    double gx = 0, gy = 0, gz = 0, e = 0;
+    for (int j = 0; j < nat; ++j) {
+      if (j == i) continue;
+      const ElemTable& ej = M.elem[zs[j]];
+      const double dx = xyz[3 * j] - xyz[3 * i], dy = xyz[3 * j + 1] - xyz[3 * i + 1], dz = xyz[3 * j + 2] - xyz[3 * i + 2];
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      if (r2 <= 1e-24 || r2 > 625.0) continue;
+      const double r = sqrt(r2);
+      const double alpha = sqrt(ei.repa * ej.repa);
+      const double zeff = ei.repb * ej.repb;
+      const double k = (zs[i] <= 2 && zs[j] <= 2) ? M.g.kexplight : M.g.kexp;
+      const double rk = pow(r, k);
+      const double en = zeff * exp(-alpha * rk) / r;
+      const double pref = (alpha * rk * k + 1.0) * en / r2;
+      e += 0.5 * en;
+      gx += dx * pref;
+      gy += dy * pref;
+      gz += dz * pref;
+    }
+    erep += e;
+    B.grad_classic[3 * (a0 + i)] = gx;
+    B.grad_classic[3 * (a0 + i) + 1] = gy;
+    B.grad_classic[3 * (a0 + i) + 2] = gz;
+  }
+  erep = block_sum(erep, red);
+
+  // ---- D3(BJ)
+  double edisp = 0.0;
+  if (enable_dispersion) {
+    for (int i = tid; i < nat; i += nt) {  // reference weights, src/dispersion.rs:1629-1692
+      const ElemTable& e = M.elem[zs[i]];
+      const int nr = e.d3_nref;
+      double logit[kMaxRef], mx = -INFINITY;
+      for (int k = 0; k < nr; ++k) {
+        const double d = cnd[i] - e.d3_cnref[k];
+        logit[k] = -4.0 * d * d;
+        mx = fmax(mx, logit[k]);
+      }
+      double raw[kMaxRef], norm = 0.0, dnorm = 0.0;
+      for (int k = 0; k < nr; ++k) {
+        raw[k] = exp(logit[k] - mx);
+        norm += raw[k];
+        dnorm += 8.0 * (e.d3_cnref[k] - cnd[i]) * raw[k];
+      }
+      const double ninv = 1.0 / norm;
+      for (int k = 0; k < kMaxRef; ++k) {
+        double gwk = 0.0, dgk = 0.0;
+        if (k < nr) {
+          const double expd = 8.0 * (e.d3_cnref[k] - cnd[i]) * raw[k];
+          gwk = raw[k] * ninv;
+          dgk = expd * ninv - raw[k] * dnorm * ninv * ninv;
+          if (!isfinite(gwk)) gwk = 0.0;
+          if (!isfinite(dgk)) dgk = 0.0;
+        }
+        gw[k * maxn + i] = gwk;
+        dgw[k * maxn + i] = dgk;
+      }
+    }
+    __syncthreads();
+    const double s6 = M.g.s6, s8 = M.g.s8, a1 = M.g.a1, a2 = M.g.a2;
+    for (int i = tid; i < nat; i += nt) {  // pair terms, src/dispersion.rs:1260-1297
+      const int zi = zs[i];
+      const ElemTable& ei = M.elem[zi];
+      double gx = 0, gy = 0, gz = 0, e = 0, dc = 0;
+      for (int j = 0; j < nat; ++j) {
+        if (j == i) continue;
+        const int zj = zs[j];
+        const ElemTable& ej = M.elem[zj];
+        const double dx = xyz[3 * i] - xyz[3 * j], dy = xyz[3 * i + 1] - xyz[3 * j + 1], dz = xyz[3 * i + 2] - xyz[3 * j + 2];
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 <= 1e-24 || r2 > 2500.0 || r2 <= 1e-14) continue;
+        const double* c6r = M.c6ref + (long long)(zi * kNZ + zj) * (kMaxRef * kMaxRef);
+        double c6 = 0.0, dc6 = 0.0;
+        for (int ra = 0; ra < ei.d3_nref; ++ra) {
+          double rowc = 0.0;
+          for (int rb = 0; rb < ej.d3_nref; ++rb) rowc += gw[rb * maxn + j] * c6r[ra * kMaxRef + rb];
+          c6 += gw[ra * maxn + i] * rowc;
+          dc6 += dgw[ra * maxn + i] * rowc;
+        }
+        const double r4r2ij = 3.0 * ei.r4r2 * ej.r4r2;
+        const double r0 = a1 * sqrt(r4r2ij) + a2;
+        const double r02 = r0 * r0, r06 = r02 * r02 * r02, r08 = r06 * r02;
+        const double r4 = r2 * r2;
+        const double t6 = 1.0 / (r4 * r2 + r06);
+        const double t8 = 1.0 / (r4 * r4 + r08);
+        const double d6 = -6.0 * r4 * t6 * t6;
+        const double d8 = -8.0 * r4 * r2 * t8 * t8;
+        const double ed = s6 * t6 + s8 * r4r2ij * t8;
+        const double gd = s6 * d6 + s8 * r4r2ij * d8;
+        e -= 0.5 * c6 * ed;
+        gx += dx * (-c6 * gd);
+        gy += dy * (-c6 * gd);
+        gz += dz * (-c6 * gd);
+        dc -= dc6 * ed;
+      }
+      edisp += e;
+      dedcn[i] = dc;
+      B.grad_classic[3 * (a0 + i)] += gx;
+      B.grad_classic[3 * (a0 + i) + 1] += gy;
+      B.grad_classic[3 * (a0 + i) + 2] += gz;
+    }
+    __syncthreads();
+    for (int i = tid; i < nat; i += nt) {  // CN chain, src/dispersion.rs:1330-1342
+      const double ri = M.elem[zs[i]].rcov;
+      double gx = 0, gy = 0, gz = 0;
+      for (int j = 0; j < nat; ++j) {
+        if (j == i) continue;
+        const double dx = xyz[3 * i] - xyz[3 * j], dy = xyz[3 * i + 1] - xyz[3 * j + 1], dz = xyz[3 * i + 2] - xyz[3 * j + 2];
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 <= 1e-24 || r2 > 625.0) continue;
+        const double r = sqrt(r2);
+        double v, dv;
+        exp_count(r, ri + M.elem[zs[j]].rcov, v, dv);
+        const double pref = (dedcn[i] + dedcn[j]) * dv / r;
+        gx += dx * pref;
+        gy += dy * pref;
+        gz += dz * pref;
+      }
+      B.grad_classic[3 * (a0 + i)] += gx;
+      B.grad_classic[3 * (a0 + i) + 1] += gy;
+      B.grad_classic[3 * (a0 + i) + 2] += gz;
+    }
+    edisp = block_sum(edisp, red);
+  }
+  if (tid == 0) {
+    double* t = B.terms + (long long)m * kTerms;
+    for (int k = 0; k < kTerms; ++k) t[k] = 0.0;
+    t[2] = erep;
+    t[7] = edisp;
+  }
+}
+
+}  // namespace gfn1

@@ -1,0 +1,159 @@
+"""ctypes binding of the C ABI in include/gfn1_b200.h.
+
+The engine library must exist: there is no CPU fallback.  A missing or
+unloadable ``libgfn1_b200.so`` raises ``ImportError``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+from ._build import LIB_PATH, PKG_ROOT
+
+TABLES_PATH = os.path.join(PKG_ROOT, "data", "gfn1_tables.txt")
+
+GFN1_OK = 0
+STATUS_NAMES = {
+    0: "OK", 1: "Io", 2: "Parse", 3: "InvalidInput", 4: "MissingElement", 5: "MissingGlobal",
+    6: "LinearAlgebra", 7: "SingularCell", 8: "SccNotConverged", 9: "Device", 10: "Timeout",
+    11: "NonFinite", 12: "Unsupported",
+}
+TERM_NAMES = (
+    "total_free", "total_internal", "repulsion", "electronic", "isotropic_scc", "third_order",
+    "higher_order", "dispersion", "halogen", "multipole", "exchange", "spin_polarization",
+    "plus_u", "external_field", "electronic_entropy",
+)
+
+
+class Options(ctypes.Structure):
+    _fields_ = [
+        ("max_scc", ctypes.c_int32),
+        ("energy_tolerance", ctypes.c_double),
+        ("charge_tolerance", ctypes.c_double),
+        ("mixing", ctypes.c_double),
+        ("scc_broyden", ctypes.c_int32),
+        ("scc_broyden_size", ctypes.c_int32),
+        ("electronic_temperature", ctypes.c_double),
+        ("enable_dispersion", ctypes.c_int32),
+        ("compute_gradient", ctypes.c_int32),
+    ]
+
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int32)
+
+
+class Outputs(ctypes.Structure):
+    _fields_ = [
+        ("energy", _dp), ("terms", _dp), ("gradient", _dp), ("shell_charges", _dp),
+        ("atomic_charges", _dp), ("dipole", _dp), ("fermi_level", _dp), ("iterations", _ip),
+        ("status", _ip),
+    ]
+
+
+class Gfn1Error(ValueError):
+    """Engine error; ``code`` is the C status (1..8 mirror gfn1-rs Gfn1Error)."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(message)
+        self.code = code
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load():
+    """Load the engine library (raises ImportError if it was not built)."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"GFN1 B200 engine library not built: {LIB_PATH} (run __graft_entry__.build())")
+        L = ctypes.CDLL(LIB_PATH)
+        vp = ctypes.c_void_p
+        L.gfn1_default_options.argtypes = [ctypes.POINTER(Options)]
+        L.gfn1_last_error.argtypes = [vp]
+        L.gfn1_last_error.restype = ctypes.c_char_p
+        L.gfn1_engine_create.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(vp)]
+        L.gfn1_engine_destroy.argtypes = [vp]
+        L.gfn1_basis_size.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_uint8), _ip, _ip]
+        L.gfn1_run.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_uint8), _dp, ctypes.c_double, _dp,
+                               ctypes.POINTER(Options), ctypes.POINTER(Outputs)]
+        L.gfn1_batch_energy_gradient.argtypes = [vp, ctypes.c_int, _ip, ctypes.POINTER(ctypes.c_uint8), _dp, _dp, _dp,
+                                                 ctypes.POINTER(Options), ctypes.POINTER(Outputs)]
+        L.gfn1_batch_create.argtypes = [vp, ctypes.c_int, _ip, ctypes.POINTER(ctypes.c_uint8), _dp,
+                                        ctypes.POINTER(Options), ctypes.POINTER(vp)]
+        L.gfn1_batch_destroy.argtypes = [vp]
+        L.gfn1_batch_set_positions.argtypes = [vp, vp, ctypes.c_int]
+        L.gfn1_batch_set_initial_charges.argtypes = [vp, vp, ctypes.c_int]
+        L.gfn1_batch_launch.argtypes = [vp, vp]
+        L.gfn1_batch_download.argtypes = [vp, ctypes.POINTER(Outputs)]
+        L.gfn1_batch_outputs_device.argtypes = [vp, ctypes.POINTER(Outputs)]
+        L.gfn1_batch_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
+                                      ctypes.POINTER(ctypes.c_int64), _ip]
+        for name in ("gfn1_engine_create", "gfn1_basis_size", "gfn1_run", "gfn1_batch_energy_gradient",
+                     "gfn1_batch_create", "gfn1_batch_set_positions", "gfn1_batch_set_initial_charges",
+                     "gfn1_batch_launch", "gfn1_batch_download", "gfn1_batch_outputs_device", "gfn1_batch_info"):
+            getattr(L, name).restype = ctypes.c_int
+        _lib = L
+        return L
+
+
+def last_error(engine_handle=None) -> str:
+    return load().gfn1_last_error(engine_handle).decode()
+
+
+def check(rc: int, handle=None) -> None:
+    if rc != GFN1_OK:
+        raise Gfn1Error(rc, last_error(handle))
+
+
+def default_options(**kw) -> Options:
+    o = Options()
+    load().gfn1_default_options(ctypes.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise TypeError(f"unknown option {k}")
+        setattr(o, k, type(getattr(o, k))(v))
+    return o
+
+
+def ptr(a: np.ndarray | None, ctype=ctypes.c_double):
+    if a is None:
+        return None
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+class Engine:
+    """Owns a ``gfn1_engine`` (device tables + stream) for one CUDA device."""
+
+    def __init__(self, param_path: str | None = None, device: int = 0):
+        L = load()
+        spec = TABLES_PATH if param_path in (None, "", "builtin", "builtin:gfn1") else param_path
+        h = ctypes.c_void_p()
+        check(L.gfn1_engine_create(spec.encode(), int(device), ctypes.byref(h)))
+        self.handle = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "handle", None):
+            load().gfn1_engine_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def basis_size(self, numbers) -> tuple[int, int]:
+        z = np.ascontiguousarray(numbers, dtype=np.uint8)
+        nao, nsh = ctypes.c_int32(), ctypes.c_int32()
+        check(load().gfn1_basis_size(self.handle, len(z), ptr(z, ctypes.c_uint8), ctypes.byref(nao), ctypes.byref(nsh)),
+              self.handle)
+        return nao.value, nsh.value

@@ -1,0 +1,196 @@
+"""Batched GFN1-xTB energy + gradient of many independent molecules.
+
+``BatchCalculator.calculate`` is the host-buffer path (one C call; the host to
+device copies of the inputs and the device to host copies of the results are
+inside).  ``ResidentBatch`` keeps the topology and workspace on the device so
+coordinates can be replaced and the batch re-run with inputs already in HBM.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from .native import build_system, unit_scale
+
+
+@dataclass
+class BatchResult:
+    energy: np.ndarray          # [nmol] total_free (Eh)
+    terms: np.ndarray           # [nmol, 15]
+    gradient: np.ndarray | None  # [natoms, 3] (Eh/bohr)
+    shell_charges: np.ndarray   # [nshells]
+    atomic_charges: np.ndarray  # [natoms]
+    dipole: np.ndarray          # [nmol, 3]
+    fermi_level: np.ndarray     # [nmol]
+    iterations: np.ndarray      # [nmol]
+    status: np.ndarray          # [nmol]
+    atom_offsets: np.ndarray
+    shell_offsets: np.ndarray
+
+
+def _flatten(molecules, unit):
+    offs = [0]
+    zs, xs = [], []
+    for numbers, positions in molecules:
+        z, x = build_system(numbers, positions, unit)
+        zs.append(z)
+        xs.append(x)
+        offs.append(offs[-1] + len(z))
+    return (np.asarray(offs, dtype=np.int32), np.concatenate(zs).astype(np.uint8),
+            np.ascontiguousarray(np.concatenate(xs)))
+
+
+def _options(opts: dict, compute_gradient: bool) -> _lib.Options:
+    return _lib.default_options(compute_gradient=int(bool(compute_gradient)), **opts)
+
+
+class BatchCalculator:
+    def __init__(self, param_path=None, device=0, max_scc=250, energy_tolerance=1.0e-6, charge_tolerance=2.0e-5,
+                 mixing=0.4, scc_broyden=True, scc_broyden_size=250, electronic_temperature=300.0,
+                 enable_dispersion=True):
+        self.engine = _lib.Engine(param_path, device)
+        self.opts = dict(max_scc=max_scc, energy_tolerance=energy_tolerance, charge_tolerance=charge_tolerance,
+                         mixing=mixing, scc_broyden=int(bool(scc_broyden)), scc_broyden_size=scc_broyden_size,
+                         electronic_temperature=electronic_temperature,
+                         enable_dispersion=int(bool(enable_dispersion)))
+
+    def shell_offsets(self, atom_offsets, numbers) -> np.ndarray:
+        off = np.asarray(atom_offsets)
+        out = np.zeros(len(off), dtype=np.int64)
+        for m in range(len(off) - 1):
+            out[m + 1] = out[m] + self.engine.basis_size(numbers[off[m]:off[m + 1]])[1]
+        return out
+
+    def calculate_flat(self, atom_offsets, numbers, xyz_bohr, charges=None, initial_shell_charges=None,
+                       compute_gradient=True, raise_on_error=False) -> BatchResult:
+        """Flat inputs: atom_offsets [nmol+1], numbers [natoms], xyz_bohr [natoms,3]."""
+        L = _lib.load()
+        off = np.ascontiguousarray(atom_offsets, dtype=np.int32)
+        z = np.ascontiguousarray(numbers, dtype=np.uint8)
+        xyz = np.ascontiguousarray(xyz_bohr, dtype=np.float64).reshape(-1, 3)
+        nmol, natoms = len(off) - 1, int(off[-1])
+        shoff = self.shell_offsets(off, z)
+        nsh = int(shoff[-1])
+        ch = None if charges is None else np.ascontiguousarray(charges, dtype=np.float64)
+        q0 = None if initial_shell_charges is None else np.ascontiguousarray(initial_shell_charges, dtype=np.float64)
+        energy = np.zeros(nmol)
+        terms = np.zeros((nmol, 15))
+        grad = np.zeros((natoms, 3)) if compute_gradient else None
+        qsh = np.zeros(nsh)
+        qat = np.zeros(natoms)
+        dip = np.zeros((nmol, 3))
+        fermi = np.zeros(nmol)
+        iters = np.zeros(nmol, dtype=np.int32)
+        status = np.zeros(nmol, dtype=np.int32)
+        out = _lib.Outputs(_lib.ptr(energy), _lib.ptr(terms), _lib.ptr(grad), _lib.ptr(qsh), _lib.ptr(qat),
+                           _lib.ptr(dip), _lib.ptr(fermi), _lib.ptr(iters, ctypes.c_int32),
+                           _lib.ptr(status, ctypes.c_int32))
+        opt = _options(self.opts, compute_gradient)
+        rc = L.gfn1_batch_energy_gradient(self.engine.handle, nmol, _lib.ptr(off, ctypes.c_int32),
+                                          _lib.ptr(z, ctypes.c_uint8), _lib.ptr(xyz), _lib.ptr(ch), _lib.ptr(q0),
+                                          ctypes.byref(opt), ctypes.byref(out))
+        if rc != 0 and (raise_on_error or rc not in (3, 4, 8, 12)):
+            _lib.check(rc, self.engine.handle)
+        return BatchResult(energy, terms, grad, qsh, qat, dip, fermi, iters, status, off, shoff)
+
+    def calculate(self, molecules, unit="angstrom", charges=None, compute_gradient=True, **kw) -> BatchResult:
+        """molecules: iterable of (numbers, positions) in `unit`."""
+        off, z, xyz = _flatten(molecules, unit)
+        return self.calculate_flat(off, z, xyz, charges=charges, compute_gradient=compute_gradient, **kw)
+
+    def resident(self, atom_offsets, numbers, charges=None, compute_gradient=True) -> "ResidentBatch":
+        return ResidentBatch(self, atom_offsets, numbers, charges, compute_gradient)
+
+
+class ResidentBatch:
+    """Device-resident batch: topology uploaded once, coordinates replaceable."""
+
+    def __init__(self, calc: BatchCalculator, atom_offsets, numbers, charges=None, compute_gradient=True):
+        L = _lib.load()
+        self.calc = calc
+        self.atom_offsets = np.ascontiguousarray(atom_offsets, dtype=np.int32)
+        self.numbers = np.ascontiguousarray(numbers, dtype=np.uint8)
+        self.nmol = len(self.atom_offsets) - 1
+        ch = None if charges is None else np.ascontiguousarray(charges, dtype=np.float64)
+        opt = _options(calc.opts, compute_gradient)
+        h = ctypes.c_void_p()
+        _lib.check(L.gfn1_batch_create(calc.engine.handle, self.nmol, _lib.ptr(self.atom_offsets, ctypes.c_int32),
+                                       _lib.ptr(self.numbers, ctypes.c_uint8), _lib.ptr(ch), ctypes.byref(opt),
+                                       ctypes.byref(h)), calc.engine.handle)
+        self.handle = h
+        na, ns, no = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        nl = ctypes.c_int32()
+        L.gfn1_batch_info(h, ctypes.byref(na), ctypes.byref(ns), ctypes.byref(no), ctypes.byref(nl))
+        self.natoms, self.nshells, self.naos, self.launches = na.value, ns.value, no.value, nl.value
+        self.compute_gradient = compute_gradient
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _lib.load().gfn1_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_positions(self, xyz, on_device: bool = False):
+        """xyz: numpy array (bohr) or, with on_device=True, an integer device pointer."""
+        if on_device:
+            p = ctypes.c_void_p(int(xyz))
+        else:
+            arr = np.ascontiguousarray(xyz, dtype=np.float64)
+            self._xyz_keep = arr
+            p = arr.ctypes.data_as(ctypes.c_void_p)
+        _lib.check(_lib.load().gfn1_batch_set_positions(self.handle, p, int(on_device)), self.calc.engine.handle)
+
+    def set_initial_charges(self, q, on_device: bool = False):
+        if q is None:
+            p = None
+        elif on_device:
+            p = ctypes.c_void_p(int(q))
+        else:
+            arr = np.ascontiguousarray(q, dtype=np.float64)
+            self._q_keep = arr
+            p = arr.ctypes.data_as(ctypes.c_void_p)
+        _lib.check(_lib.load().gfn1_batch_set_initial_charges(self.handle, p, int(on_device)), self.calc.engine.handle)
+
+    def launch(self, stream: int | None = None):
+        """Enqueue the kernels on a CUDA stream handle (int) or the engine stream."""
+        s = None if stream is None else ctypes.c_void_p(int(stream))
+        _lib.check(_lib.load().gfn1_batch_launch(self.handle, s), self.calc.engine.handle)
+
+    def device_outputs(self) -> dict:
+        out = _lib.Outputs()
+        _lib.check(_lib.load().gfn1_batch_outputs_device(self.handle, ctypes.byref(out)), self.calc.engine.handle)
+        def addr(p):
+            return ctypes.cast(p, ctypes.c_void_p).value
+        return {k: addr(getattr(out, k)) for k in ("terms", "gradient", "shell_charges", "atomic_charges", "dipole",
+                                                   "fermi_level", "iterations", "status")}
+
+    def download(self) -> BatchResult:
+        L = _lib.load()
+        energy = np.zeros(self.nmol)
+        terms = np.zeros((self.nmol, 15))
+        grad = np.zeros((self.natoms, 3)) if self.compute_gradient else None
+        qsh = np.zeros(self.nshells)
+        qat = np.zeros(self.natoms)
+        dip = np.zeros((self.nmol, 3))
+        fermi = np.zeros(self.nmol)
+        iters = np.zeros(self.nmol, dtype=np.int32)
+        status = np.zeros(self.nmol, dtype=np.int32)
+        out = _lib.Outputs(_lib.ptr(energy), _lib.ptr(terms), _lib.ptr(grad), _lib.ptr(qsh), _lib.ptr(qat),
+                           _lib.ptr(dip), _lib.ptr(fermi), _lib.ptr(iters, ctypes.c_int32),
+                           _lib.ptr(status, ctypes.c_int32))
+        rc = L.gfn1_batch_download(self.handle, ctypes.byref(out))
+        if rc not in (0, 3, 4, 8, 12):
+            _lib.check(rc, self.calc.engine.handle)
+        shoff = self.calc.shell_offsets(self.atom_offsets, self.numbers)
+        return BatchResult(energy, terms, grad, qsh, qat, dip, fermi, iters, status, self.atom_offsets, shoff)
+
+
+__all__ = ["BatchCalculator", "BatchResult", "ResidentBatch", "unit_scale"]

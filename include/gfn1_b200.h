@@ -1,0 +1,126 @@
+/* C ABI of the B200 GFN1-xTB single-point engine (non-periodic SCC energy plus
+ * analytic gradient).  Plain pointers and sizes only; no CUDA or torch types.
+ *
+ * Units: bohr and Hartree (the reference's Rust API units).  Matrices and
+ * per-atom vectors are row-major, atoms in input order.
+ *
+ * Status codes: 0 = OK; 1..8 mirror the reference's Gfn1Error variants
+ * (gfn1-rs src/error.rs:8-17); 9..12 are device-side conditions.
+ */
+#ifndef GFN1_B200_H
+#define GFN1_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  GFN1_OK = 0,
+  GFN1_E_IO = 1,                /* Gfn1Error::Io */
+  GFN1_E_PARSE = 2,             /* Gfn1Error::Parse */
+  GFN1_E_INVALID_INPUT = 3,     /* Gfn1Error::InvalidInput (also: overlap not positive definite) */
+  GFN1_E_MISSING_ELEMENT = 4,   /* Gfn1Error::MissingElement */
+  GFN1_E_MISSING_GLOBAL = 5,    /* Gfn1Error::MissingGlobal */
+  GFN1_E_LINEAR_ALGEBRA = 6,    /* Gfn1Error::LinearAlgebra */
+  GFN1_E_SINGULAR_CELL = 7,     /* Gfn1Error::SingularCell (periodic input is rejected) */
+  GFN1_E_SCC_NOT_CONVERGED = 8, /* Gfn1Error::SccNotConverged */
+  GFN1_E_DEVICE = 9,            /* CUDA error */
+  GFN1_E_TIMEOUT = 10,          /* host-side wait exceeded */
+  GFN1_E_NAN = 11,              /* non-finite input or result */
+  GFN1_E_UNSUPPORTED = 12       /* element outside the device path (d/f shells, halogen-bond donors) */
+};
+
+typedef struct gfn1_engine gfn1_engine;
+typedef struct gfn1_batch gfn1_batch;
+
+/* Plain-path subset of ElectronicOptions (gfn1-rs src/electronic.rs:157-453,
+ * defaults :395-452) plus the gradient switch of AnalyticGradientOptions
+ * (src/gradient.rs:21-41). */
+typedef struct gfn1_options {
+  int32_t max_scc;               /* 250 */
+  double energy_tolerance;       /* 1e-6 Eh */
+  double charge_tolerance;       /* 2e-5 e */
+  double mixing;                 /* 0.4 */
+  int32_t scc_broyden;           /* 1 */
+  int32_t scc_broyden_size;      /* 250 */
+  double electronic_temperature; /* 300 K */
+  int32_t enable_dispersion;     /* 1 */
+  int32_t compute_gradient;      /* 1 */
+} gfn1_options;
+
+/* Per-batch outputs; any pointer may be NULL.  For gfn1_batch_download the
+ * pointers are host memory, for gfn1_batch_outputs_device they receive device
+ * pointers owned by the batch. */
+typedef struct gfn1_outputs {
+  double* energy;         /* [nmol]   total_free (src/python.rs:2926) */
+  double* terms;          /* [nmol*15] EnergyTerms::named_values order (src/electronic.rs:681-699) */
+  double* gradient;       /* [natoms*3] dE/dR (src/gradient.rs:44-54) */
+  double* shell_charges;  /* [nshells] Mulliken shell charges */
+  double* atomic_charges; /* [natoms] */
+  double* dipole;         /* [nmol*3] Mulliken dipole (src/field.rs:89-95) */
+  double* fermi_level;    /* [nmol] */
+  int32_t* iterations;    /* [nmol] */
+  int32_t* status;        /* [nmol] per-molecule status code */
+} gfn1_outputs;
+
+/* Fills the ElectronicOptions defaults. */
+void gfn1_default_options(gfn1_options* opt);
+
+/* Replaces Gfn1Parameters::resolve (gfn1-rs src/params.rs:206-227) plus the
+ * engine state: param_spec is NULL/"builtin" (the bundled GFN1-xTB tables) or a
+ * path to a tables file written by gen_tables.py.  device = CUDA ordinal. */
+int gfn1_engine_create(const char* param_spec, int device, gfn1_engine** out);
+void gfn1_engine_destroy(gfn1_engine* eng);
+
+/* Thread-local message of the last failing call on this engine (never NULL). */
+const char* gfn1_last_error(const gfn1_engine* eng);
+
+/* Number of AOs and shells of a molecule; mirrors BasisSet::build
+ * (src/basis.rs:121-233).  Returns GFN1_E_UNSUPPORTED for elements outside the
+ * device path. */
+int gfn1_basis_size(const gfn1_engine* eng, int nat, const uint8_t* z, int32_t* nao, int32_t* nshells);
+
+/* One molecule, host buffers.  Replaces run_electronic (src/electronic.rs:800-804)
+ * when opt->compute_gradient == 0 and analytic_gradient (src/gradient.rs:56-60)
+ * otherwise.  `out` arrays are sized for this one molecule. */
+int gfn1_run(gfn1_engine* eng, int nat, const uint8_t* z, const double* xyz_bohr, double charge,
+             const double* init_shell_q, const gfn1_options* opt, const gfn1_outputs* out);
+
+/* Batched energy + gradient of independent molecules, host buffers in and out
+ * (host<->device copies inside).  atom_offsets has nmol+1 entries; charge and
+ * init_shell_q (initial SCC shell charges, the hook of
+ * ElectronicOptions::scc_initial_shell_charges, src/electronic.rs:386-392) may
+ * be NULL.  Returns GFN1_OK when every molecule succeeded, otherwise the largest
+ * per-molecule status (see out->status). */
+int gfn1_batch_energy_gradient(gfn1_engine* eng, int nmol, const int32_t* atom_offsets, const uint8_t* z,
+                               const double* xyz_bohr, const double* charge, const double* init_shell_q,
+                               const gfn1_options* opt, const gfn1_outputs* out);
+
+/* Resident-batch interface: the topology (atom counts, elements, charges) is
+ * uploaded once; coordinates can then be replaced and the batch re-run with
+ * inputs already on the device (molecular dynamics, benchmarking).
+ * gfn1_batch_create validates the input and sizes the device workspace. */
+int gfn1_batch_create(gfn1_engine* eng, int nmol, const int32_t* atom_offsets, const uint8_t* z,
+                      const double* charge, const gfn1_options* opt, gfn1_batch** out);
+void gfn1_batch_destroy(gfn1_batch* b);
+/* Copies natoms*3 coordinates (bohr); `on_device` = 1 when xyz is a device pointer. */
+int gfn1_batch_set_positions(gfn1_batch* b, const double* xyz, int on_device);
+/* Initial shell charges (nshells values) or NULL for the zero guess. */
+int gfn1_batch_set_initial_charges(gfn1_batch* b, const double* q, int on_device);
+/* Enqueues setup, SCC and gradient kernels on `stream` (a cudaStream_t passed as
+ * a void pointer; NULL = the engine's stream).  Asynchronous. */
+int gfn1_batch_launch(gfn1_batch* b, void* stream);
+/* Synchronises and copies results to host buffers. */
+int gfn1_batch_download(gfn1_batch* b, const gfn1_outputs* out);
+/* Device pointers of the batch-owned result arrays (valid until destroy). */
+int gfn1_batch_outputs_device(gfn1_batch* b, gfn1_outputs* out);
+/* Sizes of the batch: natoms, nshells, total AOs; launches = kernels per run. */
+int gfn1_batch_info(const gfn1_batch* b, int64_t* natoms, int64_t* nshells, int64_t* naos, int32_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GFN1_B200_H */

@@ -1,0 +1,137 @@
+"""GPU engine vs the CPU FP64 oracle through the C ABI.
+
+Tolerances (stated per result): |dE| <= 1e-6 Eh, max|dg| <= 1e-5 Eh/bohr,
+max|dq_shell| <= 1e-5 e.  Both sides run the same SCC options; the SCC is
+converged tightly (1e-10 Eh / 1e-8 e) in the parity cases so the comparison
+measures the arithmetic, not the convergence threshold.
+"""
+import numpy as np
+import pytest
+
+from conftest import ANGSTROM_TO_BOHR, smoke_molecule
+
+pytestmark = pytest.mark.gpu
+
+E_TOL, G_TOL, Q_TOL = 1e-6, 1e-5, 1e-5
+TIGHT = dict(energy_tolerance=1e-10, charge_tolerance=1e-8)
+
+
+def _compare(calc, oracle_mod, z, x, opts=None, e_tol=E_TOL, g_tol=G_TOL, q_tol=Q_TOL):
+    opts = opts or {}
+    calc.opts.update(opts)
+    r = calc.calculate_flat([0, len(z)], z, x, raise_on_error=True)
+    o = oracle_mod.run(z, x, options=oracle_mod.make_options(**opts))
+    assert r.status[0] == 0
+    de = abs(r.energy[0] - o.energy)
+    dg = np.max(np.abs(r.gradient - o.gradient))
+    dq = np.max(np.abs(r.shell_charges - o.shell_charges))
+    assert de <= e_tol, f"dE={de:.3e}"
+    assert dg <= g_tol, f"dg={dg:.3e}"
+    assert dq <= q_tol, f"dq={dq:.3e}"
+    for k, name in enumerate(("total_free", "total_internal", "repulsion", "electronic", "isotropic_scc",
+                              "third_order")):
+        assert abs(r.terms[0, k] - o.terms[name]) <= e_tol, name
+    return r, o
+
+
+@pytest.fixture
+def calc(gpu_calc):
+    saved = dict(gpu_calc.opts)
+    yield gpu_calc
+    gpu_calc.opts.clear()
+    gpu_calc.opts.update(saved)
+
+
+def test_h2_golden_on_gpu(calc, fixtures):
+    g = fixtures["h2_engrad"]
+    r = calc.calculate_flat([0, 2], g["numbers"], g["positions_bohr"], raise_on_error=True)
+    assert abs(r.energy[0] - g["energy"]) < 1e-9
+    assert np.max(np.abs(r.gradient - np.array(g["gradient"]))) < 1e-7
+
+
+@pytest.mark.parametrize("name", ["hydrogen", "hydrogen fluoride", "water", "borane", "caffeine"])
+def test_reference_molecules(calc, oracle_mod, fixtures, name):
+    z, x = smoke_molecule(fixtures, name)
+    _compare(calc, oracle_mod, z, x, TIGHT, e_tol=1e-8, g_tol=1e-7, q_tol=1e-7)
+
+
+@pytest.mark.parametrize("name", ["water", "ammonia", "methane"])
+def test_reference_examples_default_options(calc, oracle_mod, fixtures, name):
+    rec = fixtures["xyz"][name]
+    z = np.array(rec["numbers"])
+    x = np.array(rec["positions_angstrom"]) * ANGSTROM_TO_BOHR
+    _compare(calc, oracle_mod, z, x)
+
+
+def test_water16_cluster(calc, oracle_mod):
+    from gfn1_rs import workloads
+
+    z, x = workloads.water_cluster(16, 0)
+    _compare(calc, oracle_mod, z, x * ANGSTROM_TO_BOHR, dict(energy_tolerance=1e-8))
+
+
+def test_mixed_batch_vs_oracle(calc, oracle_mod):
+    from gfn1_rs import workloads
+
+    off, z, x = workloads.mixed_batch(48, 1000)
+    xb = x * ANGSTROM_TO_BOHR
+    r = calc.calculate_flat(off, z, xb, raise_on_error=True)
+    e, g, q, shoff, it, st = oracle_mod.run_batch(off, z, xb)
+    assert np.all(r.status == 0) and np.all(st == 0)
+    assert np.max(np.abs(r.energy - e)) <= E_TOL
+    assert np.max(np.abs(r.gradient - g)) <= G_TOL
+    assert np.max(np.abs(r.shell_charges - q)) <= Q_TOL
+
+
+def test_batch_order_independence_and_determinism(calc):
+    from gfn1_rs import workloads
+
+    off, z, x = workloads.mixed_batch(24, 2000)
+    xb = x * ANGSTROM_TO_BOHR
+    r1 = calc.calculate_flat(off, z, xb)
+    r2 = calc.calculate_flat(off, z, xb)
+    assert np.array_equal(r1.energy, r2.energy)
+    assert np.array_equal(r1.gradient, r2.gradient)
+    # each molecule alone gives the same numbers as inside the batch
+    for m in (0, 7, 23):
+        a0, a1 = off[m], off[m + 1]
+        rs = calc.calculate_flat([0, a1 - a0], z[a0:a1], xb[a0:a1])
+        assert abs(rs.energy[0] - r1.energy[m]) < 1e-12
+        assert np.max(np.abs(rs.gradient - r1.gradient[a0:a1])) < 1e-12
+
+
+def test_translation_invariance_gpu(calc, fixtures):
+    z, x = smoke_molecule(fixtures, "caffeine")
+    r0 = calc.calculate_flat([0, len(z)], z, x)
+    r1 = calc.calculate_flat([0, len(z)], z, x + np.array([5.0, -3.0, 2.0]))
+    assert abs(r0.energy[0] - r1.energy[0]) < 1e-9
+    assert np.max(np.abs(r0.gradient.sum(axis=0))) < 1e-9
+
+
+def test_unsupported_element_is_rejected(calc, fixtures):
+    z, x = smoke_molecule(fixtures, "phosphine")  # P carries a 3d shell
+    r = calc.calculate_flat([0, len(z)], z, x)
+    assert r.status[0] == 12
+
+
+def test_not_converged_status(calc, fixtures):
+    z, x = smoke_molecule(fixtures, "caffeine")
+    calc.opts.update(max_scc=2, energy_tolerance=1e-12, charge_tolerance=1e-12)
+    r = calc.calculate_flat([0, len(z)], z, x)
+    assert r.status[0] == 8
+
+
+def test_charged_molecule(calc, oracle_mod, fixtures):
+    z, x = smoke_molecule(fixtures, "water")
+    r = calc.calculate_flat([0, len(z)], z, x, charges=[1.0], raise_on_error=True)
+    o = oracle_mod.run(z, x, options=oracle_mod.make_options(charge=1.0))
+    assert abs(r.energy[0] - o.energy) < E_TOL
+    assert abs(r.atomic_charges.sum() - 1.0) < 1e-8
+
+
+def test_initial_guess_converges_to_same_result(calc, oracle_mod, fixtures):
+    z, x = smoke_molecule(fixtures, "caffeine")
+    o = oracle_mod.run(z, x)
+    r = calc.calculate_flat([0, len(z)], z, x, initial_shell_charges=o.shell_charges, raise_on_error=True)
+    assert abs(r.energy[0] - o.energy) < E_TOL
+    assert r.iterations[0] <= o.iterations

@@ -1,0 +1,119 @@
+"""The CPU FP64 oracle against the reference's own fixtures and gates.
+
+* examples/h2.engrad (the only stored absolute result): energy to 1e-9 Eh;
+  the gradient to 1e-7 Eh/bohr (the file's gradient differs from the exact
+  derivative of its own energy by 2.6e-8 Eh/bohr; see test_h2_gradient_is_exact_derivative);
+* the finite-difference gradient gate of tests/nonpbc_smoke.rs:108-150
+  (h = 1e-4 bohr, 5e-5 Eh/bohr) on its H/B/F/O/P molecules;
+* the single-coordinate probe of tests/nonpbc_smoke.rs:152-180 on caffeine;
+* mixer independence (tests/scf_accelerators.rs:41-75), translation/rotation
+  invariance (tests/physical_consistency.rs:285-302) and the energy bookkeeping
+  identity (src/electronic.rs:4057-4125).
+"""
+import numpy as np
+import pytest
+
+from conftest import ANGSTROM_TO_BOHR, smoke_molecule
+
+
+def test_h2_golden(oracle_mod, fixtures):
+    g = fixtures["h2_engrad"]
+    r = oracle_mod.run(g["numbers"], g["positions_bohr"], gradient=True)
+    assert r.converged
+    assert abs(r.energy - g["energy"]) < 1e-9
+    assert np.max(np.abs(r.gradient - np.array(g["gradient"]))) < 1e-7
+
+
+def test_h2_gradient_is_exact_derivative(oracle_mod, fixtures):
+    g = fixtures["h2_engrad"]
+    opt = oracle_mod.make_options(energy_tolerance=1e-12, charge_tolerance=1e-10)
+    x0 = np.array(g["positions_bohr"])
+
+    def e(dx):
+        x = x0.copy()
+        x[1, 0] += dx
+        return oracle_mod.run(g["numbers"], x, options=opt, gradient=False).energy
+
+    fd = lambda h: (e(h) - e(-h)) / (2 * h)
+    rich = (4 * fd(1e-3) - fd(2e-3)) / 3
+    an = oracle_mod.run(g["numbers"], x0, options=opt).gradient[1, 0]
+    assert abs(rich - an) < 1e-10
+
+
+@pytest.mark.parametrize("name", ["hydrogen", "hydrogen fluoride", "water", "phosphine", "borane"])
+def test_fd_gradient_gate(oracle_mod, fixtures, name):
+    z, x = smoke_molecule(fixtures, name)
+    r = oracle_mod.run(z, x, gradient=True)
+    h = 1e-4
+    for a in range(len(z)):
+        for k in range(3):
+            xp, xm = x.copy(), x.copy()
+            xp[a, k] += h
+            xm[a, k] -= h
+            fd = (oracle_mod.run(z, xp, gradient=False).energy - oracle_mod.run(z, xm, gradient=False).energy) / (2 * h)
+            assert abs(fd - r.gradient[a, k]) < 5e-5
+
+
+def test_caffeine_single_coordinate_probe(oracle_mod, fixtures):
+    z, x = smoke_molecule(fixtures, "caffeine")
+    r = oracle_mod.run(z, x, gradient=True)
+    h = 1e-4
+    xp, xm = x.copy(), x.copy()
+    xp[0, 0] += h
+    xm[0, 0] -= h
+    fd = (oracle_mod.run(z, xp, gradient=False).energy - oracle_mod.run(z, xm, gradient=False).energy) / (2 * h)
+    assert abs(fd - r.gradient[0, 0]) < 1e-4
+
+
+def test_mixer_independence(oracle_mod, fixtures):
+    z, x = smoke_molecule(fixtures, "caffeine")
+    tight = dict(energy_tolerance=1e-10, charge_tolerance=1e-8)
+    eb = oracle_mod.run(z, x, options=oracle_mod.make_options(scc_broyden=True, **tight), gradient=False).energy
+    el = oracle_mod.run(z, x, options=oracle_mod.make_options(scc_broyden=False, max_scc=800, **tight),
+                        gradient=False).energy
+    assert abs(eb - el) < 1e-7
+
+
+def test_translation_rotation_invariance(oracle_mod, fixtures):
+    z, x = smoke_molecule(fixtures, "water")
+    r0 = oracle_mod.run(z, x)
+    rng = np.random.default_rng(5)
+    q = rng.normal(size=4)
+    q /= np.linalg.norm(q)
+    w, a, b, c = q
+    R = np.array([[1 - 2 * (b * b + c * c), 2 * (a * b - c * w), 2 * (a * c + b * w)],
+                  [2 * (a * b + c * w), 1 - 2 * (a * a + c * c), 2 * (b * c - a * w)],
+                  [2 * (a * c - b * w), 2 * (b * c + a * w), 1 - 2 * (a * a + b * b)]])
+    x2 = x @ R.T + np.array([3.0, -7.0, 11.0])
+    r1 = oracle_mod.run(z, x2)
+    assert abs(r0.energy - r1.energy) < 1e-9
+    assert np.max(np.abs(r0.gradient @ R.T - r1.gradient)) < 1e-7
+    assert np.max(np.abs(r0.gradient.sum(axis=0))) < 1e-9
+
+
+def test_energy_bookkeeping(oracle_mod, fixtures):
+    z, x = smoke_molecule(fixtures, "caffeine")
+    t = oracle_mod.run(z, x, gradient=False).terms
+    comp = sum(t[k] for k in ("repulsion", "electronic", "isotropic_scc", "third_order", "higher_order",
+                              "dispersion", "halogen", "multipole", "exchange", "spin_polarization", "plus_u",
+                              "external_field"))
+    assert abs(comp - t["total_internal"]) < 1e-12
+    assert abs(t["total_internal"] + t["electronic_entropy"] - t["total_free"]) < 1e-12
+
+
+def test_reference_example_geometries(oracle_mod, fixtures):
+    for name in ("water", "ammonia", "methane"):
+        rec = fixtures["xyz"][name]
+        r = oracle_mod.run(rec["numbers"], np.array(rec["positions_angstrom"]) * ANGSTROM_TO_BOHR)
+        assert r.converged and np.isfinite(r.energy)
+        assert abs(r.atomic_charges.sum()) < 1e-6
+
+
+def test_robust_ladder_recovers(oracle_mod, fixtures):
+    """max_scc = 1 fails rung 0; the linear-mixing + level-shift rungs of the
+    fallback ladder (src/electronic.rs:1390-1447) converge to the same energy."""
+    z, x = smoke_molecule(fixtures, "water")
+    ref = oracle_mod.run(z, x, gradient=False).energy
+    r = oracle_mod.run(z, x, options=oracle_mod.make_options(max_scc=1), gradient=False)
+    assert r.converged and r.iterations > 1
+    assert abs(r.energy - ref) < 1e-6
