@@ -1,0 +1,349 @@
+#!/usr/bin/env python
+"""SCC energy + analytic gradient evaluations per second on B200.
+
+Workload (the batched configuration the headline metric is quoted on): 4096
+independent molecules, each a seeded cluster of 1-15 rigid H2O/NH3/CH4 monomers
+(3-75 atoms, 8-180 AOs; seeds 1000 + i, rank r uses 1000 + r*4096 + i), default
+SCC options (FP64, Broyden, T_el = 300 K, 1e-6 Eh / 2e-5 e), analytic gradient.
+A step is one full evaluation of the batch: setup kernel (CN, S, H0, Coulomb,
+repulsion, D3), persistent SCC kernel, gradient kernel.
+
+value: evals/s with the coordinates resident in HBM, kernels timed with CUDA
+events on the launching stream, L2 flushed (256 MiB write) between steps.
+e2e: the same metric through gfn1_batch_energy_gradient with host buffers (the
+host->device input copy and the device->host result copy inside every step).
+
+--impl reference times the CPU restatement of gfn1-rs's path (oracle/, C++ FP64,
+all host threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "gfn1-rs_b200", "python"))
+
+import numpy as np  # noqa: E402
+
+A2B = 1.8897261246257702
+METRIC = "SCC energy+grad evals/s on 1 B200: learned+batched vs plain, |dE|<=1e-6 Eh"
+UNIT = "evals/s"
+NMOL = 4096
+SEED0 = 1000
+
+
+def workload_config(nmol, natoms, naos):
+    return {
+        "workload": f"batched plain GFN1-xTB SCC energy+gradient, {nmol} mixed H2O/NH3/CH4 clusters "
+                    f"(1-15 monomers, 3-75 atoms, 8-180 AOs, seeds 1000+i)",
+        "nmol": nmol,
+        "natoms": int(natoms),
+        "naos": int(naos),
+        "scc": "FP64, Broyden(250), T_el 300 K, 1e-6 Eh / 2e-5 e",
+        "guess": "zero shell charges (plain)",
+        "l2": "256 MiB flush between timed steps",
+    }
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nmol", type=int, default=NMOL)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        try:
+            for line in open(self.path):
+                p = [x.strip() for x in line.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    sm.append(float(p[1]))
+                    mx = float(p[2])
+                except ValueError:
+                    continue
+                for n, v in zip(names, p[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        except OSError:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except OSError:
+                pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def fp64_peak_tflops(torch, dev) -> float:
+    """cuBLAS FP64 GEMM burst throughput on this GPU (8192^3, best of 3)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    best = float("inf")
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def scc_flops(off, z, iters, nao_z, nsh_z) -> float:
+    """Algorithmic FP64 work of the SCC kernel: per molecule iterations x
+    (12 N^3 + 2 N^2 + 2 nsh^2) + 14 N^3 (orthogonaliser and energy-weighted density)."""
+    cn = np.concatenate([[0], np.cumsum(nao_z[z])])
+    cs = np.concatenate([[0], np.cumsum(nsh_z[z])])
+    N = (cn[off[1:]] - cn[off[:-1]]).astype(np.float64)
+    S = (cs[off[1:]] - cs[off[:-1]]).astype(np.float64)
+    return float(np.sum(iters * (12 * N ** 3 + 2 * N ** 2 + 2 * S ** 2) + 14 * N ** 3))
+
+
+def read_traffic():
+    """dram bytes per SCC launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "scc_kernel_mixed.md")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_full_launch:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_baseline(off, z, xyz_bohr, budget_s=15.0):
+    """The CPU FP64 restatement of the reference path on all host threads, on a
+    growing prefix sample of the workload until about `budget_s` of wall time."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    cores = os.cpu_count() or 1
+    n = min(16, len(off) - 1)
+    total_t, total_n = 0.0, 0
+    while True:
+        t0 = time.perf_counter()
+        _, _, _, _, _, st = oracle.run_batch(off[:n + 1], z[:off[n]], xyz_bohr[:off[n]], nthreads=cores)
+        dt = time.perf_counter() - t0
+        total_t, total_n = dt, n
+        if dt * 2.5 > budget_s or n >= len(off) - 1:
+            break
+        n = min(len(off) - 1, n * 2)
+    return {"value": total_n / total_t, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"first {total_n} molecules of the workload, C++ FP64 restatement (oracle/), {total_t:.1f} s"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    from gfn1_rs import workloads
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    off, z, x = workloads.mixed_batch(args.nmol, SEED0)
+    xb = x * A2B
+    cores = os.cpu_count() or 1
+    sample = min(args.nmol, 192)
+    # each step evaluates the next `sample` molecules of the workload (wrapping)
+    times = []
+    for step in range(args.warmup + args.steps):
+        m0 = (step * sample) % (args.nmol - sample + 1)
+        sub_off = off[m0:m0 + sample + 1] - off[m0]
+        t0 = time.perf_counter()
+        _, _, _, _, _, st = oracle.run_batch(sub_off, z[off[m0]:off[m0 + sample]], xb[off[m0]:off[m0 + sample]],
+                                             nthreads=cores)
+        dt = time.perf_counter() - t0
+        if step >= args.warmup:
+            times.append(dt)
+    t = sum(times)
+    value = sample * len(times) / t
+    naos = sum(int({1: 2, 6: 4, 7: 4, 8: 4}[int(a)]) for a in z)
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1e3 * t / len(times), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded clusters)", "impl": "reference",
+           "config": workload_config(args.nmol, off[-1], naos),
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                            "sample": f"{sample} molecules per step, C++ FP64 restatement of gfn1-rs (oracle/)"},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+
+    from gfn1_rs import BatchCalculator, workloads
+
+    off, z, x = workloads.mixed_batch(args.nmol, SEED0 + rank * args.nmol)
+    xb = np.ascontiguousarray(x * A2B)
+    calc = BatchCalculator(device=local)
+    nao_z, nsh_z = calc.engine.element_sizes()
+    naos = int(np.sum(nao_z[z]))
+
+    # ---- device-resident timing (value, per-kernel roofline)
+    rb = calc.resident(off, z)
+    d_xyz = torch.tensor(xb, dtype=torch.float64, device=dev)
+    rb.set_positions(d_xyz.data_ptr(), on_device=True)
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            rb.launch(stream.cuda_stream)
+    stream.synchronize()
+    res0 = rb.download()
+    if np.any(res0.status != 0):
+        bad = np.flatnonzero(res0.status)
+        raise SystemExit(f"{len(bad)} molecules failed (first {bad[0]}: status {res0.status[bad[0]]})")
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            for k in range(args.steps):
+                flush.fill_(float(k))
+                ev[k][0].record(stream)
+                rb.launch_stage(0, stream.cuda_stream)
+                ev[k][1].record(stream)
+                rb.launch_stage(1, stream.cuda_stream)
+                ev[k][2].record(stream)
+                rb.launch_stage(2, stream.cuda_stream)
+                ev[k][3].record(stream)
+        stream.synchronize()
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    setup_ms = [e[0].elapsed_time(e[1]) for e in ev]
+    scc_ms = [e[1].elapsed_time(e[2]) for e in ev]
+    grad_ms = [e[2].elapsed_time(e[3]) for e in ev]
+    step_ms = [e[0].elapsed_time(e[3]) for e in ev]
+    total_s = sum(step_ms) / 1e3
+    res = rb.download()
+    if dist:
+        t = torch.tensor([total_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_s = float(t.item())
+    value = args.nmol * world * args.steps / total_s
+
+    # ---- roofline of the dominant kernel (SCC)
+    peak = fp64_peak_tflops(torch, dev)
+    flops = scc_flops(off, z, res.iterations.astype(np.float64), nao_z, nsh_z)
+    scc_s = statistics.mean(scc_ms) / 1e3
+    achieved = flops / scc_s / 1e12
+    roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": read_traffic(),
+                "kernel": "scc_kernel (FP64)",
+                "peak_source": "cuBLAS FP64 DGEMM 8192^3 burst measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
+                "work": "sum over molecules of iterations*(12N^3+2N^2+2nsh^2)+14N^3 (algorithmic FLOPs)"}
+
+    # ---- end to end through the public C ABI with host buffers
+    e2e_times = []
+    for k in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = calc.calculate_flat(off, z, xb, compute_gradient=True)
+        dt = time.perf_counter() - t0
+        if k >= args.warmup:
+            e2e_times.append(dt)
+    e2e_s = sum(e2e_times)
+    if dist:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d, d2h = rb.io_bytes()
+    dE = float(np.max(np.abs(r.energy - res.energy)))
+    e2e = {"value": args.nmol * world * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(d2h), "call": "gfn1_batch_energy_gradient (host buffers)",
+           "max_abs_dE_vs_resident": dE}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(off, z, xb)
+    if rank == 0:
+        cfg = workload_config(args.nmol, off[-1], naos)
+        cfg["parallelism"] = f"one molecule per CTA; weak scaling over {world} GPU(s)"
+        cfg["kernel_ms"] = {"setup": statistics.mean(setup_ms), "scc": statistics.mean(scc_ms),
+                            "grad": statistics.mean(grad_ms)}
+        cfg["scc_iterations_mean"] = float(res.iterations.mean())
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded clusters)",
+               "config": cfg, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+               "gpu_launches": int(rb.launches * args.steps), "clocks": clk.summary()}
+        print(json.dumps(out), flush=True)
+    rb.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -155,6 +155,7 @@ int gfn1_kind(int z) {  // src/basis.rs:295-302
   return 0;
 }
 
+// Grow-only device buffer.
 template <class T>
 struct DevBuf {
   T* p = nullptr;
@@ -176,7 +177,32 @@ struct DevBuf {
   }
 };
 
+// Grow-only pinned host buffer.
+struct HostBuf {
+  unsigned char* p = nullptr;
+  size_t n = 0;
+  bool ensure(size_t bytes) {
+    if (bytes <= n && p) return true;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    n = 0;
+    if (cudaHostAlloc((void**)&p, std::max<size_t>(bytes, 256), cudaHostAllocDefault) != cudaSuccess) return false;
+    n = std::max<size_t>(bytes, 256);
+    return true;
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
 }  // namespace
+
+
+struct gfn1_batch;
 
 struct gfn1_engine {
   int device = 0;
@@ -191,6 +217,7 @@ struct gfn1_engine {
   double* d_pair = nullptr;
   double* d_c6 = nullptr;
   cudaStream_t stream = nullptr;
+  gfn1_batch* oneshot = nullptr;  // reused by gfn1_batch_energy_gradient / gfn1_run
   Model model() const {
     Model m;
     m.elem = d_elem;
@@ -201,6 +228,13 @@ struct gfn1_engine {
   }
 };
 
+// Layout of the per-batch input blob (one host->device copy) and output blob
+// (one device->host copy); byte offsets, 256-byte aligned.
+struct BlobLayout {
+  size_t atom_off, shell_off, ao_off, mat_off, gam_off, pair_off, order, status0, z, charge, xyz, init_q, in_bytes;
+  size_t terms, grad, shell_q, atom_q, dipole, fermi, iterations, status, out_bytes;
+};
+
 struct gfn1_batch {
   gfn1_engine* eng = nullptr;
   int nmol = 0;
@@ -208,30 +242,38 @@ struct gfn1_batch {
   int max_nat = 0, max_nsh = 0, max_n = 0, cap = 0, n_cta = 0;
   long long ws_stride = 0;
   gfn1_options opt;
-  std::vector<int> h_status;
-  std::vector<int> h_atom_off;
-  std::vector<int> h_shell_off;
   bool has_init_q = false;
-  DevBuf<int> atom_off, shell_off, ao_off, order, z, status, iterations, queue;
-  DevBuf<long long> mat_off, gam_off, pair_off;
-  DevBuf<double> xyz, charge, init_q, S, H0, P, W, ws, gam, pairbuf, cn, shell_q, shell_pot, atom_q, se, terms,
-      grad, grad_classic, dipole, fermi;
+  bool profiling = false;
+  BlobLayout lay;
+  HostBuf h_in, h_out;               // pinned staging
+  DevBuf<unsigned char> d_in, d_out; // device blobs
+  DevBuf<double> S, H0, P, W, ws, gam, pairbuf, cn, shell_pot, se, grad_classic;
+  DevBuf<int> queue;
+  DevBuf<unsigned long long> stage;
+  template <class T>
+  T* din(size_t off) const { return (T*)(d_in.p + off); }
+  template <class T>
+  T* dout(size_t off) const { return (T*)(d_out.p + off); }
+  template <class T>
+  T* hin(size_t off) const { return (T*)(h_in.p + off); }
+  template <class T>
+  T* hout(size_t off) const { return (T*)(h_out.p + off); }
   Batch dev() const {
     Batch B;
     std::memset(&B, 0, sizeof B);
     B.nmol = nmol;
     B.max_nat = max_nat;
-    B.atom_off = atom_off.p;
-    B.shell_off = shell_off.p;
-    B.ao_off = ao_off.p;
-    B.mat_off = mat_off.p;
-    B.gam_off = gam_off.p;
-    B.pair_off = pair_off.p;
-    B.order = order.p;
-    B.z = z.p;
-    B.xyz = xyz.p;
-    B.charge = charge.p;
-    B.init_q = has_init_q ? init_q.p : nullptr;
+    B.atom_off = din<int>(lay.atom_off);
+    B.shell_off = din<int>(lay.shell_off);
+    B.ao_off = din<int>(lay.ao_off);
+    B.mat_off = din<long long>(lay.mat_off);
+    B.gam_off = din<long long>(lay.gam_off);
+    B.pair_off = din<long long>(lay.pair_off);
+    B.order = din<int>(lay.order);
+    B.z = din<int>(lay.z);
+    B.xyz = din<double>(lay.xyz);
+    B.charge = din<double>(lay.charge);
+    B.init_q = has_init_q ? din<double>(lay.init_q) : nullptr;
     B.S = S.p;
     B.H0 = H0.p;
     B.P = P.p;
@@ -244,19 +286,29 @@ struct gfn1_batch {
     B.gam = gam.p;
     B.pairbuf = pairbuf.p;
     B.cn = cn.p;
-    B.shell_q = shell_q.p;
+    B.shell_q = dout<double>(lay.shell_q);
     B.shell_pot = shell_pot.p;
-    B.atom_q = atom_q.p;
+    B.atom_q = dout<double>(lay.atom_q);
     B.se = se.p;
-    B.terms = terms.p;
-    B.grad = grad.p;
+    B.terms = dout<double>(lay.terms);
+    B.grad = dout<double>(lay.grad);
     B.grad_classic = grad_classic.p;
-    B.dipole = dipole.p;
-    B.fermi = fermi.p;
-    B.iterations = iterations.p;
-    B.status = status.p;
+    B.dipole = dout<double>(lay.dipole);
+    B.fermi = dout<double>(lay.fermi);
+    B.iterations = dout<int>(lay.iterations);
+    B.status = dout<int>(lay.status);
     B.queue = queue.p;
+    B.stage_cycles = profiling ? stage.p : nullptr;
     return B;
+  }
+  void release() {
+    h_in.release();
+    h_out.release();
+    d_in.release();
+    d_out.release();
+    for (DevBuf<double>* d : {&S, &H0, &P, &W, &ws, &gam, &pairbuf, &cn, &shell_pot, &se, &grad_classic}) d->release();
+    queue.release();
+    stage.release();
   }
 };
 
@@ -451,13 +503,254 @@ void fill_default(gfn1_options* o) {
   o->compute_gradient = 1;
 }
 
-template <class T>
-int upload(gfn1_engine* eng, DevBuf<T>& buf, const T* host, size_t n, cudaStream_t s) {
-  if (!buf.ensure(n)) return fail(eng, GFN1_E_DEVICE, "device allocation failed");
-  if (n == 0) return GFN1_OK;
-  cudaError_t e = cudaMemcpyAsync(buf.p, host, n * sizeof(T), cudaMemcpyHostToDevice, s);
-  if (e != cudaSuccess) return cuda_fail(eng, e, "host to device copy");
+}  // namespace
+
+
+namespace {
+
+// Fills the topology part of a batch (sizes, offsets, order, element check,
+// electron count) into the pinned input blob and grows every buffer.  Buffers
+// are never shrunk, so a reused batch allocates only when a larger batch comes.
+int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t* z, const double* charge,
+            const gfn1_options* opt, std::string& first_err, int& worst) {
+  gfn1_engine* eng = b->eng;
+  gfn1_options o;
+  if (opt) o = *opt;
+  else fill_default(&o);
+  if (o.max_scc < 1) return fail(eng, GFN1_E_INVALID_INPUT, "max_scc must be at least 1");
+  if (atom_offsets[0] != 0) return fail(eng, GFN1_E_INVALID_INPUT, "atom_offsets[0] must be 0");
+  for (int m = 0; m < nmol; ++m)
+    if (atom_offsets[m + 1] < atom_offsets[m]) return fail(eng, GFN1_E_INVALID_INPUT, "atom_offsets must be non-decreasing");
+  b->nmol = nmol;
+  b->opt = o;
+  b->has_init_q = false;
+  const long long natoms = atom_offsets[nmol];
+  b->natoms = natoms;
+  b->max_nat = b->max_nsh = b->max_n = 0;
+  // sizes first (for the blob layout)
+  std::vector<int> nsh_m(nmol), n_m(nmol), st_m(nmol, GFN1_OK);
+  std::vector<double> nref_m(nmol, 0.0);
+  long long nshells = 0, naos = 0, mat_total = 0, gam_total = 0, pair_total = 0;
+  worst = GFN1_OK;
+  for (int m = 0; m < nmol; ++m) {
+    const int a0 = atom_offsets[m], a1 = atom_offsets[m + 1];
+    int n = 0, s = 0, st = GFN1_OK;
+    if (a1 <= a0) {
+      st = GFN1_E_INVALID_INPUT;
+      if (first_err.empty()) first_err = "molecule " + std::to_string(m) + ": cannot run GFN1 SCC for an empty basis";
+    }
+    for (int a = a0; a < a1; ++a) {
+      const int zz = z[a];
+      if (zz < 1 || zz > kMaxZ) {
+        st = GFN1_E_MISSING_ELEMENT;
+        if (first_err.empty()) first_err = "missing GFN1 parameter block for Z=" + std::to_string(zz);
+        continue;
+      }
+      if (!eng->device_ok[zz]) {
+        st = std::max(st, (int)GFN1_E_UNSUPPORTED);
+        if (first_err.empty()) first_err = "element Z=" + std::to_string(zz) + " has d/f shells; outside the device path";
+        continue;
+      }
+      n += eng->elem[zz].nao;
+      s += eng->elem[zz].nsh;
+      nref_m[m] += eng->refocc_total[zz];
+    }
+    const double ch = charge ? charge[m] : 0.0;
+    const double nelec = nref_m[m] - ch;  // src/electronic.rs:491-510
+    if (st == GFN1_OK && (!std::isfinite(nelec) || nelec < -1e-8 || nelec > 2.0 * n + 1e-8)) {
+      st = GFN1_E_INVALID_INPUT;
+      if (first_err.empty()) first_err = "molecule " + std::to_string(m) + ": invalid electron count";
+    }
+    st_m[m] = st;
+    worst = std::max(worst, st);
+    nsh_m[m] = s;
+    n_m[m] = n;
+    nshells += s;
+    naos += n;
+    mat_total += (((long long)n * n + 31) / 32) * 32;
+    gam_total += (long long)s * s;
+    pair_total += (long long)(a1 - a0) * (a1 - a0 - 1) / 2;
+    b->max_nat = std::max(b->max_nat, a1 - a0);
+    b->max_nsh = std::max(b->max_nsh, s);
+    b->max_n = std::max(b->max_n, n);
+  }
+  b->nshells = nshells;
+  b->naos = naos;
+  b->mat_total = mat_total;
+  b->gam_total = gam_total;
+  b->pair_total = pair_total;
+  // blob layout
+  BlobLayout& L = b->lay;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t at = off;
+    off = align256(off + bytes);
+    return at;
+  };
+  L.atom_off = take(sizeof(int) * (nmol + 1));
+  L.shell_off = take(sizeof(int) * (nmol + 1));
+  L.ao_off = take(sizeof(int) * (nmol + 1));
+  L.mat_off = take(sizeof(long long) * (nmol + 1));
+  L.gam_off = take(sizeof(long long) * (nmol + 1));
+  L.pair_off = take(sizeof(long long) * (nmol + 1));
+  L.order = take(sizeof(int) * nmol);
+  L.status0 = take(sizeof(int) * nmol);
+  L.z = take(sizeof(int) * std::max<long long>(natoms, 1));
+  L.charge = take(sizeof(double) * nmol);
+  L.xyz = take(sizeof(double) * 3 * std::max<long long>(natoms, 1));
+  L.init_q = take(sizeof(double) * std::max<long long>(nshells, 1));
+  L.in_bytes = off;
+  off = 0;
+  L.terms = take(sizeof(double) * kTerms * nmol);
+  L.grad = take(sizeof(double) * 3 * std::max<long long>(natoms, 1));
+  L.shell_q = take(sizeof(double) * std::max<long long>(nshells, 1));
+  L.atom_q = take(sizeof(double) * std::max<long long>(natoms, 1));
+  L.dipole = take(sizeof(double) * 3 * nmol);
+  L.fermi = take(sizeof(double) * nmol);
+  L.iterations = take(sizeof(int) * nmol);
+  L.status = take(sizeof(int) * nmol);
+  L.out_bytes = off;
+  if (!b->h_in.ensure(L.in_bytes) || !b->h_out.ensure(L.out_bytes))
+    return fail(eng, GFN1_E_DEVICE, "pinned host allocation failed");
+  int* h_atom = b->hin<int>(L.atom_off);
+  int* h_shell = b->hin<int>(L.shell_off);
+  int* h_ao = b->hin<int>(L.ao_off);
+  long long* h_mat = b->hin<long long>(L.mat_off);
+  long long* h_gam = b->hin<long long>(L.gam_off);
+  long long* h_pair = b->hin<long long>(L.pair_off);
+  int* h_order = b->hin<int>(L.order);
+  int* h_st = b->hin<int>(L.status0);
+  int* h_z = b->hin<int>(L.z);
+  double* h_ch = b->hin<double>(L.charge);
+  h_atom[0] = h_shell[0] = h_ao[0] = 0;
+  h_mat[0] = h_gam[0] = h_pair[0] = 0;
+  for (int m = 0; m < nmol; ++m) {
+    const int a0 = atom_offsets[m], a1 = atom_offsets[m + 1];
+    h_atom[m + 1] = a1;
+    h_shell[m + 1] = h_shell[m] + nsh_m[m];
+    h_ao[m + 1] = h_ao[m] + n_m[m];
+    h_mat[m + 1] = h_mat[m] + (((long long)n_m[m] * n_m[m] + 31) / 32) * 32;
+    h_gam[m + 1] = h_gam[m] + (long long)nsh_m[m] * nsh_m[m];
+    h_pair[m + 1] = h_pair[m] + (long long)(a1 - a0) * (a1 - a0 - 1) / 2;
+    h_st[m] = st_m[m];
+    h_ch[m] = charge ? charge[m] : 0.0;
+    for (int a = a0; a < a1; ++a) {
+      const int zz = z[a];
+      h_z[a] = (zz >= 1 && zz <= kMaxZ && eng->device_ok[zz]) ? zz : 1;  // rejected molecules are skipped
+    }
+  }
+  // most expensive molecules first (cost ~ N^3)
+  for (int m = 0; m < nmol; ++m) h_order[m] = m;
+  std::stable_sort(h_order, h_order + nmol, [&](int x, int y) { return n_m[x] > n_m[y]; });
+  b->cap = std::max(1, std::min(std::max(o.scc_broyden_size, 2), o.max_scc));
+  b->ws_stride = scc_workspace_doubles(b->max_n, b->max_nsh, b->cap, b->max_nat);
+  const int per_sm = 2;
+  b->n_cta = std::max(1, std::min(nmol, per_sm * eng->num_sms));
+  bool ok = b->d_in.ensure(L.in_bytes) && b->d_out.ensure(L.out_bytes) && b->queue.ensure(4) &&
+            b->stage.ensure(kStages) && b->S.ensure(mat_total) && b->H0.ensure(mat_total) && b->P.ensure(mat_total) &&
+            b->W.ensure(mat_total) && b->ws.ensure((size_t)b->ws_stride * b->n_cta) && b->gam.ensure(gam_total) &&
+            b->pairbuf.ensure(8 * std::max<long long>(pair_total, 1)) && b->cn.ensure(natoms) &&
+            b->shell_pot.ensure(nshells) && b->se.ensure(nshells) && b->grad_classic.ensure(3 * natoms);
+  if (!ok) return fail(eng, GFN1_E_DEVICE, "device allocation failed for the batch workspace");
   return GFN1_OK;
+}
+
+// Copies the whole input blob (topology, coordinates, optional initial charges).
+int upload_inputs(gfn1_batch* b, cudaStream_t st) {
+  cudaError_t e = cudaMemcpyAsync(b->d_in.p, b->h_in.p, b->lay.in_bytes, cudaMemcpyHostToDevice, st);
+  return e == cudaSuccess ? GFN1_OK : cuda_fail(b->eng, e, "host to device copy");
+}
+
+int launch_stage(gfn1_batch* b, int stage, cudaStream_t st) {
+  gfn1_engine* eng = b->eng;
+  const Batch B = b->dev();
+  const Model M = eng->model();
+  const int nt = 256;
+  cudaError_t e = cudaSuccess;
+  if (stage == 0) {
+    // reset status from the host-validated copy and the work counter
+    if ((e = cudaMemcpyAsync(B.status, b->din<int>(b->lay.status0), sizeof(int) * b->nmol, cudaMemcpyDeviceToDevice,
+                             st)) != cudaSuccess ||
+        (e = cudaMemsetAsync(b->queue.p, 0, sizeof(int) * 4, st)) != cudaSuccess)
+      return cuda_fail(eng, e, "batch reset");
+    if (b->profiling && (e = cudaMemsetAsync(b->stage.p, 0, sizeof(unsigned long long) * kStages, st)) != cudaSuccess)
+      return cuda_fail(eng, e, "batch reset");
+    const size_t smem = sizeof(double) * (16 * (size_t)b->max_nat + 32) +
+                        sizeof(int) * (3 * (size_t)b->max_nat + 2 + 2 * (size_t)b->max_nsh);
+    if (smem > 48 * 1024) cudaFuncSetAttribute(setup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    setup_kernel<<<b->nmol, nt, smem, st>>>(B, M, b->opt.enable_dispersion, b->max_nsh);
+  } else if (stage == 1) {
+    SccOptions so;
+    so.max_scc = b->opt.max_scc;
+    so.broyden = b->opt.scc_broyden;
+    so.broyden_size = b->opt.scc_broyden_size;
+    so.enable_dispersion = b->opt.enable_dispersion;
+    so.energy_tol = b->opt.energy_tolerance;
+    so.charge_tol = b->opt.charge_tolerance;
+    so.mixing = b->opt.mixing;
+    so.etemp = b->opt.electronic_temperature;
+    const size_t smem = sizeof(int) * (3 * (size_t)b->max_nsh + b->max_n + b->max_nat + 1);
+    if (smem > 48 * 1024) cudaFuncSetAttribute(scc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    scc_kernel<<<b->n_cta, nt, smem, st>>>(B, M, so, b->max_nsh, b->max_n);
+  } else if (stage == 2) {
+    if (!b->opt.compute_gradient) return GFN1_OK;
+    const size_t smem = sizeof(double) * 7 * (size_t)b->max_nat + sizeof(int) * (3 * (size_t)b->max_nat + 2);
+    if (smem > 48 * 1024) cudaFuncSetAttribute(grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    grad_kernel<<<b->nmol, nt, smem, st>>>(B, M);
+  } else {
+    return fail(eng, GFN1_E_INVALID_INPUT, "unknown stage");
+  }
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(eng, e, "kernel launch");
+  return GFN1_OK;
+}
+
+// Synchronises `st`, scatters the output blob into the caller's buffers and
+// turns per-molecule statuses into the call's return code.
+int finish(gfn1_batch* b, const gfn1_outputs* out, cudaStream_t st) {
+  gfn1_engine* eng = b->eng;
+  const BlobLayout& L = b->lay;
+  cudaError_t e = cudaMemcpyAsync(b->h_out.p, b->d_out.p, L.out_bytes, cudaMemcpyDeviceToHost, st);
+  if (e != cudaSuccess) return cuda_fail(eng, e, "device to host copy");
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(eng, e, "batch execution");
+  const double* terms = b->hout<double>(L.terms);
+  const int* status = b->hout<int>(L.status);
+  if (out) {
+    const int nmol = b->nmol;
+    if (out->energy)
+      for (int m = 0; m < nmol; ++m) out->energy[m] = terms[(size_t)kTerms * m];
+    if (out->terms) std::memcpy(out->terms, terms, sizeof(double) * kTerms * nmol);
+    if (out->gradient && b->opt.compute_gradient)
+      std::memcpy(out->gradient, b->hout<double>(L.grad), sizeof(double) * 3 * b->natoms);
+    if (out->shell_charges) std::memcpy(out->shell_charges, b->hout<double>(L.shell_q), sizeof(double) * b->nshells);
+    if (out->atomic_charges) std::memcpy(out->atomic_charges, b->hout<double>(L.atom_q), sizeof(double) * b->natoms);
+    if (out->dipole) std::memcpy(out->dipole, b->hout<double>(L.dipole), sizeof(double) * 3 * nmol);
+    if (out->fermi_level) std::memcpy(out->fermi_level, b->hout<double>(L.fermi), sizeof(double) * nmol);
+    if (out->iterations) std::memcpy(out->iterations, b->hout<int>(L.iterations), sizeof(int) * nmol);
+    if (out->status) std::memcpy(out->status, status, sizeof(int) * nmol);
+  }
+  int worst = GFN1_OK, first = -1;
+  for (int m = 0; m < b->nmol; ++m) {
+    if (status[m] > worst) worst = status[m];
+    if (status[m] != GFN1_OK && first < 0) first = m;
+  }
+  if (worst != GFN1_OK) {
+    std::string msg = "molecule " + std::to_string(first) + ": ";
+    switch (status[first]) {
+      case GFN1_E_SCC_NOT_CONVERGED: msg += "GFN1 SCC did not converge"; break;
+      case GFN1_E_INVALID_INPUT: msg += "invalid input (empty molecule, electron count or non-positive-definite overlap)"; break;
+      case GFN1_E_UNSUPPORTED: msg += "element outside the device path (d/f shells)"; break;
+      case GFN1_E_MISSING_ELEMENT: msg += "missing GFN1 parameter block"; break;
+      default: msg += "error " + std::to_string(status[first]);
+    }
+    return fail(eng, worst, msg);
+  }
+  return GFN1_OK;
+}
+
+bool finite_all(const double* x, long long n) {
+  for (long long i = 0; i < n; ++i)
+    if (!std::isfinite(x[i])) return false;
+  return true;
 }
 
 }  // namespace
@@ -517,6 +810,7 @@ int gfn1_engine_create(const char* param_spec, int device, gfn1_engine** out) {
 
 void gfn1_engine_destroy(gfn1_engine* eng) {
   if (!eng) return;
+  if (eng->oneshot) gfn1_batch_destroy(eng->oneshot);
   if (eng->d_elem) cudaFree(eng->d_elem);
   if (eng->d_pair) cudaFree(eng->d_pair);
   if (eng->d_c6) cudaFree(eng->d_c6);
@@ -544,113 +838,22 @@ int gfn1_batch_create(gfn1_engine* eng, int nmol, const int32_t* atom_offsets, c
                       const gfn1_options* opt, gfn1_batch** out) {
   if (!eng || !out || nmol < 1 || !atom_offsets || !z) return fail(eng, GFN1_E_INVALID_INPUT, "invalid batch arguments");
   *out = nullptr;
-  gfn1_options o;
-  if (opt) o = *opt;
-  else fill_default(&o);
-  if (o.max_scc < 1) return fail(eng, GFN1_E_INVALID_INPUT, "max_scc must be at least 1");
   cudaSetDevice(eng->device);
   gfn1_batch* b = new gfn1_batch();
   b->eng = eng;
-  b->nmol = nmol;
-  b->opt = o;
-  const long long natoms = atom_offsets[nmol];
-  b->natoms = natoms;
-  std::vector<int> shell_off(nmol + 1, 0), ao_off(nmol + 1, 0);
-  std::vector<long long> mat_off(nmol + 1, 0), gam_off(nmol + 1, 0), pair_off(nmol + 1, 0);
-  std::vector<int> status(nmol, GFN1_OK), zi(std::max<long long>(natoms, 1));
-  std::vector<double> ch(nmol, 0.0);
+  const char* prof = std::getenv("GFN1_PROFILE");
+  b->profiling = prof && *prof && *prof != '0';
   std::string first_err;
   int worst = GFN1_OK;
-  for (int m = 0; m < nmol; ++m) {
-    const int a0 = atom_offsets[m], a1 = atom_offsets[m + 1];
-    int n = 0, s = 0, st = GFN1_OK;
-    double nref = 0.0;
-    if (a1 <= a0) {
-      st = GFN1_E_INVALID_INPUT;
-      if (first_err.empty()) first_err = "molecule " + std::to_string(m) + ": cannot run GFN1 SCC for an empty basis";
-    }
-    for (int a = a0; a < a1; ++a) {
-      const int zz = z[a];
-      zi[a] = zz;
-      if (zz < 1 || zz > kMaxZ) {
-        st = GFN1_E_MISSING_ELEMENT;
-        if (first_err.empty()) first_err = "missing GFN1 parameter block for Z=" + std::to_string(zz);
-        zi[a] = 1;
-        continue;
-      }
-      if (!eng->device_ok[zz]) {
-        st = GFN1_E_UNSUPPORTED;
-        if (first_err.empty()) first_err = "element Z=" + std::to_string(zz) + " has d/f shells; outside the device path";
-        zi[a] = 1;
-        continue;
-      }
-      n += eng->elem[zz].nao;
-      s += eng->elem[zz].nsh;
-      nref += eng->refocc_total[zz];
-    }
-    ch[m] = charge ? charge[m] : 0.0;
-    const double nelec = nref - ch[m];  // src/electronic.rs:491-510
-    if (st == GFN1_OK && (!std::isfinite(nelec) || nelec < -1e-8 || nelec > 2.0 * n + 1e-8)) {
-      st = GFN1_E_INVALID_INPUT;
-      if (first_err.empty()) first_err = "molecule " + std::to_string(m) + ": invalid electron count";
-    }
-    status[m] = st;
-    worst = std::max(worst, st);
-    shell_off[m + 1] = shell_off[m] + s;
-    ao_off[m + 1] = ao_off[m] + n;
-    mat_off[m + 1] = mat_off[m] + (((long long)n * n + 31) / 32) * 32;
-    gam_off[m + 1] = gam_off[m] + (long long)s * s;
-    pair_off[m + 1] = pair_off[m] + (long long)(a1 - a0) * (a1 - a0 - 1) / 2;
-    b->max_nat = std::max(b->max_nat, a1 - a0);
-    b->max_nsh = std::max(b->max_nsh, s);
-    b->max_n = std::max(b->max_n, n);
+  int rc = prepare(b, nmol, atom_offsets, z, charge, opt, first_err, worst);
+  if (rc == GFN1_OK) rc = upload_inputs(b, eng->stream);
+  if (rc == GFN1_OK) {
+    cudaError_t e = cudaStreamSynchronize(eng->stream);
+    if (e != cudaSuccess) rc = cuda_fail(eng, e, "batch upload");
   }
-  b->nshells = shell_off[nmol];
-  b->naos = ao_off[nmol];
-  b->mat_total = mat_off[nmol];
-  b->gam_total = gam_off[nmol];
-  b->pair_total = pair_off[nmol];
-  b->h_status = status;
-  b->h_atom_off.assign(atom_offsets, atom_offsets + nmol + 1);
-  b->h_shell_off = shell_off;
-  b->cap = std::max(1, std::min(std::max(o.scc_broyden_size, 2), o.max_scc));
-  b->ws_stride = scc_workspace_doubles(b->max_n, b->max_nsh, b->cap, b->max_nat);
-  // most expensive molecules first (cost ~ N^3)
-  std::vector<int> order(nmol);
-  for (int m = 0; m < nmol; ++m) order[m] = m;
-  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-    return (ao_off[x + 1] - ao_off[x]) > (ao_off[y + 1] - ao_off[y]);
-  });
-  const int per_sm = 2;
-  b->n_cta = std::max(1, std::min(nmol, per_sm * eng->num_sms));
-  cudaStream_t st = eng->stream;
-  int rc;
-  if ((rc = upload(eng, b->atom_off, atom_offsets, nmol + 1, st)) ||
-      (rc = upload(eng, b->shell_off, shell_off.data(), nmol + 1, st)) ||
-      (rc = upload(eng, b->ao_off, ao_off.data(), nmol + 1, st)) ||
-      (rc = upload(eng, b->mat_off, mat_off.data(), nmol + 1, st)) ||
-      (rc = upload(eng, b->gam_off, gam_off.data(), nmol + 1, st)) ||
-      (rc = upload(eng, b->pair_off, pair_off.data(), nmol + 1, st)) ||
-      (rc = upload(eng, b->order, order.data(), nmol, st)) ||
-      (rc = upload(eng, b->z, zi.data(), (size_t)natoms, st)) || (rc = upload(eng, b->charge, ch.data(), nmol, st))) {
+  if (rc != GFN1_OK) {
     gfn1_batch_destroy(b);
     return rc;
-  }
-  bool ok = b->xyz.ensure(3 * natoms) && b->status.ensure(nmol) && b->iterations.ensure(nmol) && b->queue.ensure(4) &&
-            b->S.ensure(b->mat_total) && b->H0.ensure(b->mat_total) && b->P.ensure(b->mat_total) &&
-            b->W.ensure(b->mat_total) && b->ws.ensure((size_t)b->ws_stride * b->n_cta) && b->gam.ensure(b->gam_total) &&
-            b->pairbuf.ensure(8 * std::max<long long>(b->pair_total, 1)) && b->cn.ensure(natoms) &&
-            b->shell_q.ensure(b->nshells) && b->shell_pot.ensure(b->nshells) && b->atom_q.ensure(natoms) &&
-            b->se.ensure(b->nshells) && b->terms.ensure((size_t)kTerms * nmol) && b->grad.ensure(3 * natoms) &&
-            b->grad_classic.ensure(3 * natoms) && b->dipole.ensure(3 * nmol) && b->fermi.ensure(nmol);
-  if (!ok) {
-    gfn1_batch_destroy(b);
-    return fail(eng, GFN1_E_DEVICE, "device allocation failed for the batch workspace");
-  }
-  cudaError_t e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) {
-    gfn1_batch_destroy(b);
-    return cuda_fail(eng, e, "batch upload");
   }
   *out = b;
   if (worst != GFN1_OK) fail(eng, worst, first_err);
@@ -659,28 +862,16 @@ int gfn1_batch_create(gfn1_engine* eng, int nmol, const int32_t* atom_offsets, c
 
 void gfn1_batch_destroy(gfn1_batch* b) {
   if (!b) return;
-  b->atom_off.release();
-  b->shell_off.release();
-  b->ao_off.release();
-  b->order.release();
-  b->z.release();
-  b->status.release();
-  b->iterations.release();
-  b->queue.release();
-  b->mat_off.release();
-  b->gam_off.release();
-  b->pair_off.release();
-  for (DevBuf<double>* d : {&b->xyz, &b->charge, &b->init_q, &b->S, &b->H0, &b->P, &b->W, &b->ws, &b->gam,
-                            &b->pairbuf, &b->cn, &b->shell_q, &b->shell_pot, &b->atom_q, &b->se, &b->terms, &b->grad,
-                            &b->grad_classic, &b->dipole, &b->fermi})
-    d->release();
+  b->release();
   delete b;
 }
 
 int gfn1_batch_set_positions(gfn1_batch* b, const double* xyz, int on_device) {
   if (!b || !xyz) return fail(b ? b->eng : nullptr, GFN1_E_INVALID_INPUT, "invalid arguments");
-  cudaError_t e = cudaMemcpyAsync(b->xyz.p, xyz, sizeof(double) * 3 * b->natoms,
+  cudaError_t e = cudaMemcpyAsync(b->din<double>(b->lay.xyz), xyz, sizeof(double) * 3 * b->natoms,
                                   on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, b->eng->stream);
+  if (e != cudaSuccess) return cuda_fail(b->eng, e, "set positions");
+  if (!on_device) e = cudaStreamSynchronize(b->eng->stream);  // the caller may reuse its buffer
   if (e != cudaSuccess) return cuda_fail(b->eng, e, "set positions");
   return GFN1_OK;
 }
@@ -691,62 +882,44 @@ int gfn1_batch_set_initial_charges(gfn1_batch* b, const double* q, int on_device
     b->has_init_q = false;
     return GFN1_OK;
   }
-  if (!b->init_q.ensure(b->nshells)) return fail(b->eng, GFN1_E_DEVICE, "device allocation failed");
-  cudaError_t e = cudaMemcpyAsync(b->init_q.p, q, sizeof(double) * b->nshells,
+  cudaError_t e = cudaMemcpyAsync(b->din<double>(b->lay.init_q), q, sizeof(double) * b->nshells,
                                   on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, b->eng->stream);
+  if (e == cudaSuccess && !on_device) e = cudaStreamSynchronize(b->eng->stream);
   if (e != cudaSuccess) return cuda_fail(b->eng, e, "set initial charges");
   b->has_init_q = true;
   return GFN1_OK;
 }
 
-int gfn1_batch_launch(gfn1_batch* b, void* stream) {
+int gfn1_batch_launch_stage(gfn1_batch* b, int stage, void* stream) {
   if (!b) return fail(nullptr, GFN1_E_INVALID_INPUT, "null batch");
-  gfn1_engine* eng = b->eng;
-  cudaStream_t st = stream ? (cudaStream_t)stream : eng->stream;
-  if (stream) {  // order the engine-stream uploads before work on the caller's stream
+  cudaStream_t st = stream ? (cudaStream_t)stream : b->eng->stream;
+  if (stream && stage <= 0) {  // order earlier engine-stream copies before the caller's stream
     cudaEvent_t ev;
     cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
-    cudaEventRecord(ev, eng->stream);
+    cudaEventRecord(ev, b->eng->stream);
     cudaStreamWaitEvent(st, ev, 0);
     cudaEventDestroy(ev);
   }
-  const Batch B = b->dev();
-  const Model M = eng->model();
-  cudaError_t e;
-  if ((e = cudaMemcpyAsync(b->status.p, b->h_status.data(), sizeof(int) * b->nmol, cudaMemcpyHostToDevice, st)) !=
-          cudaSuccess ||
-      (e = cudaMemsetAsync(b->queue.p, 0, sizeof(int) * 4, st)) != cudaSuccess)
-    return cuda_fail(eng, e, "batch reset");
-  const int nt = 256;
-  const size_t smem_setup = sizeof(double) * (16 * (size_t)b->max_nat + 32) +
-                            sizeof(int) * (3 * (size_t)b->max_nat + 2 + 2 * (size_t)b->max_nsh);
-  const size_t smem_scc = sizeof(int) * (3 * (size_t)b->max_nsh + b->max_n + b->max_nat + 1);
-  const size_t smem_grad = sizeof(double) * 7 * (size_t)b->max_nat + sizeof(int) * (3 * (size_t)b->max_nat + 2);
-  if (smem_setup > 48 * 1024) cudaFuncSetAttribute(setup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_setup);
-  if (smem_scc > 48 * 1024) cudaFuncSetAttribute(scc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_scc);
-  if (smem_grad > 48 * 1024) cudaFuncSetAttribute(grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_grad);
-  setup_kernel<<<b->nmol, nt, smem_setup, st>>>(B, M, b->opt.enable_dispersion, b->max_nsh);
-  SccOptions so;
-  so.max_scc = b->opt.max_scc;
-  so.broyden = b->opt.scc_broyden;
-  so.broyden_size = b->opt.scc_broyden_size;
-  so.enable_dispersion = b->opt.enable_dispersion;
-  so.energy_tol = b->opt.energy_tolerance;
-  so.charge_tol = b->opt.charge_tolerance;
-  so.mixing = b->opt.mixing;
-  so.etemp = b->opt.electronic_temperature;
-  scc_kernel<<<b->n_cta, nt, smem_scc, st>>>(B, M, so, b->max_nsh, b->max_n);
-  if (b->opt.compute_gradient) grad_kernel<<<b->nmol, nt, smem_grad, st>>>(B, M);
-  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(eng, e, "kernel launch");
-  if (stream) {  // later engine-stream copies wait for the caller's stream
+  if (stage < 0) {
+    for (int s = 0; s < 3; ++s) {
+      int rc = launch_stage(b, s, st);
+      if (rc != GFN1_OK) return rc;
+    }
+  } else {
+    int rc = launch_stage(b, stage, st);
+    if (rc != GFN1_OK) return rc;
+  }
+  if (stream && (stage < 0 || stage == 2)) {  // later engine-stream copies wait for the caller's stream
     cudaEvent_t ev;
     cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
     cudaEventRecord(ev, st);
-    cudaStreamWaitEvent(eng->stream, ev, 0);
+    cudaStreamWaitEvent(b->eng->stream, ev, 0);
     cudaEventDestroy(ev);
   }
   return GFN1_OK;
 }
+
+int gfn1_batch_launch(gfn1_batch* b, void* stream) { return gfn1_batch_launch_stage(b, -1, stream); }
 
 int gfn1_batch_info(const gfn1_batch* b, int64_t* natoms, int64_t* nshells, int64_t* naos, int32_t* launches) {
   if (!b) return fail(nullptr, GFN1_E_INVALID_INPUT, "null batch");
@@ -759,87 +932,66 @@ int gfn1_batch_info(const gfn1_batch* b, int64_t* natoms, int64_t* nshells, int6
 
 int gfn1_batch_outputs_device(gfn1_batch* b, gfn1_outputs* out) {
   if (!b || !out) return fail(nullptr, GFN1_E_INVALID_INPUT, "invalid arguments");
+  const BlobLayout& L = b->lay;
   out->energy = nullptr;  // total_free is terms[m*15 + 0]
-  out->terms = b->terms.p;
-  out->gradient = b->grad.p;
-  out->shell_charges = b->shell_q.p;
-  out->atomic_charges = b->atom_q.p;
-  out->dipole = b->dipole.p;
-  out->fermi_level = b->fermi.p;
-  out->iterations = b->iterations.p;
-  out->status = b->status.p;
+  out->terms = b->dout<double>(L.terms);
+  out->gradient = b->dout<double>(L.grad);
+  out->shell_charges = b->dout<double>(L.shell_q);
+  out->atomic_charges = b->dout<double>(L.atom_q);
+  out->dipole = b->dout<double>(L.dipole);
+  out->fermi_level = b->dout<double>(L.fermi);
+  out->iterations = b->dout<int>(L.iterations);
+  out->status = b->dout<int>(L.status);
   return GFN1_OK;
 }
 
 int gfn1_batch_download(gfn1_batch* b, const gfn1_outputs* out) {
   if (!b) return fail(nullptr, GFN1_E_INVALID_INPUT, "null batch");
-  gfn1_engine* eng = b->eng;
-  cudaStream_t st = eng->stream;
-  std::vector<double> terms((size_t)kTerms * b->nmol);
-  std::vector<int> status(b->nmol);
-  cudaError_t e;
-  if ((e = cudaMemcpyAsync(terms.data(), b->terms.p, sizeof(double) * terms.size(), cudaMemcpyDeviceToHost, st)) !=
-          cudaSuccess ||
-      (e = cudaMemcpyAsync(status.data(), b->status.p, sizeof(int) * b->nmol, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
-    return cuda_fail(eng, e, "device to host copy");
-  if (out) {
-    auto cp = [&](void* dst, const void* src, size_t bytes) {
-      if (dst && bytes && e == cudaSuccess) e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st);
-    };
-    if (b->opt.compute_gradient) cp(out->gradient, b->grad.p, sizeof(double) * 3 * b->natoms);
-    cp(out->shell_charges, b->shell_q.p, sizeof(double) * b->nshells);
-    cp(out->atomic_charges, b->atom_q.p, sizeof(double) * b->natoms);
-    cp(out->dipole, b->dipole.p, sizeof(double) * 3 * b->nmol);
-    cp(out->fermi_level, b->fermi.p, sizeof(double) * b->nmol);
-    cp(out->iterations, b->iterations.p, sizeof(int) * b->nmol);
-    if (e != cudaSuccess) return cuda_fail(eng, e, "device to host copy");
-  }
-  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(eng, e, "batch execution");
-  int worst = GFN1_OK, first = -1;
-  for (int m = 0; m < b->nmol; ++m) {
-    if (status[m] > worst) worst = status[m];
-    if (status[m] != GFN1_OK && first < 0) first = m;
-  }
-  if (out) {
-    if (out->energy)
-      for (int m = 0; m < b->nmol; ++m) out->energy[m] = terms[(size_t)kTerms * m];
-    if (out->terms) std::memcpy(out->terms, terms.data(), sizeof(double) * terms.size());
-    if (out->status) std::memcpy(out->status, status.data(), sizeof(int) * b->nmol);
-  }
-  if (worst != GFN1_OK) {
-    std::string msg = "molecule " + std::to_string(first) + ": ";
-    switch (status[first]) {
-      case GFN1_E_SCC_NOT_CONVERGED: msg += "GFN1 SCC did not converge"; break;
-      case GFN1_E_INVALID_INPUT: msg += "invalid input (empty molecule, electron count or non-positive-definite overlap)"; break;
-      case GFN1_E_UNSUPPORTED: msg += "element outside the device path"; break;
-      case GFN1_E_MISSING_ELEMENT: msg += "missing GFN1 parameter block"; break;
-      default: msg += "error " + std::to_string(status[first]);
-    }
-    return fail(eng, worst, msg);
-  }
+  return finish(b, out, b->eng->stream);
+}
+
+int gfn1_batch_stage_cycles(const gfn1_batch* b, uint64_t* cycles, int n) {
+  if (!b || !cycles) return fail(nullptr, GFN1_E_INVALID_INPUT, "invalid arguments");
+  if (!b->profiling) return fail(b->eng, GFN1_E_INVALID_INPUT, "stage profiling is off (set GFN1_PROFILE=1)");
+  const int k = std::min(n, (int)kStages);
+  cudaError_t e = cudaMemcpy(cycles, b->stage.p, sizeof(uint64_t) * k, cudaMemcpyDeviceToHost);
+  return e == cudaSuccess ? GFN1_OK : cuda_fail(b->eng, e, "stage cycles");
+}
+
+int gfn1_batch_io_bytes(const gfn1_batch* b, int64_t* h2d, int64_t* d2h) {
+  if (!b) return fail(nullptr, GFN1_E_INVALID_INPUT, "null batch");
+  if (h2d) *h2d = (int64_t)b->lay.in_bytes;
+  if (d2h) *d2h = (int64_t)b->lay.out_bytes;
   return GFN1_OK;
 }
 
 int gfn1_batch_energy_gradient(gfn1_engine* eng, int nmol, const int32_t* atom_offsets, const uint8_t* z,
                                const double* xyz_bohr, const double* charge, const double* init_shell_q,
                                const gfn1_options* opt, const gfn1_outputs* out) {
-  if (!xyz_bohr) return fail(eng, GFN1_E_INVALID_INPUT, "null coordinates");
-  gfn1_batch* b = nullptr;
-  int rc = gfn1_batch_create(eng, nmol, atom_offsets, z, charge, opt, &b);
-  if (rc != GFN1_OK) return rc;
-  for (long long i = 0; i < 3 * b->natoms; ++i)
-    if (!std::isfinite(xyz_bohr[i])) {
-      gfn1_batch_destroy(b);
-      return fail(eng, GFN1_E_NAN, "non-finite coordinate");
-    }
-  if ((rc = gfn1_batch_set_positions(b, xyz_bohr, 0)) != GFN1_OK ||
-      (rc = gfn1_batch_set_initial_charges(b, init_shell_q, 0)) != GFN1_OK || (rc = gfn1_batch_launch(b, nullptr)) != GFN1_OK) {
-    gfn1_batch_destroy(b);
-    return rc;
+  if (!eng || nmol < 1 || !atom_offsets || !z || !xyz_bohr) return fail(eng, GFN1_E_INVALID_INPUT, "invalid arguments");
+  cudaSetDevice(eng->device);
+  if (!eng->oneshot) {
+    eng->oneshot = new gfn1_batch();
+    eng->oneshot->eng = eng;
   }
-  rc = gfn1_batch_download(b, out);
-  gfn1_batch_destroy(b);
-  return rc;
+  gfn1_batch* b = eng->oneshot;
+  const char* prof = std::getenv("GFN1_PROFILE");
+  b->profiling = prof && *prof && *prof != '0';
+  std::string first_err;
+  int worst = GFN1_OK;
+  int rc = prepare(b, nmol, atom_offsets, z, charge, opt, first_err, worst);
+  if (rc != GFN1_OK) return rc;
+  if (!finite_all(xyz_bohr, 3 * b->natoms)) return fail(eng, GFN1_E_NAN, "non-finite coordinate");
+  std::memcpy(b->hin<double>(b->lay.xyz), xyz_bohr, sizeof(double) * 3 * b->natoms);
+  if (init_shell_q) {
+    std::memcpy(b->hin<double>(b->lay.init_q), init_shell_q, sizeof(double) * b->nshells);
+    b->has_init_q = true;
+  }
+  cudaStream_t st = eng->stream;
+  if ((rc = upload_inputs(b, st)) != GFN1_OK) return rc;
+  for (int s = 0; s < 3; ++s)
+    if ((rc = launch_stage(b, s, st)) != GFN1_OK) return rc;
+  return finish(b, out, st);
 }
 
 int gfn1_run(gfn1_engine* eng, int nat, const uint8_t* z, const double* xyz_bohr, double charge,

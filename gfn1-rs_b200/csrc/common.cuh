@@ -101,6 +101,24 @@ struct Batch {
   int* iterations;          // [nmol]
   int* status;              // [nmol]
   int* queue;               // work counters
+  unsigned long long* stage_cycles;  // [kStages] per-stage clock totals, or null
+};
+
+// SCC stages timed when Batch::stage_cycles is set (the device counterpart of
+// the reference's GFN1_PROFILE scopes, src/electronic.rs:1448, :2089-2157).
+enum Stage : int {
+  kStPrologue = 0,  // Cholesky, L^-1, H0'
+  kStFock,          // shell potential + F'
+  kStTridiag,       // Householder reduction
+  kStEigval,        // bisection
+  kStFermi,         // occupations
+  kStInvIter,       // inverse iteration
+  kStBackTr,        // back-transformation
+  kStPop,           // C, D, Mulliken populations
+  kStEnergy,        // output charges, energies, convergence test
+  kStMix,           // Broyden / damped mixing
+  kStFinal,         // P, W and results
+  kStages
 };
 
 __host__ __device__ inline int tri_index(int a, int b, int nat) {

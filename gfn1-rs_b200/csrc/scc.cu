@@ -39,6 +39,27 @@ struct SccShared {
   int iscal[16];
 };
 
+// Per-stage clock accounting by thread 0 of the CTA (no-op without a buffer).
+struct StageClock {
+  unsigned long long* out;
+  long long t0;
+  __device__ explicit StageClock(unsigned long long* o) {
+    out = o;
+    t0 = clock64();
+  }
+  __device__ __forceinline__ void mark(int stage) {
+    if (!out) return;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const long long t = clock64();
+      atomicAdd(out + stage, (unsigned long long)(t - t0));
+      t0 = t;
+    } else {
+      t0 = clock64();
+    }
+  }
+};
+
 // Layout of one CTA's workspace slot (doubles).  maxn / maxnsh / cap / maxnat
 // are the batch maxima; matrices use the molecule's own N as leading dimension.
 struct CtaWs {
@@ -219,6 +240,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
   }
   __syncthreads();
 
+  StageClock clk(B.stage_cycles);
   // ---- Cholesky S = L L^T (right-looking, in place on L)
   for (long long i = tid; i < (long long)N * N; i += nt) L[i] = S[i];
   __syncthreads();
@@ -280,6 +302,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
   for (int i = wid; i < N; i += nw)
     for (int j = i + 1 + lane; j < N; j += 32) Hp[(long long)i * N + j] = Hp[(long long)j * N + i];
 
+  clk.mark(kStPrologue);
   // ---- SCC state
   double nref = 0.0;
   for (int s = 0; s < nsh; ++s) nref += M.elem[B.z[a0 + sh_atom[s]]].refocc[sh_k[s]];
@@ -325,6 +348,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
         A[(long long)j * N + i] = f;
       }
     __syncthreads();
+    clk.mark(kStFock);
     // (3) Householder tridiagonalisation; v_k kept in row k right of the diagonal
     for (int k = 0; k < N - 2; ++k) {
       const int mlen = N - k - 1;
@@ -390,6 +414,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
       tau[N - 1] = 0.0;
     }
     __syncthreads();
+    clk.mark(kStTridiag);
     // (4) eigenvalues by bisection
     double gl = INFINITY, gu = -INFINITY, onenrm = 0.0, emax2 = 0.0;
     for (int i = tid; i < N; i += nt) {
@@ -423,6 +448,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
       eps[k] = 0.5 * (lo + hi);
     }
     __syncthreads();
+    clk.mark(kStEigval);
     // (5) occupations (src/electronic.rs:3815-3921), warp 0
     if (wid == 0) {
       double f_mu = 0.0, f_ts = 0.0;
@@ -479,6 +505,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     for (int i = tid; i < N; i += nt)
       if (occ[i] > 1e-30) nocc_loc = max(nocc_loc, i + 1);
     const int nocc = (int)block_max((double)nocc_loc, sh.red);
+    clk.mark(kStFermi);
     // (6) inverse iteration for the occupied eigenvectors (columns of Z)
     const double ortol = 1e-5 * onenrm;
     const double tiny = DBL_EPSILON * fmax(onenrm, 1e-300);
@@ -513,6 +540,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
       }
     }
     __syncthreads();
+    clk.mark(kStInvIter);
     // (7) back-transformation Z := Q Z, one thread per eigenvector column
     for (int j = tid; j < nocc; j += nt) {
       for (int k = N - 3; k >= 0; --k) {
@@ -526,6 +554,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
       }
     }
     __syncthreads();
+    clk.mark(kStBackTr);
     // (8) C = L^-T Z, D = L Z and the AO populations (S P)_mu,mu
     for (int mu_ = wid; mu_ < N; mu_ += nw) {
       double popp = 0.0;
@@ -541,6 +570,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
       if (lane == 0) pop[mu_] = popp;
     }
     __syncthreads();
+    clk.mark(kStPop);
     // (9) output charges, energies (src/electronic.rs:2173-2191)
     for (int s = tid; s < nsh; s += nt) {
       const ElemTable& el = M.elem[B.z[a0 + sh_atom[s]]];
@@ -583,6 +613,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
       converged = true;
       break;
     }
+    clk.mark(kStEnergy);
     // (10) charge mixing
     bool have_next = false;
     if (opt.broyden) {
@@ -742,6 +773,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     last_e = escc;
     have_e = true;
     __syncthreads();
+    clk.mark(kStMix);
   }
   if (iter > opt.max_scc) iter = opt.max_scc;
 
@@ -793,6 +825,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
       B.W[mo + (long long)j * N + i] = q;
     }
   __syncthreads();
+  clk.mark(kStFinal);
 }
 
 __global__ void __launch_bounds__(256) scc_kernel(Batch B, Model M, SccOptions opt, int max_nsh, int max_n) {

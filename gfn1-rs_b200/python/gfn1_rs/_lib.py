@@ -96,7 +96,11 @@ def load():
         L.gfn1_batch_outputs_device.argtypes = [vp, ctypes.POINTER(Outputs)]
         L.gfn1_batch_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
                                       ctypes.POINTER(ctypes.c_int64), _ip]
-        for name in ("gfn1_engine_create", "gfn1_basis_size", "gfn1_run", "gfn1_batch_energy_gradient",
+        L.gfn1_batch_launch_stage.argtypes = [vp, ctypes.c_int, vp]
+        L.gfn1_batch_stage_cycles.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
+        L.gfn1_batch_io_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
+        for name in ("gfn1_batch_launch_stage", "gfn1_batch_stage_cycles", "gfn1_batch_io_bytes",
+                     "gfn1_engine_create", "gfn1_basis_size", "gfn1_run", "gfn1_batch_energy_gradient",
                      "gfn1_batch_create", "gfn1_batch_set_positions", "gfn1_batch_set_initial_charges",
                      "gfn1_batch_launch", "gfn1_batch_download", "gfn1_batch_outputs_device", "gfn1_batch_info"):
             getattr(L, name).restype = ctypes.c_int
@@ -150,6 +154,20 @@ class Engine:
             self.close()
         except Exception:
             pass
+
+    def element_sizes(self) -> tuple[np.ndarray, np.ndarray]:
+        """(nao[Z], nshells[Z]) for Z = 0..86; -1 where the device path lacks the element."""
+        if getattr(self, "_elem_sizes", None) is None:
+            nao = np.full(87, -1, dtype=np.int64)
+            nsh = np.full(87, -1, dtype=np.int64)
+            L = load()
+            a, s = ctypes.c_int32(), ctypes.c_int32()
+            for zz in range(1, 87):
+                z = np.array([zz], dtype=np.uint8)
+                if L.gfn1_basis_size(self.handle, 1, ptr(z, ctypes.c_uint8), ctypes.byref(a), ctypes.byref(s)) == 0:
+                    nao[zz], nsh[zz] = a.value, s.value
+            self._elem_sizes = (nao, nsh)
+        return self._elem_sizes
 
     def basis_size(self, numbers) -> tuple[int, int]:
         z = np.ascontiguousarray(numbers, dtype=np.uint8)

@@ -58,11 +58,14 @@ class BatchCalculator:
                          enable_dispersion=int(bool(enable_dispersion)))
 
     def shell_offsets(self, atom_offsets, numbers) -> np.ndarray:
-        off = np.asarray(atom_offsets)
-        out = np.zeros(len(off), dtype=np.int64)
-        for m in range(len(off) - 1):
-            out[m + 1] = out[m] + self.engine.basis_size(numbers[off[m]:off[m + 1]])[1]
-        return out
+        """Prefix sums of the shell counts, laid out as the C side does (atoms of
+        unsupported elements contribute no shells)."""
+        off = np.asarray(atom_offsets, dtype=np.int64)
+        z = np.asarray(numbers, dtype=np.int64)
+        nsh_z = self.engine.element_sizes()[1]
+        per_atom = np.where((z >= 1) & (z <= 86), nsh_z[np.clip(z, 0, 86)], 0)
+        cum = np.concatenate([[0], np.cumsum(np.maximum(per_atom, 0))])
+        return cum[off]
 
     def calculate_flat(self, atom_offsets, numbers, xyz_bohr, charges=None, initial_shell_charges=None,
                        compute_gradient=True, raise_on_error=False) -> BatchResult:
@@ -163,6 +166,25 @@ class ResidentBatch:
         """Enqueue the kernels on a CUDA stream handle (int) or the engine stream."""
         s = None if stream is None else ctypes.c_void_p(int(stream))
         _lib.check(_lib.load().gfn1_batch_launch(self.handle, s), self.calc.engine.handle)
+
+    def launch_stage(self, stage: int, stream: int | None = None):
+        """0 = setup, 1 = SCC, 2 = gradient (for per-kernel timing)."""
+        s = None if stream is None else ctypes.c_void_p(int(stream))
+        _lib.check(_lib.load().gfn1_batch_launch_stage(self.handle, int(stage), s), self.calc.engine.handle)
+
+    STAGES = ("prologue", "fock", "tridiag", "eigval", "fermi", "inviter", "backtr", "pop", "energy", "mix", "final")
+
+    def stage_cycles(self) -> dict:
+        """Per-stage SCC clock totals (batch created with GFN1_PROFILE=1)."""
+        buf = (ctypes.c_uint64 * len(self.STAGES))()
+        _lib.check(_lib.load().gfn1_batch_stage_cycles(self.handle, buf, len(self.STAGES)), self.calc.engine.handle)
+        return dict(zip(self.STAGES, list(buf)))
+
+    def io_bytes(self) -> tuple[int, int]:
+        h2d, d2h = ctypes.c_int64(), ctypes.c_int64()
+        _lib.check(_lib.load().gfn1_batch_io_bytes(self.handle, ctypes.byref(h2d), ctypes.byref(d2h)),
+                   self.calc.engine.handle)
+        return h2d.value, d2h.value
 
     def device_outputs(self) -> dict:
         out = _lib.Outputs()

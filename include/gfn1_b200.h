@@ -112,6 +112,17 @@ int gfn1_batch_set_initial_charges(gfn1_batch* b, const double* q, int on_device
 /* Enqueues setup, SCC and gradient kernels on `stream` (a cudaStream_t passed as
  * a void pointer; NULL = the engine's stream).  Asynchronous. */
 int gfn1_batch_launch(gfn1_batch* b, void* stream);
+/* Enqueues one stage: 0 = setup (CN, S, H0, Coulomb matrix, repulsion, D3),
+ * 1 = persistent SCC, 2 = gradient; -1 = all three (same as gfn1_batch_launch).
+ * Lets a caller time each kernel with events on its own stream. */
+int gfn1_batch_launch_stage(gfn1_batch* b, int stage, void* stream);
+/* Per-stage SCC clock totals (GFN1_PROFILE=1 at batch creation), n <= 11:
+ * prologue, Fock, tridiagonalisation, eigenvalues, occupations, inverse
+ * iteration, back-transformation, populations, energy, mixing, final. */
+int gfn1_batch_stage_cycles(const gfn1_batch* b, uint64_t* cycles, int n);
+/* Bytes of the input blob (one host->device copy per call) and of the output
+ * blob (one device->host copy per call). */
+int gfn1_batch_io_bytes(const gfn1_batch* b, int64_t* h2d, int64_t* d2h);
 /* Synchronises and copies results to host buffers. */
 int gfn1_batch_download(gfn1_batch* b, const gfn1_outputs* out);
 /* Device pointers of the batch-owned result arrays (valid until destroy). */
