@@ -1001,3 +1001,206 @@ int gfn1_run(gfn1_engine* eng, int nat, const uint8_t* z, const double* xyz_bohr
 }
 
 }  // extern "C"
+
+// ============================================================== no-allocation entry point
+//
+// gfn1_run_noalloc evaluates one molecule without allocating anything: no
+// cudaMalloc, cudaHostAlloc or cudaFree, and no allocating library routine.
+// Every device buffer the three kernels need lives in g_noalloc_scratch below,
+// a fixed 4.25 MiB array that exists on every GPU that loads this library for
+// as long as the process runs.  The host side stages its few kilobytes on the
+// stack.  Sizes beyond kNa* are rejected.
+namespace {
+constexpr int kNaMaxAtoms = 64;
+constexpr int kNaMaxAo = 128;
+constexpr int kNaMaxShells = 128;
+constexpr int kNaMaxHist = 250;
+constexpr size_t kNoallocBytes = 4456448;  // 4.25 MiB
+constexpr int kNaMaxDevices = 64;
+unsigned char* g_noalloc_dev_ptr[kNaMaxDevices];  // device address of the array, per device
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
+
+extern "C" int gfn1_run_noalloc(gfn1_engine* eng, int nat, const uint8_t* z, const double* xyz_bohr, double charge,
+                                const double* init_shell_q, const gfn1_options* opt, const gfn1_outputs* out,
+                                void* stream) {
+  if (!eng || nat < 1 || !z || !xyz_bohr) return fail(eng, GFN1_E_INVALID_INPUT, "invalid arguments");
+  gfn1_options o;
+  if (opt) o = *opt;
+  else fill_default(&o);
+  if (o.max_scc < 1) return fail(eng, GFN1_E_INVALID_INPUT, "max_scc must be at least 1");
+  if (nat > kNaMaxAtoms)
+    return fail(eng, GFN1_E_INVALID_INPUT, "gfn1_run_noalloc handles at most " + std::to_string(kNaMaxAtoms) +
+                                               " atoms; got " + std::to_string(nat) + " (use gfn1_run)");
+  int n = 0, nsh = 0;
+  double nref = 0.0;
+  for (int a = 0; a < nat; ++a) {
+    const int zz = z[a];
+    if (zz < 1 || zz > kMaxZ) return fail(eng, GFN1_E_MISSING_ELEMENT, "missing GFN1 parameter block for Z=" + std::to_string(zz));
+    if (!eng->device_ok[zz])
+      return fail(eng, GFN1_E_UNSUPPORTED, "element Z=" + std::to_string(zz) + " has d/f shells; outside the device path");
+    n += eng->elem[zz].nao;
+    nsh += eng->elem[zz].nsh;
+    nref += eng->refocc_total[zz];
+  }
+  const int cap = std::max(1, std::min(std::max(o.scc_broyden_size, 2), o.max_scc));
+  if (n > kNaMaxAo || nsh > kNaMaxShells)
+    return fail(eng, GFN1_E_INVALID_INPUT, "gfn1_run_noalloc handles at most " + std::to_string(kNaMaxAo) +
+                                               " AOs and shells; got " + std::to_string(n) + " AOs, " +
+                                               std::to_string(nsh) + " shells (use gfn1_run)");
+  if (cap > kNaMaxHist)
+    return fail(eng, GFN1_E_INVALID_INPUT, "gfn1_run_noalloc keeps at most " + std::to_string(kNaMaxHist) +
+                                               " Broyden history vectors (min(scc_broyden_size, max_scc))");
+  if (!finite_all(xyz_bohr, 3LL * nat)) return fail(eng, GFN1_E_NAN, "non-finite coordinate");
+  const double nelec = nref - charge;
+  if (!std::isfinite(nelec) || nelec < -1e-8 || nelec > 2.0 * n + 1e-8)
+    return fail(eng, GFN1_E_INVALID_INPUT, "invalid electron count");
+  const int dev = eng->device;
+  if (dev < 0 || dev >= kNaMaxDevices) return fail(eng, GFN1_E_INVALID_INPUT, "device ordinal out of range");
+  cudaError_t e = cudaSetDevice(dev);
+  if (e != cudaSuccess) return cuda_fail(eng, e, "cudaSetDevice");
+  if (!g_noalloc_dev_ptr[dev]) {  // once per device, with that device current
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(eng, e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    g_noalloc_dev_ptr[dev] = (unsigned char*)p;
+  }
+  unsigned char* base = g_noalloc_dev_ptr[dev];
+  cudaStream_t st = stream ? (cudaStream_t)stream : eng->stream;
+
+  // ---- layout inside the scratch array (byte offsets, 256-aligned)
+  const long long n2 = (((long long)n * n + 31) / 32) * 32;
+  const long long npair = (long long)nat * (nat - 1) / 2;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t at = off;
+    off = align256(off + bytes);
+    return at;
+  };
+  // input region, mirrored by the stack staging buffer
+  const size_t i_atom = take(2 * sizeof(int)), i_shell = take(2 * sizeof(int)), i_ao = take(2 * sizeof(int));
+  const size_t i_mat = take(2 * sizeof(long long)), i_gam = take(2 * sizeof(long long)),
+               i_pair = take(2 * sizeof(long long));
+  const size_t i_order = take(sizeof(int)), i_st0 = take(sizeof(int)), i_z = take(sizeof(int) * nat);
+  const size_t i_charge = take(sizeof(double)), i_xyz = take(sizeof(double) * 3 * nat),
+               i_q0 = take(sizeof(double) * nsh);
+  const size_t in_bytes = off;
+  // output region
+  const size_t o_terms = take(sizeof(double) * kTerms), o_grad = take(sizeof(double) * 3 * nat),
+               o_shq = take(sizeof(double) * nsh), o_atq = take(sizeof(double) * nat),
+               o_dip = take(sizeof(double) * 3), o_fermi = take(sizeof(double)), o_iter = take(sizeof(int)),
+               o_status = take(sizeof(int));
+  const size_t out_end = off;
+  // work region
+  const size_t w_S = take(sizeof(double) * n2), w_H0 = take(sizeof(double) * n2), w_P = take(sizeof(double) * n2),
+               w_W = take(sizeof(double) * n2);
+  const long long ws_doubles = scc_workspace_doubles(n, nsh, cap, nat);
+  const size_t w_ws = take(sizeof(double) * ws_doubles), w_gam = take(sizeof(double) * (size_t)nsh * nsh),
+               w_pair = take(sizeof(double) * 8 * std::max<long long>(npair, 1)), w_cn = take(sizeof(double) * nat),
+               w_pot = take(sizeof(double) * nsh), w_se = take(sizeof(double) * nsh),
+               w_gcl = take(sizeof(double) * 3 * nat), w_queue = take(4 * sizeof(int));
+  if (off > kNoallocBytes) return fail(eng, GFN1_E_INVALID_INPUT, "molecule exceeds the no-allocation scratch");
+
+  // ---- stage inputs on the stack and copy them into the scratch array
+  alignas(256) unsigned char hin[12288];
+  alignas(256) unsigned char hout[8192];
+  if (in_bytes > sizeof hin || out_end - o_terms > sizeof hout)
+    return fail(eng, GFN1_E_INVALID_INPUT, "molecule exceeds the no-allocation staging buffers");
+  std::memset(hin, 0, in_bytes);
+  ((int*)(hin + i_atom))[1] = nat;
+  ((int*)(hin + i_shell))[1] = nsh;
+  ((int*)(hin + i_ao))[1] = n;
+  ((long long*)(hin + i_mat))[1] = n2;
+  ((long long*)(hin + i_gam))[1] = (long long)nsh * nsh;
+  ((long long*)(hin + i_pair))[1] = npair;
+  for (int a = 0; a < nat; ++a) ((int*)(hin + i_z))[a] = z[a];
+  *(double*)(hin + i_charge) = charge;
+  std::memcpy(hin + i_xyz, xyz_bohr, sizeof(double) * 3 * nat);
+  if (init_shell_q) std::memcpy(hin + i_q0, init_shell_q, sizeof(double) * nsh);
+  if ((e = cudaMemcpyAsync(base, hin, in_bytes, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+    return cuda_fail(eng, e, "host to device copy");
+  // every call reuses the array: clear what the kernels expect to start at zero
+  if ((e = cudaMemsetAsync(base + o_status, 0, sizeof(int), st)) != cudaSuccess ||
+      (e = cudaMemsetAsync(base + w_queue, 0, 4 * sizeof(int), st)) != cudaSuccess)
+    return cuda_fail(eng, e, "scratch reset");
+
+  Batch B;
+  std::memset(&B, 0, sizeof B);
+  B.nmol = 1;
+  B.max_nat = nat;
+  B.atom_off = (const int*)(base + i_atom);
+  B.shell_off = (const int*)(base + i_shell);
+  B.ao_off = (const int*)(base + i_ao);
+  B.mat_off = (const long long*)(base + i_mat);
+  B.gam_off = (const long long*)(base + i_gam);
+  B.pair_off = (const long long*)(base + i_pair);
+  B.order = (const int*)(base + i_order);
+  B.z = (const int*)(base + i_z);
+  B.xyz = (const double*)(base + i_xyz);
+  B.charge = (const double*)(base + i_charge);
+  B.init_q = init_shell_q ? (const double*)(base + i_q0) : nullptr;
+  B.S = (double*)(base + w_S);
+  B.H0 = (double*)(base + w_H0);
+  B.P = (double*)(base + w_P);
+  B.W = (double*)(base + w_W);
+  B.ws = (double*)(base + w_ws);
+  B.ws_stride = ws_doubles;
+  B.ws_maxn = n;
+  B.ws_maxnsh = nsh;
+  B.ws_cap = cap;
+  B.gam = (double*)(base + w_gam);
+  B.pairbuf = (double*)(base + w_pair);
+  B.cn = (double*)(base + w_cn);
+  B.shell_q = (double*)(base + o_shq);
+  B.shell_pot = (double*)(base + w_pot);
+  B.atom_q = (double*)(base + o_atq);
+  B.se = (double*)(base + w_se);
+  B.terms = (double*)(base + o_terms);
+  B.grad = (double*)(base + o_grad);
+  B.grad_classic = (double*)(base + w_gcl);
+  B.dipole = (double*)(base + o_dip);
+  B.fermi = (double*)(base + o_fermi);
+  B.iterations = (int*)(base + o_iter);
+  B.status = (int*)(base + o_status);
+  B.queue = (int*)(base + w_queue);
+  B.stage_cycles = nullptr;
+  const Model M = eng->model();
+  SccOptions so;
+  so.max_scc = o.max_scc;
+  so.broyden = o.scc_broyden;
+  so.broyden_size = o.scc_broyden_size;
+  so.enable_dispersion = o.enable_dispersion;
+  so.energy_tol = o.energy_tolerance;
+  so.charge_tol = o.charge_tolerance;
+  so.mixing = o.mixing;
+  so.etemp = o.electronic_temperature;
+  const size_t sm_setup = sizeof(double) * (16 * (size_t)nat + 32) + sizeof(int) * (3 * (size_t)nat + 2 + 2 * (size_t)nsh);
+  const size_t sm_scc = sizeof(int) * (3 * (size_t)nsh + n + nat + 1);
+  const size_t sm_grad = sizeof(double) * 7 * (size_t)nat + sizeof(int) * (3 * (size_t)nat + 2);
+  setup_kernel<<<1, 256, sm_setup, st>>>(B, M, o.enable_dispersion, nsh);
+  scc_kernel<<<1, 256, sm_scc, st>>>(B, M, so, nsh, n);
+  if (o.compute_gradient) grad_kernel<<<1, 256, sm_grad, st>>>(B, M);
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(eng, e, "kernel launch");
+  if ((e = cudaMemcpyAsync(hout, base + o_terms, out_end - o_terms, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+    return cuda_fail(eng, e, "device to host copy");
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(eng, e, "no-allocation run");
+  auto hp = [&](size_t o_) { return hout + (o_ - o_terms); };
+  const int status = *(const int*)hp(o_status);
+  const double* terms = (const double*)hp(o_terms);
+  if (out) {
+    if (out->energy) out->energy[0] = terms[0];
+    if (out->terms) std::memcpy(out->terms, terms, sizeof(double) * kTerms);
+    if (out->gradient && o.compute_gradient) std::memcpy(out->gradient, hp(o_grad), sizeof(double) * 3 * nat);
+    if (out->shell_charges) std::memcpy(out->shell_charges, hp(o_shq), sizeof(double) * nsh);
+    if (out->atomic_charges) std::memcpy(out->atomic_charges, hp(o_atq), sizeof(double) * nat);
+    if (out->dipole) std::memcpy(out->dipole, hp(o_dip), sizeof(double) * 3);
+    if (out->fermi_level) std::memcpy(out->fermi_level, hp(o_fermi), sizeof(double));
+    if (out->iterations) std::memcpy(out->iterations, hp(o_iter), sizeof(int));
+    if (out->status) out->status[0] = status;
+  }
+  if (status != GFN1_OK)
+    return fail(eng, status, status == GFN1_E_SCC_NOT_CONVERGED ? "GFN1 SCC did not converge"
+                                                                 : "molecule failed with status " + std::to_string(status));
+  return GFN1_OK;
+}

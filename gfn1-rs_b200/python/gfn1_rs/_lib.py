@@ -99,7 +99,9 @@ def load():
         L.gfn1_batch_launch_stage.argtypes = [vp, ctypes.c_int, vp]
         L.gfn1_batch_stage_cycles.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
         L.gfn1_batch_io_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
-        for name in ("gfn1_batch_launch_stage", "gfn1_batch_stage_cycles", "gfn1_batch_io_bytes",
+        L.gfn1_run_noalloc.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_uint8), _dp, ctypes.c_double, _dp,
+                                       ctypes.POINTER(Options), ctypes.POINTER(Outputs), vp]
+        for name in ("gfn1_run_noalloc", "gfn1_batch_launch_stage", "gfn1_batch_stage_cycles", "gfn1_batch_io_bytes",
                      "gfn1_engine_create", "gfn1_basis_size", "gfn1_run", "gfn1_batch_energy_gradient",
                      "gfn1_batch_create", "gfn1_batch_set_positions", "gfn1_batch_set_initial_charges",
                      "gfn1_batch_launch", "gfn1_batch_download", "gfn1_batch_outputs_device", "gfn1_batch_info"):

@@ -130,6 +130,24 @@ int gfn1_batch_outputs_device(gfn1_batch* b, gfn1_outputs* out);
 /* Sizes of the batch: natoms, nshells, total AOs; launches = kernels per run. */
 int gfn1_batch_info(const gfn1_batch* b, int64_t* natoms, int64_t* nshells, int64_t* naos, int32_t* launches);
 
+/* One molecule without allocating anything (no reference counterpart: the Rust
+ * library has no device memory).  For callers that cannot call cudaMalloc or
+ * cudaHostAlloc at the point of use -- code running under a memory manager that
+ * owns all device memory, real-time loops that forbid allocation, or a step
+ * that must not change the process's memory footprint.  All device scratch is a
+ * fixed 4.25 MiB library array that every GPU loading the library holds until
+ * exit; host staging uses the stack.  Limits: at most 64 atoms, 128 AOs,
+ * 128 shells and 250 Broyden history vectors (min(scc_broyden_size, max_scc));
+ * larger inputs return GFN1_E_INVALID_INPUT with a message naming the limit.
+ * The first call on a device looks up the array's device address (once per
+ * device, that device current); make that first call before any stream
+ * capture.  Every call reuses the same array, so calls that overlap on the GPU
+ * (two host threads, or asynchronous streams) race: serialise them.  Inputs
+ * and `out` are host memory; `stream` is a cudaStream_t or NULL for the
+ * engine's stream.  Synchronous. */
+int gfn1_run_noalloc(gfn1_engine* eng, int nat, const uint8_t* z, const double* xyz_bohr, double charge,
+                     const double* init_shell_q, const gfn1_options* opt, const gfn1_outputs* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
