@@ -23,9 +23,12 @@
 
 namespace gfn1 {
 __global__ void setup_kernel(Batch B, Model M, int enable_dispersion, int max_nsh);
-__global__ void scc_kernel(Batch B, Model M, SccOptions opt, int max_nsh, int max_n);
 __global__ void grad_kernel(Batch B, Model M);
 long long scc_workspace_doubles(int maxn, int maxnsh, int cap, int maxnat);
+size_t scc_smem_bytes(int maxnsh, int maxn, int maxnat, int matrix_n);
+size_t scc_max_dynamic_smem(int nt);
+cudaError_t launch_scc(int nt, int grid, size_t smem, cudaStream_t st, const Batch& B, const Model& M,
+                       const SccOptions& opt, const SccLaunch& SL);
 }  // namespace gfn1
 
 using namespace gfn1;
@@ -239,8 +242,15 @@ struct gfn1_batch {
   gfn1_engine* eng = nullptr;
   int nmol = 0;
   long long natoms = 0, nshells = 0, naos = 0, mat_total = 0, gam_total = 0, pair_total = 0;
-  int max_nat = 0, max_nsh = 0, max_n = 0, cap = 0, n_cta = 0;
-  long long ws_stride = 0;
+  int max_nat = 0, max_nsh = 0, max_n = 0, cap = 0;
+  // SCC size classes: [0] large molecules (512 threads, 1 CTA/SM), [1] the rest
+  struct SccClass {
+    int q_begin = 0, q_end = 0, n_cta = 0, nt = 256, maxn = 0, maxnsh = 0, maxnat = 0;
+    long long ws_offset = 0, ws_stride = 0;
+    size_t smem = 0;
+  } cls[2];
+  cudaStream_t side = nullptr;  // second stream for the concurrent class launch
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   gfn1_options opt;
   bool has_init_q = false;
   bool profiling = false;
@@ -279,7 +289,7 @@ struct gfn1_batch {
     B.P = P.p;
     B.W = W.p;
     B.ws = ws.p;
-    B.ws_stride = ws_stride;
+    B.ws_stride = 0;
     B.ws_maxn = max_n;
     B.ws_maxnsh = max_nsh;
     B.ws_cap = cap;
@@ -309,6 +319,11 @@ struct gfn1_batch {
     for (DevBuf<double>* d : {&S, &H0, &P, &W, &ws, &gam, &pairbuf, &cn, &shell_pot, &se, &grad_classic}) d->release();
     queue.release();
     stage.release();
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (side) cudaStreamDestroy(side);
+    ev_fork = ev_join = nullptr;
+    side = nullptr;
   }
 };
 
@@ -643,12 +658,44 @@ int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t*
   for (int m = 0; m < nmol; ++m) h_order[m] = m;
   std::stable_sort(h_order, h_order + nmol, [&](int x, int y) { return n_m[x] > n_m[y]; });
   b->cap = std::max(1, std::min(std::max(o.scc_broyden_size, 2), o.max_scc));
-  b->ws_stride = scc_workspace_doubles(b->max_n, b->max_nsh, b->cap, b->max_nat);
-  const int per_sm = 2;
-  b->n_cta = std::max(1, std::min(nmol, per_sm * eng->num_sms));
+  // size classes over the sorted order: N > kLargeN runs 512-thread CTAs, one
+  // per SM, with up to 227 KB of shared memory; the rest 256-thread CTAs, two per SM
+  const int kLargeN = 96;
+  int n_large = 0;
+  while (n_large < nmol && n_m[h_order[n_large]] > kLargeN) ++n_large;
+  long long ws_total = 0;
+  for (int c = 0; c < 2; ++c) {
+    gfn1_batch::SccClass& K = b->cls[c];
+    K.q_begin = c == 0 ? 0 : n_large;
+    K.q_end = c == 0 ? n_large : nmol;
+    K.nt = c == 0 ? 512 : 256;
+    K.maxn = K.maxnsh = K.maxnat = 0;
+    for (int q = K.q_begin; q < K.q_end; ++q) {
+      const int mm = h_order[q];
+      K.maxn = std::max(K.maxn, n_m[mm]);
+      K.maxnsh = std::max(K.maxnsh, nsh_m[mm]);
+      K.maxnat = std::max(K.maxnat, atom_offsets[mm + 1] - atom_offsets[mm]);
+    }
+    const int count = K.q_end - K.q_begin;
+    K.n_cta = count == 0 ? 0 : std::max(1, std::min(count, (c == 0 ? 1 : 2) * eng->num_sms));
+    K.ws_stride = count == 0 ? 0 : scc_workspace_doubles(std::max(K.maxn, 1), std::max(K.maxnsh, 1), b->cap,
+                                                           std::max(K.maxnat, 1));
+    K.ws_offset = ws_total;
+    ws_total += K.ws_stride * K.n_cta;
+    const size_t full = scc_smem_bytes(K.maxnsh, K.maxn, K.maxnat, K.maxn);
+    const size_t fixed = scc_smem_bytes(K.maxnsh, K.maxn, K.maxnat, 0);
+    const size_t limit = scc_max_dynamic_smem(K.nt);
+    K.smem = std::max(fixed, std::min(full, limit));
+  }
+  if (!b->side) {
+    if (cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) != cudaSuccess)
+      return fail(eng, GFN1_E_DEVICE, "stream creation failed");
+  }
   bool ok = b->d_in.ensure(L.in_bytes) && b->d_out.ensure(L.out_bytes) && b->queue.ensure(4) &&
             b->stage.ensure(kStages) && b->S.ensure(mat_total) && b->H0.ensure(mat_total) && b->P.ensure(mat_total) &&
-            b->W.ensure(mat_total) && b->ws.ensure((size_t)b->ws_stride * b->n_cta) && b->gam.ensure(gam_total) &&
+            b->W.ensure(mat_total) && b->ws.ensure((size_t)std::max<long long>(ws_total, 1)) && b->gam.ensure(gam_total) &&
             b->pairbuf.ensure(8 * std::max<long long>(pair_total, 1)) && b->cn.ensure(natoms) &&
             b->shell_pot.ensure(nshells) && b->se.ensure(nshells) && b->grad_classic.ensure(3 * natoms);
   if (!ok) return fail(eng, GFN1_E_DEVICE, "device allocation failed for the batch workspace");
@@ -689,9 +736,28 @@ int launch_stage(gfn1_batch* b, int stage, cudaStream_t st) {
     so.charge_tol = b->opt.charge_tolerance;
     so.mixing = b->opt.mixing;
     so.etemp = b->opt.electronic_temperature;
-    const size_t smem = sizeof(int) * (3 * (size_t)b->max_nsh + b->max_n + b->max_nat + 1);
-    if (smem > 48 * 1024) cudaFuncSetAttribute(scc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    scc_kernel<<<b->n_cta, nt, smem, st>>>(B, M, so, b->max_nsh, b->max_n);
+    // fork: the small-molecule class runs on the side stream next to the large one
+    if ((e = cudaEventRecord(b->ev_fork, st)) != cudaSuccess || (e = cudaStreamWaitEvent(b->side, b->ev_fork, 0)) != cudaSuccess)
+      return cuda_fail(eng, e, "stream fork");
+    for (int c = 0; c < 2; ++c) {
+      const gfn1_batch::SccClass& K = b->cls[c];
+      if (K.n_cta == 0) continue;
+      SccLaunch SL;
+      SL.q_begin = K.q_begin;
+      SL.q_end = K.q_end;
+      SL.counter = b->queue.p + c;
+      SL.ws = b->ws.p + K.ws_offset;
+      SL.ws_stride = K.ws_stride;
+      SL.maxn = K.maxn;
+      SL.maxnsh = K.maxnsh;
+      SL.maxnat = K.maxnat;
+      SL.cap = b->cap;
+      SL.smem_bytes = (int)K.smem;
+      if ((e = launch_scc(K.nt, K.n_cta, K.smem, c == 0 ? st : b->side, B, M, so, SL)) != cudaSuccess)
+        return cuda_fail(eng, e, "scc launch");
+    }
+    if ((e = cudaEventRecord(b->ev_join, b->side)) != cudaSuccess || (e = cudaStreamWaitEvent(st, b->ev_join, 0)) != cudaSuccess)
+      return cuda_fail(eng, e, "stream join");
   } else if (stage == 2) {
     if (!b->opt.compute_gradient) return GFN1_OK;
     const size_t smem = sizeof(double) * 7 * (size_t)b->max_nat + sizeof(int) * (3 * (size_t)b->max_nat + 2);
@@ -1176,10 +1242,23 @@ extern "C" int gfn1_run_noalloc(gfn1_engine* eng, int nat, const uint8_t* z, con
   so.mixing = o.mixing;
   so.etemp = o.electronic_temperature;
   const size_t sm_setup = sizeof(double) * (16 * (size_t)nat + 32) + sizeof(int) * (3 * (size_t)nat + 2 + 2 * (size_t)nsh);
-  const size_t sm_scc = sizeof(int) * (3 * (size_t)nsh + n + nat + 1);
+  const size_t sm_scc = std::max(scc_smem_bytes(nsh, n, nat, 0),
+                                 std::min(scc_smem_bytes(nsh, n, nat, n), scc_max_dynamic_smem(n > 96 ? 512 : 256)));
   const size_t sm_grad = sizeof(double) * 7 * (size_t)nat + sizeof(int) * (3 * (size_t)nat + 2);
   setup_kernel<<<1, 256, sm_setup, st>>>(B, M, o.enable_dispersion, nsh);
-  scc_kernel<<<1, 256, sm_scc, st>>>(B, M, so, nsh, n);
+  SccLaunch SL;
+  SL.q_begin = 0;
+  SL.q_end = 1;
+  SL.counter = B.queue;
+  SL.ws = B.ws;
+  SL.ws_stride = ws_doubles;
+  SL.maxn = n;
+  SL.maxnsh = nsh;
+  SL.maxnat = nat;
+  SL.cap = cap;
+  SL.smem_bytes = (int)sm_scc;
+  if ((e = launch_scc(n > 96 ? 512 : 256, 1, sm_scc, st, B, M, so, SL)) != cudaSuccess)
+    return cuda_fail(eng, e, "scc launch");
   if (o.compute_gradient) grad_kernel<<<1, 256, sm_grad, st>>>(B, M);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(eng, e, "kernel launch");
   if ((e = cudaMemcpyAsync(hout, base + o_terms, out_end - o_terms, cudaMemcpyDeviceToHost, st)) != cudaSuccess)

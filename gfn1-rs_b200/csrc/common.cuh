@@ -64,6 +64,16 @@ struct SccOptions {
   double energy_tol, charge_tol, mixing, etemp;
 };
 
+// Parameters of one launch of the persistent SCC kernel (one size class).
+struct SccLaunch {
+  int q_begin, q_end;   // range of Batch::order processed by this launch
+  int* counter;         // work counter, zeroed before the launch
+  double* ws;           // per-CTA global workspace, ws_stride doubles each
+  long long ws_stride;
+  int maxn, maxnsh, maxnat, cap;  // maxima of the class (workspace layout)
+  int smem_bytes;       // dynamic shared memory of the launch
+};
+
 // Everything a kernel needs about a batch of molecules.  All pointers are
 // device pointers; offsets index the flat per-batch arrays.
 struct Batch {

@@ -1,7 +1,10 @@
 // Persistent SCC kernel: each CTA pulls molecules from a work queue (most
 // expensive first) and runs the complete self-consistent-charge loop of
 // gfn1-rs `run_scc_with_core` (src/electronic.rs:849-2054, plain charge-vector
-// branch, ladder rung 0) on the device.
+// branch, ladder rung 0) on the device.  Two size classes are launched
+// concurrently: 512 threads with one CTA per SM for the large molecules, 256
+// threads with two CTAs per SM for the rest.  The working matrix of the
+// eigensolver lives in shared memory whenever it fits.
 //
 // Algorithmic choices that differ from the reference but give the same results
 // up to FP64 rounding:
@@ -11,9 +14,10 @@
 //    the potential term  -1/2 (M + M^T),  M = L^-1 diag(v) L  (lower triangular),
 //    because  L^-1 (S o V) L^-T = L^-1 diag(v) L + (L^-1 diag(v) L)^T  for
 //    V_mu,nu = v_mu + v_nu (src/electronic.rs:3133-3158).
-//  * eigensolver: Householder tridiagonalisation, Sturm-sequence bisection for the
-//    eigenvalues and inverse iteration (with modified Gram-Schmidt inside
-//    eigenvalue clusters) for the occupied eigenvectors only, followed by the
+//  * eigensolver: Householder tridiagonalisation (two barriers per column),
+//    Sturm-sequence multisection for the eigenvalues the occupations need,
+//    inverse iteration (with modified Gram-Schmidt inside eigenvalue clusters)
+//    for the occupied eigenvectors only, and a blocked (compact-WY)
 //    back-transformation (replaces faer's self_adjoint_eigen, src/linalg.rs:153-191).
 //  * electronic energy: tr(H0 P) = sum_i f_i eps_i + sum_mu v_mu (S P)_mu,mu,
 //    which holds exactly for the F that was diagonalised, so P is only formed once
@@ -31,12 +35,15 @@
 namespace gfn1 {
 
 constexpr double kBoltzmann = 3.1668115634556e-6;  // src/constants.rs:26
-constexpr int kVecSlots = 12;                         // N-length scratch vectors per CTA
+constexpr int kVecSlots = 9;                          // N-length vectors kept in shared memory
+constexpr int kBackNB = 16;                           // reflectors per compact-WY block
 
 struct SccShared {
   double red[32];
   double scal[16];
   int iscal[16];
+  double Tm[kBackNB][kBackNB];
+  double VtV[kBackNB][kBackNB];
 };
 
 // Per-stage clock accounting by thread 0 of the CTA (no-op without a buffer).
@@ -60,20 +67,19 @@ struct StageClock {
   }
 };
 
-// Layout of one CTA's workspace slot (doubles).  maxn / maxnsh / cap / maxnat
-// are the batch maxima; matrices use the molecule's own N as leading dimension.
+// Layout of one CTA's global workspace slot (doubles).
 struct CtaWs {
-  double *L, *Li, *Hp, *A, *Z, *C, *D, *iw, *vec;
+  double *L, *Li, *Hp, *A, *Z, *C, *D, *iw, *W1, *W2;
   double *df, *u, *dots, *omega, *beta, *cvec, *qin, *qout, *vsh, *qlast, *dqlast, *qnext, *vout, *qat;
 };
 __host__ __device__ inline long long cta_ws_size(int maxn, int maxnsh, int cap, int maxnat) {
-  const long long n2 = (long long)maxn * maxn;
-  return 12 * n2 + (long long)kVecSlots * maxn + 2LL * cap * maxnsh + 2LL * cap * cap + 2LL * cap +
-         8LL * maxnsh + maxnat + 64;
+  const long long n2 = (long long)maxn * (maxn + 1);
+  return 12 * n2 + 2LL * kBackNB * maxn + 2LL * cap * maxnsh + 2LL * cap * cap + 2LL * cap + 8LL * maxnsh + maxnat +
+         64;
 }
 __device__ __forceinline__ CtaWs cta_ws(double* base, int maxn, int maxnsh, int cap) {
   CtaWs w;
-  const long long n2 = (long long)maxn * maxn;
+  const long long n2 = (long long)maxn * (maxn + 1);
   w.L = base;
   w.Li = w.L + n2;
   w.Hp = w.Li + n2;
@@ -82,8 +88,9 @@ __device__ __forceinline__ CtaWs cta_ws(double* base, int maxn, int maxnsh, int 
   w.C = w.Z + n2;
   w.D = w.C + n2;
   w.iw = w.D + n2;  // 5 * n2
-  w.vec = w.iw + 5 * n2;
-  w.df = w.vec + (long long)kVecSlots * maxn;
+  w.W1 = w.iw + 5 * n2;
+  w.W2 = w.W1 + (long long)kBackNB * maxn;
+  w.df = w.W2 + (long long)kBackNB * maxn;
   w.u = w.df + (long long)cap * maxnsh;
   w.dots = w.u + (long long)cap * maxnsh;
   w.beta = w.dots + (long long)cap * cap;
@@ -100,17 +107,77 @@ __device__ __forceinline__ CtaWs cta_ws(double* base, int maxn, int maxnsh, int 
   return w;
 }
 
-// Sturm count: number of eigenvalues of the symmetric tridiagonal (d, e2 = e^2)
-// that are <= x (LAPACK dlaebz convention with the pivmin guard).
-__device__ __forceinline__ int sturm_count(const double* d, const double* e2, int n, double x, double pivmin) {
-  double q = d[0] - x;
-  if (fabs(q) < pivmin) q = -pivmin;
-  int c = q <= 0.0;
-  for (int i = 1; i < n; ++i) {
-    q = d[i] - x - e2[i - 1] / q;
-    if (fabs(q) < pivmin) q = -pivmin;
-    c += q <= 0.0;
+__host__ __device__ inline int scc_ints(int maxnsh, int maxn, int maxnat) {
+  return 3 * maxnsh + maxn + maxnat + 1;
+}
+__host__ __device__ inline size_t scc_smem_fixed(int maxnsh, int maxn, int maxnat) {
+  const size_t ib = ((size_t)4 * scc_ints(maxnsh, maxn, maxnat) + 15) & ~(size_t)15;
+  return ib + sizeof(double) * kVecSlots * (size_t)maxn;
+}
+// Odd leading dimension of the working matrix: strided column accesses then
+// spread over the shared-memory banks.
+__host__ __device__ inline int work_lda(int n) { return (n & 1) ? n : n + 1; }
+
+// Sturm count and characteristic polynomial at x for the symmetric tridiagonal
+// (d, esq = e^2): returns #eigenvalues <= x and the values p, p', p'' of
+// p_n(x) = det(T - x I) up to one common positive factor.  The recurrence
+//   p_i = (d_i - x) p_{i-1} - e_{i-1}^2 p_{i-2}
+// is LAPACK dlaebz's ratio recurrence q_i = p_i / p_{i-1} multiplied through by
+// p_{i-1}, so the count (the number of negative q_i) is the same but the loop
+// needs no division.  The pair (p_i, p_{i-1}) and its derivatives are rescaled
+// by an exact power of two every 4 steps.  The pivot guard |q_i| < pivmin sets
+// q_i = -2^-600 (LAPACK: -pivmin; the two differ only when e_i^2 < 2^-600 |d_i -
+// x|, an exact split) and moves the pair to a scale where |p_i| is near 1.  The
+// derivatives may overflow; they only steer the Laguerre step.
+__device__ __forceinline__ double pow2_inv_scale(double m) {  // 2^-floor(log2 m), clamped to 2^+-1000
+  const long long ex = ((__double_as_longlong(m) >> 52) & 0x7ff) - 1023;
+  const long long sc = 1023 - (ex < -1000 ? -1000 : (ex > 1000 ? 1000 : ex));
+  return __longlong_as_double(sc << 52);
+}
+__device__ __forceinline__ int sturm_poly(const double* d, const double* esq, int n, double x, double pivmin,
+                                          double& pout, double& dpout, double& ddpout) {
+  constexpr double kGuardScale = 0x1p600;
+  double pm = 1.0, p = d[0] - x, dpm = 0.0, dp = -1.0, ddpm = 0.0, ddp = 0.0;
+  if (fabs(p) < pivmin) {
+    p = -1.0;
+    pm = kGuardScale;
+    dp = -kGuardScale;
   }
+  int c = p <= 0.0;
+  for (int i = 1; i < n; ++i) {
+    const double t = d[i] - x, e2 = esq[i - 1];
+    double pn = t * p - e2 * pm;
+    double dpn = t * dp - p - e2 * dpm;
+    double ddpn = t * ddp - 2.0 * dp - e2 * ddpm;
+    if (fabs(pn) <= pivmin * fabs(p)) {
+      const double s = pow2_inv_scale(fabs(p)) * kGuardScale;
+      pn = p * -pow2_inv_scale(fabs(p));
+      p = pn * -kGuardScale;
+      dp *= s;
+      dpn *= s;
+      ddp *= s;
+      ddpn *= s;
+    }
+    c += (pn > 0.0) != (p > 0.0);
+    pm = p;
+    p = pn;
+    dpm = dp;
+    dp = dpn;
+    ddpm = ddp;
+    ddp = ddpn;
+    if ((i & 3) == 0) {
+      const double sc = pow2_inv_scale(fmax(fabs(p), fabs(pm)));
+      p *= sc;
+      pm *= sc;
+      dp *= sc;
+      dpm *= sc;
+      ddp *= sc;
+      ddpm *= sc;
+    }
+  }
+  pout = p;
+  dpout = dp;
+  ddpout = ddp;
   return c;
 }
 
@@ -124,90 +191,474 @@ __device__ __forceinline__ double hash_unit(unsigned a, unsigned b) {
   return (double)(h & 0xFFFFFF) / 16777216.0 - 0.5;
 }
 
-// Solve (T - lam I) y = x by Gaussian elimination with partial pivoting on the
-// tridiagonal matrix; the factors are built on the fly (n steps) in `w`
-// (5 arrays of n).  Tiny pivots are replaced by +-tiny.
-__device__ void tri_factor(const double* d, const double* e, int n, double lam, double tiny, double* w) {
-  double* u0 = w;
-  double* u1 = w + n;
-  double* u2 = w + 2 * n;
-  double* ml = w + 3 * n;
-  double* pv = w + 4 * n;
-  double a = d[0] - lam;            // current pivot-row diagonal
-  double c = n > 1 ? e[0] : 0.0;    // current pivot-row superdiagonal
+// Gaussian elimination with partial pivoting of the tridiagonal T - lam I.
+// The five factor arrays of eigenvector column j are stored interleaved,
+// w[(a * n + i) * ldw + j], so the threads of a warp access consecutive words;
+// the pivots are kept as reciprocals, so the solves only multiply.
+__device__ void tri_factor(const double* d, const double* e, int n, double lam, double tiny, double* w, int ldw) {
+  double a = d[0] - lam;
+  double c = n > 1 ? e[0] : 0.0;
+  const long long s = (long long)n * ldw;
   for (int k = 0; k < n - 1; ++k) {
-    const double b = e[k];               // subdiagonal of row k+1
-    const double an = d[k + 1] - lam;    // diagonal of row k+1
-    const double cn = (k + 1 < n - 1) ? e[k + 1] : 0.0;  // superdiagonal of row k+1
+    const double b = e[k];
+    const double an = d[k + 1] - lam;
+    const double cn = (k + 1 < n - 1) ? e[k + 1] : 0.0;
+    double* wk = w + (long long)k * ldw;
     if (fabs(a) >= fabs(b)) {
       double piv = a;
       if (fabs(piv) < tiny) piv = piv >= 0.0 ? tiny : -tiny;
-      const double mult = b / piv;
-      u0[k] = piv;
-      u1[k] = c;
-      u2[k] = 0.0;
-      ml[k] = mult;
-      pv[k] = 0.0;
-      a = an - mult * c;
+      const double r = 1.0 / piv;
+      wk[0] = r;
+      wk[s] = c;
+      wk[2 * s] = 0.0;
+      wk[3 * s] = b * r;
+      wk[4 * s] = 0.0;
+      a = an - b * r * c;
       c = cn;
     } else {
-      const double mult = a / b;
-      u0[k] = b;
-      u1[k] = an;
-      u2[k] = cn;
-      ml[k] = mult;
-      pv[k] = 1.0;
+      const double r = 1.0 / b;
+      const double mult = a * r;
+      wk[0] = r;
+      wk[s] = an;
+      wk[2 * s] = cn;
+      wk[3 * s] = mult;
+      wk[4 * s] = 1.0;
       a = c - mult * an;
       c = -mult * cn;
     }
   }
   if (fabs(a) < tiny) a = a >= 0.0 ? tiny : -tiny;
-  u0[n - 1] = a;
+  w[(long long)(n - 1) * ldw] = 1.0 / a;
 }
 
-__device__ void tri_solve(const double* w, int n, double* x, long long stride) {
-  const double* u0 = w;
-  const double* u1 = w + n;
-  const double* u2 = w + 2 * n;
-  const double* ml = w + 3 * n;
-  const double* pv = w + 4 * n;
+// Solves (T - lam I) x = b in place with the factors of tri_factor.  The
+// running entries are carried in registers, so the loads of x and of the
+// factors do not wait on the stores of the previous step.
+__device__ void tri_solve(const double* w, int n, int ldw, double* x, long long stride) {
+  const long long s = (long long)n * ldw;
+  double cur = x[0];
   for (int k = 0; k < n - 1; ++k) {
-    double xk = x[k * stride], xk1 = x[(k + 1) * stride];
-    if (pv[k] != 0.0) {
+    const double* wk = w + (long long)k * ldw;
+    double xk = cur, xk1 = x[(k + 1) * stride];
+    if (wk[4 * s] != 0.0) {
       const double t = xk;
       xk = xk1;
       xk1 = t;
     }
-    xk1 -= ml[k] * xk;
+    xk1 -= wk[3 * s] * xk;
     x[k * stride] = xk;
-    x[(k + 1) * stride] = xk1;
+    cur = xk1;
   }
-  x[(n - 1) * stride] /= u0[n - 1];
-  if (n > 1) x[(n - 2) * stride] = (x[(n - 2) * stride] - u1[n - 2] * x[(n - 1) * stride]) / u0[n - 2];
-  for (int k = n - 3; k >= 0; --k)
-    x[k * stride] = (x[k * stride] - u1[k] * x[(k + 1) * stride] - u2[k] * x[(k + 2) * stride]) / u0[k];
+  double x2 = cur * w[(long long)(n - 1) * ldw];  // x[n-1]
+  x[(n - 1) * stride] = x2;
+  if (n == 1) return;
+  const double* w2 = w + (long long)(n - 2) * ldw;
+  double x1 = (x[(n - 2) * stride] - w2[s] * x2) * w2[0];  // x[n-2]
+  x[(n - 2) * stride] = x1;
+  for (int k = n - 3; k >= 0; --k) {
+    const double* wk = w + (long long)k * ldw;
+    const double x0 = (x[k * stride] - wk[s] * x1 - wk[2 * s] * x2) * wk[0];
+    x[k * stride] = x0;
+    x2 = x1;
+    x1 = x0;
+  }
 }
 
-__device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& opt, int m, SccShared& sh,
-                             int* sh_atom, int* sh_k, int* ao_sh, int* atom_sh, int* sh_ao0) {
-  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
+// ---------------------------------------------------------------- stages
+
+// Householder reduction of the symmetric A (full storage, leading dimension lda)
+// to tridiagonal (d, e); reflector k is kept in row k right of the diagonal
+// with its factor in tau[k] (H_k = I - tau_k v v^T).  Two barriers per column:
+// the matrix-vector product and the p.v partial sums, then the rank-2 update,
+// during which warp 0 also forms the norm of the next pivot row.
+template <int NT>
+__device__ void tridiagonalize(double* A, int lda, int N, double* d, double* e, double* tau, double* pvec,
+                               SccShared& sh) {
+  constexpr int NW = NT / 32;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  double part = 0.0;
+  if (N >= 3)
+    for (int j = 1 + tid; j < N; j += NT) part += A[j] * A[j];
+  double xn2 = block_sum(part, sh.red);
+  for (int k = 0; k < N - 2; ++k) {
+    const int m = N - k - 1;
+    double* rowk = A + (long long)k * lda + (k + 1);
+    const double x0 = rowk[0];
+    const double tail = xn2 - x0 * x0;
+    if (tail == 0.0) {  // column already reduced
+      __syncthreads();
+      if (tid == 0) {
+        d[k] = A[(long long)k * lda + k];
+        e[k] = x0;
+        tau[k] = 0.0;
+      }
+      double p2 = 0.0;
+      const double* nrow = A + (long long)(k + 1) * lda;
+      for (int j = k + 2 + tid; j < N; j += NT) p2 += nrow[j] * nrow[j];
+      xn2 = block_sum(p2, sh.red);
+      continue;
+    }
+    const double xn = sqrt(xn2);
+    const double alpha = x0 >= 0.0 ? -xn : xn;
+    const double v0 = x0 - alpha;
+    const double beta = 2.0 / (v0 * v0 + tail);
+    double pv_part = 0.0;
+    for (int i = wid; i < m; i += NW) {
+      const double* brow = A + (long long)(k + 1 + i) * lda + (k + 1);
+      double s = 0.0;
+      for (int j = lane; j < m; j += 32) s += brow[j] * (j == 0 ? v0 : rowk[j]);
+      s = warp_sum(s) * beta;
+      if (lane == 0) {
+        pvec[i] = s;
+        pv_part += s * (i == 0 ? v0 : rowk[i]);
+      }
+    }
+    if (lane == 0) sh.red[wid] = pv_part;
+    __syncthreads();
+    double pv = 0.0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) pv += sh.red[w];
+    const double K = 0.5 * beta * pv;
+    if (tid == 0) {
+      d[k] = A[(long long)k * lda + k];
+      e[k] = alpha;
+      tau[k] = beta;
+      rowk[0] = v0;
+    }
+    double nrm = 0.0;
+    for (int i = wid; i < m; i += NW) {
+      double* brow = A + (long long)(k + 1 + i) * lda + (k + 1);
+      const double vi = (i == 0) ? v0 : rowk[i];
+      const double wi = pvec[i] - K * vi;
+      for (int j = lane; j < m; j += 32) {
+        const double vj = (j == 0) ? v0 : rowk[j];
+        const double wj = pvec[j] - K * vj;
+        const double nb = brow[j] - (vi * wj + wi * vj);
+        brow[j] = nb;
+        if (i == 0 && j >= 1) nrm += nb * nb;
+      }
+    }
+    if (wid == 0) {
+      nrm = warp_sum(nrm);
+      if (lane == 0) sh.scal[3] = nrm;
+    }
+    __syncthreads();
+    xn2 = sh.scal[3];
+  }
+  if (tid == 0) {
+    if (N >= 2) {
+      d[N - 2] = A[(long long)(N - 2) * lda + (N - 2)];
+      e[N - 2] = A[(long long)(N - 1) * lda + (N - 2)];
+      tau[N - 2] = 0.0;
+    }
+    d[N - 1] = A[(long long)(N - 1) * lda + (N - 1)];
+    e[N - 1] = 0.0;
+    tau[N - 1] = 0.0;
+  }
+  __syncthreads();
+}
+
+// Eigenvalues k = 0..nneed-1 and N-1 of the tridiagonal, one thread each.
+// Bisection on the Sturm count until the count at the iterate x says that
+// eigenvalue k is the nearest one above (count k) or below (count k+1); from
+// there Laguerre steps toward it.  For a polynomial with real roots the
+// Laguerre step in a chosen direction lands between x and the adjacent root on
+// that side, so the iterates approach eigenvalue k monotonically and converge
+// cubically (Li & Zeng, "Laguerre's iteration in solving the symmetric
+// tridiagonal eigenproblem - revisited", SIAM J. Sci. Comput. 15, 1994).
+// Every evaluation also tightens the bisection bracket, and a step that leaves
+// it falls back to bisection.
+template <int NT>
+__device__ void eigenvalues(const double* d, const double* esq, int N, int nneed, double gl, double gu,
+                            double pivmin, double atol, double* eps) {
+  const int nlist = (nneed < N) ? nneed + 1 : N;
+  const double dn = (double)N;
+  for (int slot = threadIdx.x; slot < nlist; slot += NT) {
+    const int k = (slot < nneed) ? slot : N - 1;
+    double lo = gl, hi = gu;
+    double x = 0.5 * (lo + hi);
+    for (int it = 0; it < 160; ++it) {
+      double p, dp, ddp;
+      const int c = sturm_poly(d, esq, N, x, pivmin, p, dp, ddp);
+      if (c >= k + 1)
+        hi = x;
+      else
+        lo = x;
+      const double tol = 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)) + atol;
+      if (hi - lo <= tol) {
+        x = 0.5 * (lo + hi);
+        break;
+      }
+      double xn = 0.5 * (lo + hi);
+      if (c == k || c == k + 1) {
+        // u = p/p', w = p p''/p'^2; step = N u / (1 + sigma sqrt((N-1)(N(1-w)-1)))
+        // with sigma chosen so that the step moves toward eigenvalue k.
+        const double u = p / dp;
+        const double w = (p * ddp) / (dp * dp);
+        const double sq = sqrt((dn - 1.0) * (dn * (1.0 - w) - 1.0));
+        const bool up = (c == k);
+        const double sigma = ((u > 0.0) == up) ? -1.0 : 1.0;
+        const double step = dn * u / (1.0 + sigma * sq);
+        const double xt = x - step;
+        // The Newton ratio u points to the nearest eigenvalue: when it points
+        // away from eigenvalue k, x sits next to the neighbour on the other
+        // side, where the Laguerre step is tiny and proves nothing.
+        const bool nearest = up ? (u < 0.0) : (u > 0.0);
+        if (nearest && fabs(step) <= 32.0 * tol) {  // cubic convergence: the step bounds the error
+          x = fmin(fmax(xt, lo), hi);
+          break;
+        }
+        if (xt > lo && xt < hi && (nearest || fabs(step) >= 0.125 * (hi - lo))) xn = xt;
+      }
+      if (xn <= lo || xn >= hi) break;
+      x = xn;
+    }
+    eps[k] = x;
+  }
+  __syncthreads();
+}
+
+// Fermi occupations by bisection to the bracket fixed point (src/electronic.rs:
+// 3853-3921), one warp.  Only eps[0..nneed) and eps[N-1] are known: orbitals in
+// between lie at or above eps[nneed-1]; while a trial mu keeps them beyond the
+// +80 kT clamp each contributes exactly 2/(1+e^80).  When a decision would need
+// them, `ambiguous` is set and the caller computes every eigenvalue.
+__device__ void fermi_warp(const double* eps, int N, int nneed, double nelec, double kt, double* occ, double& mu_out,
+                           double& ts_out, bool& ambiguous) {
+  const int lane = threadIdx.x & 31;
+  ambiguous = false;
+  double mu = 0.0, ts = 0.0;
+  if (kt <= 0.0) {  // aufbau (src/electronic.rs:3830-3851); needs every orbital up to the HOMO
+    double rem = fmax(nelec, 0.0);
+    int homo = 0;
+    for (int i = 0; i < N; ++i) {
+      const double fill = fmin(rem, 2.0);
+      if (lane == 0) occ[i] = fill;
+      rem -= fill;
+      if (fill > 1e-12) homo = i;
+    }
+    if (homo >= nneed && nneed < N) ambiguous = true;
+    mu = eps[homo];
+  } else if (nelec <= 0.0) {
+    for (int i = lane; i < N; i += 32) occ[i] = 0.0;
+    mu = eps[0];
+  } else if (nelec >= 2.0 * N) {
+    for (int i = lane; i < N; i += 32) occ[i] = 2.0;
+    mu = eps[N - 1];
+  } else {
+    const double c80 = 2.0 / (1.0 + exp(80.0));
+    const double cm80 = 2.0 / (1.0 + exp(-80.0));
+    const int nunc = (nneed < N) ? (N - 1 - nneed) : 0;
+    const double etop = eps[nneed - 1];
+    const double ikt = 1.0 / kt;
+    auto fo = [&](double ei, double m) {
+      const double x = (ei - m) * ikt;
+      if (x >= 80.0) return c80;
+      if (x <= -80.0) return cm80;
+      return 2.0 / (1.0 + exp(x));
+    };
+    double lo = eps[0] - 100.0 * kt - 10.0, hi = eps[N - 1] + 100.0 * kt + 10.0;
+    for (int it = 0; it < 200; ++it) {
+      const double mid = 0.5 * (lo + hi);
+      double s = 0.0;
+      for (int i = lane; i < nneed; i += 32) s += fo(eps[i], mid);
+      if (lane == 0 && nneed < N) s += fo(eps[N - 1], mid);
+      s = warp_sum(s);
+      if (nunc > 0) {
+        if ((etop - mid) / kt >= 80.0) s += nunc * c80;
+        else if (s < nelec) {
+          ambiguous = true;
+          break;
+        }
+      }
+      double nlo = lo, nhi = hi;
+      if (s < nelec) nlo = mid;
+      else nhi = mid;
+      if (nlo == lo && nhi == hi) break;
+      lo = nlo;
+      hi = nhi;
+    }
+    mu = 0.5 * (lo + hi);
+    if (!ambiguous && nunc > 0 && !((etop - mu) / kt >= 80.0)) ambiguous = true;
+    if (!ambiguous) {
+      double t = 0.0;
+      for (int i = lane; i < N; i += 32) {
+        const bool known = i < nneed || i == N - 1;
+        const double f = known ? fo(eps[i], mu) : c80;
+        occ[i] = f;
+        const double nn = fmin(1.0 - 1e-16, fmax(1e-16, 0.5 * f));
+        t += 2.0 * kt * (nn * log(nn) + (1.0 - nn) * log(1.0 - nn));
+      }
+      ts = warp_sum(t);
+    }
+  }
+  mu_out = mu;
+  ts_out = ts;
+}
+
+// Finite-temperature occupations (kt > 0, 0 < nelec < 2N) by the whole CTA.
+// The reference bisects [eps_0 - 100 kT - 10, eps_N-1 + 100 kT + 10] on
+// "electron count < nelec" until the bracket stops shrinking
+// (src/electronic.rs:3853-3921); here each round places one trial mu per warp,
+// NW + 1 equal subintervals, and keeps the subinterval where the count crosses
+// nelec, so the bracket converges to the same crossing in log_(NW+1) rounds.
+// Eigenvalues beyond eps[nneed-1] are unknown (apart from eps[N-1]); they are
+// clamped at +80 kT like in fermi_warp, and a trial mu at which they would
+// matter makes the result ambiguous (the caller then computes all of them).
+// Shared scratch: sh.VtV rows 0 and 1.
+template <int NT>
+__device__ void fermi_cta(const double* eps, int N, int nneed, double nelec, double kt, double* occ, SccShared& sh,
+                          double& mu_out, double& ts_out, bool& ambiguous) {
+  constexpr int NW = NT / 32;
+  static_assert(NW <= 16, "one trial point per warp");
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const double c80 = 2.0 / (1.0 + exp(80.0));
+  const double cm80 = 2.0 / (1.0 + exp(-80.0));
+  const int nunc = (nneed < N) ? (N - 1 - nneed) : 0;
+  const double etop = eps[nneed - 1];
+  const double ikt = 1.0 / kt;
+  auto fo = [&](double ei, double m) {
+    const double x = (ei - m) * ikt;
+    if (x >= 80.0) return c80;
+    if (x <= -80.0) return cm80;
+    return 2.0 / (1.0 + exp(x));
+  };
+  double lo = eps[0] - 100.0 * kt - 10.0, hi = eps[N - 1] + 100.0 * kt + 10.0;
+  bool amb = false;
+  for (int round = 0; round < 64; ++round) {
+    const double h = (hi - lo) / (double)(NW + 1);
+    const double mid = fmin(lo + (double)(wid + 1) * h, hi);
+    double sm = 0.0;
+    for (int i = lane; i < nneed; i += 32) sm += fo(eps[i], mid);
+    if (lane == 0 && nneed < N) sm += fo(eps[N - 1], mid);
+    sm = warp_sum(sm);
+    double flag = 0.0;
+    if (nunc > 0) {
+      if ((etop - mid) / kt >= 80.0)
+        sm += nunc * c80;
+      else if (sm < nelec)
+        flag = 1.0;
+    }
+    if (lane == 0) {
+      sh.VtV[0][wid] = sm;
+      sh.VtV[1][wid] = flag;
+    }
+    __syncthreads();
+    int j = NW;
+    for (int q = NW - 1; q >= 0; --q)
+      if (sh.VtV[0][q] >= nelec) j = q;
+    for (int q = 0; q < NW; ++q)
+      if (sh.VtV[1][q] != 0.0) amb = true;
+    const double nlo = (j == 0) ? lo : fmin(lo + (double)j * h, hi);
+    const double nhi = (j == NW) ? hi : fmin(lo + (double)(j + 1) * h, hi);
+    __syncthreads();
+    if (amb || (nlo == lo && nhi == hi)) break;
+    lo = nlo;
+    hi = nhi;
+  }
+  const double mu = 0.5 * (lo + hi);
+  if (!amb && nunc > 0 && !((etop - mu) / kt >= 80.0)) amb = true;
+  double ts = 0.0;
+  if (!amb) {
+    double t = 0.0;
+    for (int i = tid; i < N; i += NT) {
+      const bool known = i < nneed || i == N - 1;
+      const double f = known ? fo(eps[i], mu) : c80;
+      occ[i] = f;
+      const double nn = fmin(1.0 - 1e-16, fmax(1e-16, 0.5 * f));
+      t += 2.0 * kt * (nn * log(nn) + (1.0 - nn) * log(1.0 - nn));
+    }
+    ts = block_sum(t, sh.red);
+  }
+  mu_out = mu;
+  ts_out = ts;
+  ambiguous = amb;
+}
+
+// Z := Q Z for the first ncol columns, Q = H_0 ... H_{N-3}, applied in blocks of
+// kBackNB reflectors as Q_b = I - V T V^T (compact WY, forward direction).
+template <int NT>
+__device__ void back_transform(const double* A, int lda, const double* tau, int N, double* Z, int ldz, int ncol,
+                               double* W1, double* W2, SccShared& sh) {
+  constexpr int NW = NT / 32;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int nref = N - 2;
+  if (nref <= 0 || ncol <= 0) return;
+  for (int kb = ((nref - 1) / kBackNB) * kBackNB; kb >= 0; kb -= kBackNB) {
+    const int nb = min(kBackNB, nref - kb);
+    for (int p = wid; p < nb * nb; p += NW) {
+      const int i = p / nb, j = p % nb;
+      if (i >= j) continue;
+      const double* vi = A + (long long)(kb + i) * lda;
+      const double* vj = A + (long long)(kb + j) * lda;
+      double s = 0.0;
+      for (int r = kb + j + 1 + lane; r < N; r += 32) s += vi[r] * vj[r];
+      s = warp_sum(s);
+      if (lane == 0) sh.VtV[i][j] = s;
+    }
+    __syncthreads();
+    if (wid == 0) {  // T upper triangular: T_jj = tau_j, T[0:j,j] = -tau_j T[0:j,0:j] V^T v_j
+      for (int j = 0; j < nb; ++j) {
+        const double tj = tau[kb + j];
+        if (lane < j) {
+          double s = 0.0;
+          for (int l = lane; l < j; ++l) s += sh.Tm[lane][l] * sh.VtV[l][j];
+          sh.Tm[lane][j] = -tj * s;
+        }
+        if (lane == j) sh.Tm[j][j] = tj;
+        __syncwarp();
+      }
+    }
+    for (int idx = tid; idx < nb * ncol; idx += NT) {
+      const int j = idx / ncol, c = idx - j * ncol;
+      const double* vj = A + (long long)(kb + j) * lda;
+      double s = 0.0;
+      for (int r = kb + j + 1; r < N; ++r) s += vj[r] * Z[(long long)r * ldz + c];
+      W1[j * ncol + c] = s;
+    }
+    __syncthreads();
+    for (int idx = tid; idx < nb * ncol; idx += NT) {
+      const int j = idx / ncol, c = idx - j * ncol;
+      double s = 0.0;
+      for (int l = j; l < nb; ++l) s += sh.Tm[j][l] * W1[l * ncol + c];
+      W2[j * ncol + c] = s;
+    }
+    __syncthreads();
+    for (int idx = tid; idx < (N - kb - 1) * ncol; idx += NT) {
+      const int rr = idx / ncol, c = idx - rr * ncol;
+      const int r = kb + 1 + rr;
+      const int jmax = min(nb, rr + 1);
+      double s = 0.0;
+      for (int j = 0; j < jmax; ++j) s += A[(long long)(kb + j) * lda + r] * W2[j * ncol + c];
+      Z[(long long)r * ldz + c] -= s;
+    }
+    __syncthreads();
+  }
+}
+
+template <int NT>
+__device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& opt, const SccLaunch& SL, int m,
+                             SccShared& sh, int* sh_atom, int* sh_k, int* ao_sh, int* atom_sh, int* sh_ao0,
+                             double* vec, double* As, long long as_cap) {
+  constexpr int NW = NT / 32;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int a0 = B.atom_off[m], nat = B.atom_off[m + 1] - a0;
   const int sh0 = B.shell_off[m], nsh = B.shell_off[m + 1] - sh0;
-  const int ao0 = B.ao_off[m], N = B.ao_off[m + 1] - ao0;
+  const int N = B.ao_off[m + 1] - B.ao_off[m];
   const long long mo = B.mat_off[m];
   const double* S = B.S + mo;
   const double* H0 = B.H0 + mo;
-  CtaWs w = cta_ws(B.ws + (long long)blockIdx.x * B.ws_stride, B.ws_maxn, B.ws_maxnsh, B.ws_cap);
+  CtaWs w = cta_ws(SL.ws + (long long)blockIdx.x * SL.ws_stride, SL.maxn, SL.maxnsh, SL.cap);
   double* L = w.L;
   double* Li = w.Li;
   double* Hp = w.Hp;
-  double* A = w.A;
   double* Z = w.Z;
   double* C = w.C;
   double* D = w.D;
   double* iw = w.iw;
   const double* G = B.gam + B.gam_off[m];
-  double* vec = w.vec;
+  const int lda = work_lda(N);
+  double* A = ((long long)N * lda <= as_cap) ? As : w.A;  // shared memory when it fits
   double* d = vec;
   double* e = vec + N;
   double* tau = vec + 2 * N;
@@ -215,10 +666,9 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
   double* occ = vec + 4 * N;
   double* pop = vec + 5 * N;
   double* vao = vec + 6 * N;
-  double* hv = vec + 7 * N;
-  double* pvec = vec + 8 * N;
-  double* esq = vec + 9 * N;
-  const int cap = B.ws_cap;
+  double* pvec = vec + 7 * N;
+  double* esq = vec + 8 * N;
+  const int cap = SL.cap;
 
   // ---- index tables
   if (tid == 0) {
@@ -242,7 +692,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
 
   StageClock clk(B.stage_cycles);
   // ---- Cholesky S = L L^T (right-looking, in place on L)
-  for (long long i = tid; i < (long long)N * N; i += nt) L[i] = S[i];
+  for (long long i = tid; i < (long long)N * N; i += NT) L[i] = S[i];
   __syncthreads();
   for (int k = 0; k < N; ++k) {
     if (tid == 0) {
@@ -255,9 +705,9 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     }
     __syncthreads();
     const double lkk = sh.scal[0];
-    for (int i = k + 1 + tid; i < N; i += nt) L[(long long)i * N + k] /= lkk;
+    for (int i = k + 1 + tid; i < N; i += NT) L[(long long)i * N + k] /= lkk;
     __syncthreads();
-    for (int i = k + 1 + wid; i < N; i += nw) {
+    for (int i = k + 1 + wid; i < N; i += NW) {
       const double lik = L[(long long)i * N + k];
       for (int j = k + 1 + lane; j <= i; j += 32) L[(long long)i * N + j] -= lik * L[(long long)j * N + k];
     }
@@ -270,11 +720,11 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     }
     return;
   }
-  for (int i = wid; i < N; i += nw)
+  for (int i = wid; i < N; i += NW)
     for (int j = i + 1 + lane; j < N; j += 32) L[(long long)i * N + j] = 0.0;
   __syncthreads();
   // L^-1, one thread per column
-  for (int j = tid; j < N; j += nt) {
+  for (int j = tid; j < N; j += NT) {
     for (int i = 0; i < j; ++i) Li[(long long)i * N + j] = 0.0;
     Li[(long long)j * N + j] = 1.0 / L[(long long)j * N + j];
     for (int i = j + 1; i < N; ++i) {
@@ -284,50 +734,53 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     }
   }
   __syncthreads();
-  // H0' = L^-1 H0 L^-T: T = H0 L^-T into A, then H0' = L^-1 T
-  for (int i = wid; i < N; i += nw)
+  // H0' = L^-1 H0 L^-T: T = H0 L^-T into the global work matrix, then H0' = L^-1 T
+  double* T = w.A;
+  for (int i = wid; i < N; i += NW)
     for (int j = lane; j < N; j += 32) {
       double s = 0.0;
       for (int k = 0; k <= j; ++k) s += H0[(long long)i * N + k] * Li[(long long)j * N + k];
-      A[(long long)i * N + j] = s;
+      T[(long long)i * N + j] = s;
     }
   __syncthreads();
-  for (int i = wid; i < N; i += nw)
+  for (int i = wid; i < N; i += NW)
     for (int j = lane; j <= i; j += 32) {
       double s = 0.0;
-      for (int k = 0; k <= i; ++k) s += Li[(long long)i * N + k] * A[(long long)k * N + j];
+      for (int k = 0; k <= i; ++k) s += Li[(long long)i * N + k] * T[(long long)k * N + j];
       Hp[(long long)i * N + j] = s;
     }
   __syncthreads();
-  for (int i = wid; i < N; i += nw)
+  for (int i = wid; i < N; i += NW)
     for (int j = i + 1 + lane; j < N; j += 32) Hp[(long long)i * N + j] = Hp[(long long)j * N + i];
 
-  clk.mark(kStPrologue);
   // ---- SCC state
   double nref = 0.0;
   for (int s = 0; s < nsh; ++s) nref += M.elem[B.z[a0 + sh_atom[s]]].refocc[sh_k[s]];
   const double nelec = nref - B.charge[m];
   const double kt = fmax(opt.etemp, 0.0) * kBoltzmann;
-  for (int s = tid; s < nsh; s += nt) w.qin[s] = B.init_q ? B.init_q[sh0 + s] : 0.0;
+  for (int s = tid; s < nsh; s += NT) w.qin[s] = B.init_q ? B.init_q[sh0 + s] : 0.0;
   const double mixing = fmin(1.0, fmax(0.01, opt.mixing));
   const int memory = max(opt.broyden_size, 2);
+  const int nneed0 = min(N, max(1, (int)ceil(0.5 * nelec) + 8));
   int bro_iter = 0;
   double last_e = 0.0;
   bool have_e = false;
   bool converged = false;
   int iter = 0;
+  int nocc = 0;
   double e_el = 0.0, e2 = 0.0, e3 = 0.0, ts = 0.0, mu = 0.0, rms = 0.0;
   __syncthreads();
+  clk.mark(kStPrologue);
 
   for (iter = 1; iter <= opt.max_scc; ++iter) {
     // (1) shell potential from the input charges (src/coulomb.rs:140-193)
-    for (int a = tid; a < nat; a += nt) {
+    for (int a = tid; a < nat; a += NT) {
       double q = 0.0;
       for (int s = atom_sh[a]; s < atom_sh[a + 1]; ++s) q += w.qin[s];
       w.qat[a] = q;
     }
     __syncthreads();
-    for (int i = tid; i < nsh; i += nt) {
+    for (int i = tid; i < nsh; i += NT) {
       double v = 0.0;
       for (int j = 0; j < nsh; ++j) v += G[(long long)i * nsh + j] * w.qin[j];
       const int a = sh_atom[i];
@@ -336,88 +789,43 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
       w.vsh[i] = v;
     }
     __syncthreads();
-    for (int i = tid; i < N; i += nt) vao[i] = w.vsh[ao_sh[i]];
+    for (int i = tid; i < N; i += NT) vao[i] = w.vsh[ao_sh[i]];
     __syncthreads();
-    // (2) F' = H0' - 1/2 (M + M^T), M = L^-1 diag(v) L, full symmetric storage in A
-    for (int i = wid; i < N; i += nw)
-      for (int j = lane; j <= i; j += 32) {
-        double s = 0.0;
-        for (int k = j; k <= i; ++k) s += Li[(long long)i * N + k] * vao[k] * L[(long long)k * N + j];
-        const double f = Hp[(long long)i * N + j] - (i == j ? s : 0.5 * s);
-        A[(long long)i * N + j] = f;
-        A[(long long)j * N + i] = f;
+    // (2) F' = H0' - 1/2 (M + M^T), M = L^-1 diag(v) L; warps own 4-row groups,
+    //     lanes 32 columns; L rows are read coalesced, L^-1 entries broadcast
+    for (int rg = wid; rg * 4 < N; rg += NW) {
+      const int i0 = rg * 4;
+      const int imax = min(i0 + 3, N - 1);
+      for (int j0 = 0; j0 <= imax; j0 += 32) {
+        const int j = j0 + lane;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        for (int k = j0; k <= imax; ++k) {
+          const double lkj = (k >= j && j < N) ? L[(long long)k * N + j] * vao[k] : 0.0;
+          s0 += Li[(long long)i0 * N + k] * lkj;
+          if (i0 + 1 <= imax) s1 += Li[(long long)(i0 + 1) * N + k] * lkj;
+          if (i0 + 2 <= imax) s2 += Li[(long long)(i0 + 2) * N + k] * lkj;
+          if (i0 + 3 <= imax) s3 += Li[(long long)(i0 + 3) * N + k] * lkj;
+        }
+        const double sr[4] = {s0, s1, s2, s3};
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int i = i0 + r;
+          if (i <= imax && j <= i) {
+            const double f = Hp[(long long)i * N + j] - (i == j ? sr[r] : 0.5 * sr[r]);
+            A[(long long)i * lda + j] = f;
+            A[(long long)j * lda + i] = f;
+          }
+        }
       }
+    }
     __syncthreads();
     clk.mark(kStFock);
-    // (3) Householder tridiagonalisation; v_k kept in row k right of the diagonal
-    for (int k = 0; k < N - 2; ++k) {
-      const int mlen = N - k - 1;
-      double* rowk = A + (long long)k * N + (k + 1);
-      double part = 0.0;
-      for (int i = tid; i < mlen; i += nt) part += rowk[i] * rowk[i];
-      const double xn2 = block_sum(part, sh.red);
-      const double x0 = rowk[0];
-      const double tail = xn2 - x0 * x0;
-      if (tail == 0.0) {
-        if (tid == 0) {
-          d[k] = A[(long long)k * N + k];
-          e[k] = x0;
-          tau[k] = 0.0;
-        }
-        __syncthreads();
-        continue;
-      }
-      const double xn = sqrt(xn2);
-      const double alpha = x0 >= 0.0 ? -xn : xn;
-      const double v0 = x0 - alpha;
-      const double beta = 2.0 / (v0 * v0 + tail);
-      for (int i = tid; i < mlen; i += nt) hv[i] = (i == 0) ? v0 : rowk[i];
-      __syncthreads();
-      if (tid == 0) {
-        d[k] = A[(long long)k * N + k];
-        e[k] = alpha;
-        tau[k] = beta;
-        rowk[0] = v0;
-      }
-      // p = beta * B v
-      double pv_part = 0.0;
-      for (int i = wid; i < mlen; i += nw) {
-        const double* brow = A + (long long)(k + 1 + i) * N + (k + 1);
-        double s = 0.0;
-        for (int j = lane; j < mlen; j += 32) s += brow[j] * hv[j];
-        s = warp_sum(s) * beta;
-        if (lane == 0) {
-          pvec[i] = s;
-          pv_part += s * hv[i];
-        }
-      }
-      const double pv = block_sum(pv_part, sh.red);
-      const double K = 0.5 * beta * pv;
-      for (int i = wid; i < mlen; i += nw) {
-        double* brow = A + (long long)(k + 1 + i) * N + (k + 1);
-        const double vi = hv[i], wi = pvec[i] - K * vi;
-        for (int j = lane; j < mlen; j += 32) {
-          const double vj = hv[j], wj = pvec[j] - K * vj;
-          brow[j] -= vi * wj + wi * vj;
-        }
-      }
-      __syncthreads();
-    }
-    if (tid == 0) {
-      if (N >= 2) {
-        d[N - 2] = A[(long long)(N - 2) * N + (N - 2)];
-        e[N - 2] = A[(long long)(N - 1) * N + (N - 2)];
-        tau[N - 2] = 0.0;
-      }
-      d[N - 1] = A[(long long)(N - 1) * N + (N - 1)];
-      e[N - 1] = 0.0;
-      tau[N - 1] = 0.0;
-    }
-    __syncthreads();
+    // (3) Householder tridiagonalisation
+    tridiagonalize<NT>(A, lda, N, d, e, tau, pvec, sh);
     clk.mark(kStTridiag);
-    // (4) eigenvalues by bisection
+    // (4) eigenvalues needed by the occupations
     double gl = INFINITY, gu = -INFINITY, onenrm = 0.0, emax2 = 0.0;
-    for (int i = tid; i < N; i += nt) {
+    for (int i = tid; i < N; i += NT) {
       const double off = (i > 0 ? fabs(e[i - 1]) : 0.0) + (i < N - 1 ? fabs(e[i]) : 0.0);
       gl = fmin(gl, d[i] - off);
       gu = fmax(gu, d[i] + off);
@@ -437,96 +845,63 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
       gl -= 2.1 * DBL_EPSILON * fabs(gl) + 4.0 * DBL_EPSILON * span + pivmin;
       gu += 2.1 * DBL_EPSILON * fabs(gu) + 4.0 * DBL_EPSILON * span + pivmin;
     }
-    for (int k = tid; k < N; k += nt) {
-      double lo = gl, hi = gu;
-      for (int it = 0; it < 128; ++it) {
-        const double mid = 0.5 * (lo + hi);
-        if (mid <= lo || mid >= hi) break;
-        if (sturm_count(d, esq, N, mid, pivmin) >= k + 1) hi = mid;
-        else lo = mid;
+    int nneed = nneed0;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      eigenvalues<NT>(d, esq, N, nneed, gl, gu, pivmin, 4.0 * DBL_EPSILON * onenrm, eps);
+      clk.mark(kStEigval);
+      // (5) occupations (src/electronic.rs:3815-3921)
+      if (kt > 0.0 && nelec > 0.0 && nelec < 2.0 * N) {
+        double fm, ft;
+        bool amb;
+        fermi_cta<NT>(eps, N, nneed, nelec, kt, occ, sh, fm, ft, amb);
+        if (tid == 0) {
+          sh.scal[1] = fm;
+          sh.scal[2] = ft;
+          sh.iscal[2] = amb ? 1 : 0;
+        }
+      } else if (wid == 0) {  // aufbau and the empty / full limits
+        double fm, ft;
+        bool amb;
+        fermi_warp(eps, N, nneed, nelec, kt, occ, fm, ft, amb);
+        if (lane == 0) {
+          sh.scal[1] = fm;
+          sh.scal[2] = ft;
+          sh.iscal[2] = amb ? 1 : 0;
+        }
       }
-      eps[k] = 0.5 * (lo + hi);
+      __syncthreads();
+      clk.mark(kStFermi);
+      if (!sh.iscal[2] || nneed == N) break;
+      nneed = N;
     }
-    __syncthreads();
-    clk.mark(kStEigval);
-    // (5) occupations (src/electronic.rs:3815-3921), warp 0
-    if (wid == 0) {
-      double f_mu = 0.0, f_ts = 0.0;
-      if (kt <= 0.0) {
-        double rem = fmax(nelec, 0.0);
-        int homo = 0;
-        for (int i = 0; i < N; ++i) {
-          const double fill = fmin(rem, 2.0);
-          if (lane == 0) occ[i] = fill;
-          rem -= fill;
-          if (fill > 1e-12) homo = i;
-        }
-        f_mu = eps[homo];
-      } else if (nelec <= 0.0) {
-        for (int i = lane; i < N; i += 32) occ[i] = 0.0;
-        f_mu = eps[0];
-      } else if (nelec >= 2.0 * N) {
-        for (int i = lane; i < N; i += 32) occ[i] = 2.0;
-        f_mu = eps[N - 1];
-      } else {
-        double lo = eps[0] - 100.0 * kt - 10.0, hi = eps[N - 1] + 100.0 * kt + 10.0;
-        for (int it = 0; it < 200; ++it) {
-          const double mid = 0.5 * (lo + hi);
-          double s = 0.0;
-          for (int i = lane; i < N; i += 32) s += 2.0 / (1.0 + exp(fmin(80.0, fmax(-80.0, (eps[i] - mid) / kt))));
-          s = warp_sum(s);
-          double nlo = lo, nhi = hi;
-          if (s < nelec) nlo = mid;
-          else nhi = mid;
-          if (nlo == lo && nhi == hi) break;
-          lo = nlo;
-          hi = nhi;
-        }
-        f_mu = 0.5 * (lo + hi);
-        double t = 0.0;
-        for (int i = lane; i < N; i += 32) {
-          const double f = 2.0 / (1.0 + exp(fmin(80.0, fmax(-80.0, (eps[i] - f_mu) / kt))));
-          occ[i] = f;
-          const double nn = fmin(1.0 - 1e-16, fmax(1e-16, 0.5 * f));
-          t += 2.0 * kt * (nn * log(nn) + (1.0 - nn) * log(1.0 - nn));
-        }
-        f_ts = warp_sum(t);
-      }
-      if (lane == 0) {
-        sh.scal[1] = f_mu;
-        sh.scal[2] = f_ts;
-      }
-    }
-    __syncthreads();
     mu = sh.scal[1];
     ts = sh.scal[2];
     // number of orbitals whose occupation matters at FP64 resolution
     int nocc_loc = 0;
-    for (int i = tid; i < N; i += nt)
-      if (occ[i] > 1e-30) nocc_loc = max(nocc_loc, i + 1);
-    const int nocc = (int)block_max((double)nocc_loc, sh.red);
-    clk.mark(kStFermi);
+    for (int i = tid; i < N; i += NT)
+      if ((i < nneed || i == N - 1) && occ[i] > 1e-30) nocc_loc = max(nocc_loc, i + 1);
+    nocc = (int)block_max((double)nocc_loc, sh.red);
     // (6) inverse iteration for the occupied eigenvectors (columns of Z)
     const double ortol = 1e-5 * onenrm;
     const double tiny = DBL_EPSILON * fmax(onenrm, 1e-300);
-    for (int j = tid; j < nocc; j += nt) {
+    for (int j = tid; j < nocc; j += NT) {
       const bool start = (j == 0) || (eps[j] - eps[j - 1] > ortol);
       if (!start) continue;
       int jend = j + 1;
       while (jend < nocc && eps[jend] - eps[jend - 1] <= ortol) ++jend;
-      double* ws = iw + (long long)5 * N * j;
+      double* ws = iw + j;  // column j of the interleaved factor arrays
       double lam_prev = -INFINITY;
       for (int jj = j; jj < jend; ++jj) {
         double lam = eps[jj];
         const double pert = 10.0 * DBL_EPSILON * fmax(fabs(lam), onenrm);
         if (jj > j && lam - lam_prev < pert) lam = lam_prev + pert;
         lam_prev = lam;
-        tri_factor(d, e, N, lam, tiny, ws);
+        tri_factor(d, e, N, lam, tiny, ws, N);
         double* x = Z + jj;  // column jj, stride N
         for (int i = 0; i < N; ++i) x[(long long)i * N] = hash_unit(i, jj) + 1e-3;
-        const int nit = (jend - j > 1) ? 5 : 3;
+        const int nit = (jend - j > 1) ? 4 : 2;
         for (int it = 0; it < nit; ++it) {
-          tri_solve(ws, N, x, N);
+          tri_solve(ws, N, N, x, N);
           for (int q = j; q < jj; ++q) {  // modified Gram-Schmidt inside the cluster
             double dot = 0.0;
             for (int i = 0; i < N; ++i) dot += Z[(long long)i * N + q] * x[(long long)i * N];
@@ -541,38 +916,49 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     }
     __syncthreads();
     clk.mark(kStInvIter);
-    // (7) back-transformation Z := Q Z, one thread per eigenvector column
-    for (int j = tid; j < nocc; j += nt) {
-      for (int k = N - 3; k >= 0; --k) {
-        const double tk = tau[k];
-        if (tk == 0.0) continue;
-        const double* v = A + (long long)k * N + (k + 1);
-        double s = 0.0;
-        for (int i = 0; i < N - k - 1; ++i) s += v[i] * Z[(long long)(k + 1 + i) * N + j];
-        s *= tk;
-        for (int i = 0; i < N - k - 1; ++i) Z[(long long)(k + 1 + i) * N + j] -= s * v[i];
-      }
-    }
-    __syncthreads();
+    // (7) back-transformation Z := Q Z
+    back_transform<NT>(A, lda, tau, N, Z, N, nocc, w.W1, w.W2, sh);
     clk.mark(kStBackTr);
-    // (8) C = L^-T Z, D = L Z and the AO populations (S P)_mu,mu
-    for (int mu_ = wid; mu_ < N; mu_ += nw) {
-      double popp = 0.0;
-      for (int i = lane; i < nocc; i += 32) {
-        double c = 0.0, dd = 0.0;
-        for (int k = mu_; k < N; ++k) c += Li[(long long)k * N + mu_] * Z[(long long)k * N + i];
-        for (int k = 0; k <= mu_; ++k) dd += L[(long long)mu_ * N + k] * Z[(long long)k * N + i];
-        C[(long long)mu_ * N + i] = c;
-        D[(long long)mu_ * N + i] = dd;
-        popp += occ[i] * c * dd;
+    // (8) C = L^-T Z, D = L Z and the AO populations (S P)_mu,mu; warps own
+    //     4-row groups, lanes eigenvectors
+    for (int rg = wid; rg * 4 < N; rg += NW) {
+      const int m0 = rg * 4;
+      const int mmax = min(m0 + 3, N - 1);
+      double pp[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int i0 = 0; i0 < nocc; i0 += 32) {
+        const int i = i0 + lane;
+        if (i < nocc) {
+          double c[4] = {0.0, 0.0, 0.0, 0.0}, dd[4] = {0.0, 0.0, 0.0, 0.0};
+          for (int k = 0; k < N; ++k) {
+            const double z = Z[(long long)k * N + i];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+              const int mu_ = min(m0 + r, mmax);
+              c[r] += Li[(long long)k * N + mu_] * z;  // zero for k < mu
+              dd[r] += L[(long long)mu_ * N + k] * z;  // zero for k > mu
+            }
+          }
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const int mu_ = m0 + r;
+            if (mu_ <= mmax) {
+              C[(long long)mu_ * N + i] = c[r];
+              D[(long long)mu_ * N + i] = dd[r];
+              pp[r] += occ[i] * c[r] * dd[r];
+            }
+          }
+        }
       }
-      popp = warp_sum(popp);
-      if (lane == 0) pop[mu_] = popp;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const double s = warp_sum(pp[r]);
+        if (lane == 0 && m0 + r <= mmax) pop[m0 + r] = s;
+      }
     }
     __syncthreads();
     clk.mark(kStPop);
     // (9) output charges, energies (src/electronic.rs:2173-2191)
-    for (int s = tid; s < nsh; s += nt) {
+    for (int s = tid; s < nsh; s += NT) {
       const ElemTable& el = M.elem[B.z[a0 + sh_atom[s]]];
       const int k = sh_k[s];
       double p = 0.0;
@@ -580,16 +966,16 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
       w.qout[s] = el.refocc[k] - p;
     }
     double part = 0.0;
-    for (int i = tid; i < N; i += nt) part += occ[i] * eps[i] + vao[i] * pop[i];
+    for (int i = tid; i < N; i += NT) part += (i < nocc ? occ[i] * eps[i] : 0.0) + vao[i] * pop[i];
     e_el = block_sum(part, sh.red);
-    for (int a = tid; a < nat; a += nt) {
+    for (int a = tid; a < nat; a += NT) {
       double q = 0.0;
       for (int s = atom_sh[a]; s < atom_sh[a + 1]; ++s) q += w.qout[s];
       w.qat[a] = q;
     }
     __syncthreads();
     double p2 = 0.0, p3 = 0.0, pr = 0.0;
-    for (int i = tid; i < nsh; i += nt) {
+    for (int i = tid; i < nsh; i += NT) {
       double v = 0.0;
       for (int j = 0; j < nsh; ++j) v += G[(long long)i * nsh + j] * w.qout[j];
       p2 += w.qout[i] * v;
@@ -600,7 +986,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
       const double r = w.qout[i] - w.qin[i];
       pr += r * r;
     }
-    for (int a = tid; a < nat; a += nt) {
+    for (int a = tid; a < nat; a += NT) {
       const double qa = w.qat[a];
       p3 += qa * qa * qa * M.elem[B.z[a0 + a]].gam3 / 3.0;
     }
@@ -619,7 +1005,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     if (opt.broyden) {
       bro_iter += 1;
       if (bro_iter == 1) {
-        for (int s = tid; s < nsh; s += nt) {
+        for (int s = tid; s < nsh; s += NT) {
           const double r = w.qout[s] - w.qin[s];
           w.dqlast[s] = r;
           w.qlast[s] = w.qin[s];
@@ -632,7 +1018,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
         const int it1 = (itn - 1) % memory;
         const int slot = it1 % cap;
         double pn = 0.0, pd = 0.0;
-        for (int s = tid; s < nsh; s += nt) {
+        for (int s = tid; s < nsh; s += NT) {
           const double r = w.qout[s] - w.qin[s];
           pn += r * r;
           const double dfv = r - w.dqlast[s];
@@ -643,7 +1029,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
         const double inv = 1.0 / fmax(dfn, DBL_EPSILON);
         double* dfs = w.df + (long long)slot * nsh;
         double* us = w.u + (long long)slot * nsh;
-        for (int s = tid; s < nsh; s += nt) {
+        for (int s = tid; s < nsh; s += NT) {
           const double r = w.qout[s] - w.qin[s];
           const double dfv = (r - w.dqlast[s]) * inv;
           dfs[s] = dfv;
@@ -658,7 +1044,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
         const int start = itn > memory ? itn - memory + 1 : 1;
         const int mact = itn - start + 1;
         // dot products df_new . df_j for every active slot, and c_j = omega_j df_j . dq
-        for (int r = wid; r < mact; r += nw) {
+        for (int r = wid; r < mact; r += NW) {
           const int sj = ((start + r - 1) % memory) % cap;
           const double* dj = w.df + (long long)sj * nsh;
           double s1 = 0.0, s2 = 0.0;
@@ -675,14 +1061,14 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
           }
         }
         __syncthreads();
-        for (int idx = tid; idx < mact * mact; idx += nt) {
+        for (int idx = tid; idx < mact * mact; idx += NT) {
           const int r = idx / mact, c = idx % mact;
           const int si = ((start + r - 1) % memory) % cap, sj = ((start + c - 1) % memory) % cap;
           double b = w.omega[si] * w.omega[sj] * w.dots[(long long)si * cap + sj];
           if (r == c) b += 0.01 * 0.01;
           w.beta[(long long)r * mact + c] = b;
         }
-        for (int r = tid; r < mact; r += nt) {
+        for (int r = tid; r < mact; r += NT) {
           const int si = ((start + r - 1) % memory) % cap;
           w.cvec[r] *= w.omega[si];
         }
@@ -709,7 +1095,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
             break;
           }
           if (piv != col) {
-            for (int j = tid; j < mact; j += nt) {
+            for (int j = tid; j < mact; j += NT) {
               const double t = w.beta[(long long)piv * mact + j];
               w.beta[(long long)piv * mact + j] = w.beta[(long long)col * mact + j];
               w.beta[(long long)col * mact + j] = t;
@@ -723,28 +1109,28 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
           }
           const double dg = w.beta[(long long)col * mact + col];
           __syncthreads();
-          for (int j = col + tid; j < mact; j += nt) w.beta[(long long)col * mact + j] /= dg;
+          for (int j = col + tid; j < mact; j += NT) w.beta[(long long)col * mact + j] /= dg;
           if (tid == 0) w.cvec[col] /= dg;
           __syncthreads();
-          for (int idx = tid; idx < mact * (mact - col); idx += nt) {
+          for (int idx = tid; idx < mact * (mact - col); idx += NT) {
             const int r = idx / (mact - col), j = col + idx % (mact - col);
             if (r == col) continue;
             const double f = w.beta[(long long)r * mact + col];
             if (f == 0.0 || j == col) continue;
             w.beta[(long long)r * mact + j] -= f * w.beta[(long long)col * mact + j];
           }
-          for (int r = tid; r < mact; r += nt) {
+          for (int r = tid; r < mact; r += NT) {
             if (r == col) continue;
             const double f = w.beta[(long long)r * mact + col];
             if (f != 0.0) w.cvec[r] -= f * w.cvec[col];
           }
           __syncthreads();
-          for (int r = tid; r < mact; r += nt)
+          for (int r = tid; r < mact; r += NT)
             if (r != col) w.beta[(long long)r * mact + col] = 0.0;
           __syncthreads();
         }
         if (ok) {
-          for (int s = tid; s < nsh; s += nt) {
+          for (int s = tid; s < nsh; s += NT) {
             const double r = w.qout[s] - w.qin[s];
             double qn = w.qin[s] + mixing * r;
             for (int rr = 0; rr < mact; ++rr) {
@@ -761,15 +1147,15 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
       }
       if (have_next) {  // trusted_charge_vector (src/electronic.rs:3759-3761)
         int bad = 0;
-        for (int s = tid; s < nsh; s += nt)
+        for (int s = tid; s < nsh; s += NT)
           if (!isfinite(w.qnext[s]) || fabs(w.qnext[s]) >= 10.0) bad = 1;
         if (block_max((double)bad, sh.red) > 0.0) have_next = false;
       }
     }
     if (!have_next)
-      for (int s = tid; s < nsh; s += nt) w.qnext[s] = w.qin[s] + mixing * (w.qout[s] - w.qin[s]);
+      for (int s = tid; s < nsh; s += NT) w.qnext[s] = w.qin[s] + mixing * (w.qout[s] - w.qin[s]);
     __syncthreads();
-    for (int s = tid; s < nsh; s += nt) w.qin[s] = w.qnext[s];
+    for (int s = tid; s < nsh; s += NT) w.qin[s] = w.qnext[s];
     last_e = escc;
     have_e = true;
     __syncthreads();
@@ -801,17 +1187,14 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     B.dipole[3 * m + 1] = dy;
     B.dipole[3 * m + 2] = dz;
   }
-  for (int s = tid; s < nsh; s += nt) {
+  for (int s = tid; s < nsh; s += NT) {
     B.shell_q[sh0 + s] = w.qout[s];
     B.shell_pot[sh0 + s] = w.vout[s];
   }
-  for (int a = tid; a < nat; a += nt) B.atom_q[a0 + a] = w.qat[a];
+  for (int a = tid; a < nat; a += NT) B.atom_q[a0 + a] = w.qat[a];
   // density and energy-weighted density of the last diagonalisation
   // (src/linalg.rs:243-273), kept per molecule for the gradient kernel
-  int nocc = 0;
-  for (int i = 0; i < N; ++i)
-    if (occ[i] > 1e-30) nocc = i + 1;
-  for (int i = wid; i < N; i += nw)
+  for (int i = wid; i < N; i += NW)
     for (int j = lane; j <= i; j += 32) {
       double p = 0.0, q = 0.0;
       for (int k = 0; k < nocc; ++k) {
@@ -828,29 +1211,70 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
   clk.mark(kStFinal);
 }
 
-__global__ void __launch_bounds__(256) scc_kernel(Batch B, Model M, SccOptions opt, int max_nsh, int max_n) {
-  extern __shared__ int sm_int[];
+template <int NT>
+__global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) scc_kernel(Batch B, Model M, SccOptions opt, SccLaunch SL) {
+  extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ SccShared sh;
   __shared__ int next;
-  int* sh_atom = sm_int;
-  int* sh_k = sh_atom + max_nsh;
-  int* sh_ao0 = sh_k + max_nsh;
-  int* ao_sh = sh_ao0 + max_nsh;
-  int* atom_sh = ao_sh + max_n;  // max_nat + 1
+  int* sh_atom = (int*)smraw;
+  int* sh_k = sh_atom + SL.maxnsh;
+  int* sh_ao0 = sh_k + SL.maxnsh;
+  int* ao_sh = sh_ao0 + SL.maxnsh;
+  int* atom_sh = ao_sh + SL.maxn;  // maxnat + 1
+  const size_t ib = ((size_t)4 * scc_ints(SL.maxnsh, SL.maxn, SL.maxnat) + 15) & ~(size_t)15;
+  double* vec = (double*)(smraw + ib);
+  double* As = vec + (size_t)kVecSlots * SL.maxn;
+  const long long as_cap = ((long long)SL.smem_bytes - (long long)scc_smem_fixed(SL.maxnsh, SL.maxn, SL.maxnat)) / 8;
   for (;;) {
-    if (threadIdx.x == 0) next = atomicAdd(B.queue, 1);
+    if (threadIdx.x == 0) next = SL.q_begin + atomicAdd(SL.counter, 1);
     __syncthreads();
     const int idx = next;
     __syncthreads();
-    if (idx >= B.nmol) break;
+    if (idx >= SL.q_end) break;
     const int m = B.order[idx];
     if (B.status[m] != kOk) continue;  // rejected during setup
-    scc_molecule(B, M, opt, m, sh, sh_atom, sh_k, ao_sh, atom_sh, sh_ao0);
+    scc_molecule<NT>(B, M, opt, SL, m, sh, sh_atom, sh_k, ao_sh, atom_sh, sh_ao0, vec, As, as_cap);
   }
 }
 
 long long scc_workspace_doubles(int maxn, int maxnsh, int cap, int maxnat) {
   return cta_ws_size(maxn, maxnsh, cap, maxnat);
+}
+
+// Dynamic shared memory for a class: index tables, vectors and, when
+// `matrix_n` > 0, room for a matrix_n x work_lda(matrix_n) working matrix.
+size_t scc_smem_bytes(int maxnsh, int maxn, int maxnat, int matrix_n) {
+  const size_t fixed = scc_smem_fixed(maxnsh, maxn, maxnat);
+  return matrix_n > 0 ? fixed + sizeof(double) * (size_t)matrix_n * work_lda(matrix_n) : fixed;
+}
+
+// Largest dynamic shared memory a CTA of the class may request: the 227 KB per
+// CTA limit less the kernel's static shared memory (two CTAs per SM for nt = 256
+// share the SM's 228 KB, 1 KB of which each CTA reserves).
+size_t scc_max_dynamic_smem(int nt) {
+  cudaFuncAttributes a;
+  const cudaError_t e = nt == 512 ? cudaFuncGetAttributes(&a, scc_kernel<512>) : cudaFuncGetAttributes(&a, scc_kernel<256>);
+  const size_t stat = e == cudaSuccess ? a.sharedSizeBytes : 8192;
+  const size_t per_cta = nt == 512 ? 232448 : (233472 / 2 - 1024);
+  return per_cta - stat - 256;
+}
+
+// Host launcher of one size class (nt = 512 or 256 threads per CTA).
+cudaError_t launch_scc(int nt, int grid, size_t smem, cudaStream_t st, const Batch& B, const Model& M,
+                       const SccOptions& opt, const SccLaunch& SL) {
+  cudaError_t e;
+  if (nt == 512) {
+    if ((e = cudaFuncSetAttribute(scc_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+        cudaSuccess)
+      return e;
+    scc_kernel<512><<<grid, 512, smem, st>>>(B, M, opt, SL);
+  } else {
+    if ((e = cudaFuncSetAttribute(scc_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+        cudaSuccess)
+      return e;
+    scc_kernel<256><<<grid, 256, smem, st>>>(B, M, opt, SL);
+  }
+  return cudaGetLastError();
 }
 
 }  // namespace gfn1
