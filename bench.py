@@ -1,20 +1,25 @@
 #!/usr/bin/env python
-"""SCC energy + analytic gradient evaluations per second on B200.
+"""SCC energy + analytic gradient evaluations per second on B200, learned +
+batched versus plain.
 
-Workload (the batched configuration the headline metric is quoted on): 4096
-independent molecules, each a seeded cluster of 1-15 rigid H2O/NH3/CH4 monomers
-(3-75 atoms, 8-180 AOs; seeds 1000 + i, rank r uses 1000 + r*4096 + i), default
-SCC options (FP64, Broyden, T_el = 300 K, 1e-6 Eh / 2e-5 e), analytic gradient.
-A step is one full evaluation of the batch: setup kernel (CN, S, H0, Coulomb,
-repulsion, D3), persistent SCC kernel, gradient kernel.
+Workload: 4096 independent molecules, each a seeded cluster of 1-15 rigid
+H2O/NH3/CH4 monomers (3-75 atoms, 8-180 AOs; seeds 1000 + i, rank r uses
+1000 + r*4096 + i; none of them is in the guess network's training set, seeds
+10^6 + i), default SCC options (FP64, Broyden, T_el = 300 K, 1e-6 Eh /
+2e-5 e), analytic gradient.  A step is one full evaluation of the batch:
+learned guess (descriptors, BF16 MLP, projection), setup kernel (CN, S, H0,
+Coulomb, repulsion, D3), persistent SCC kernel, gradient kernel.  The plain
+method (zero initial shell charges, the reference's default) is timed on the
+same batch and reported beside it.
 
-value: evals/s with the coordinates resident in HBM, kernels timed with CUDA
-events on the launching stream, L2 flushed (256 MiB write) between steps.
-e2e: the same metric through gfn1_batch_energy_gradient with host buffers (the
-host->device input copy and the device->host result copy inside every step).
+value: learned+batched evals/s with the coordinates resident in HBM, kernels
+timed with CUDA events on the launching stream, L2 flushed (256 MiB write)
+between steps.  e2e: the same metric through gfn1_batch_energy_gradient with
+host buffers (the host->device input copy and the device->host result copy
+inside every step).
 
 --impl reference times the CPU restatement of gfn1-rs's path (oracle/, C++ FP64,
-all host threads) on a bounded sample of the same workload.
+all host threads, zero initial guess) on a bounded sample of the same workload.
 """
 from __future__ import annotations
 
@@ -41,13 +46,13 @@ SEED0 = 1000
 
 def workload_config(nmol, natoms, naos):
     return {
-        "workload": f"batched plain GFN1-xTB SCC energy+gradient, {nmol} mixed H2O/NH3/CH4 clusters "
+        "workload": f"batched GFN1-xTB SCC energy+gradient, {nmol} mixed H2O/NH3/CH4 clusters "
                     f"(1-15 monomers, 3-75 atoms, 8-180 AOs, seeds 1000+i)",
         "nmol": nmol,
         "natoms": int(natoms),
         "naos": int(naos),
         "scc": "FP64, Broyden(250), T_el 300 K, 1e-6 Eh / 2e-5 e",
-        "guess": "zero shell charges (plain)",
+        "guess": "learned (atom-centred MLP, BF16 inference) vs zero shell charges (plain)",
         "l2": "256 MiB flush between timed steps",
     }
 
@@ -248,25 +253,29 @@ def main():
     nao_z, nsh_z = calc.engine.element_sizes()
     naos = int(np.sum(nao_z[z]))
 
-    # ---- device-resident timing (value, per-kernel roofline)
+    # ---- device-resident timing (value, per-kernel roofline): plain, then learned
+    from gfn1_rs.guess import LearnedGuess
+
+    guess = LearnedGuess.from_file(calc.engine)
     rb = calc.resident(off, z)
     d_xyz = torch.tensor(xb, dtype=torch.float64, device=dev)
     rb.set_positions(d_xyz.data_ptr(), on_device=True)
     stream = torch.cuda.Stream(device=dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
-    with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
-            rb.launch(stream.cuda_stream)
-    stream.synchronize()
-    res0 = rb.download()
-    if np.any(res0.status != 0):
-        bad = np.flatnonzero(res0.status)
-        raise SystemExit(f"{len(bad)} molecules failed (first {bad[0]}: status {res0.status[bad[0]]})")
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
-    with ClockSampler(local) as clk:
+
+    def timed(label):
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                rb.launch(stream.cuda_stream)
+        stream.synchronize()
+        r0 = rb.download()
+        if np.any(r0.status != 0):
+            bad = np.flatnonzero(r0.status)
+            raise SystemExit(f"{label}: {len(bad)} molecules failed (first {bad[0]}: status {r0.status[bad[0]]})")
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
         with torch.cuda.stream(stream):
             for k in range(args.steps):
                 flush.fill_(float(k))
@@ -279,19 +288,26 @@ def main():
                 ev[k][3].record(stream)
         stream.synchronize()
         torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    setup_ms = [e[0].elapsed_time(e[1]) for e in ev]
-    scc_ms = [e[1].elapsed_time(e[2]) for e in ev]
-    grad_ms = [e[2].elapsed_time(e[3]) for e in ev]
-    step_ms = [e[0].elapsed_time(e[3]) for e in ev]
-    total_s = sum(step_ms) / 1e3
-    res = rb.download()
-    if dist:
-        t = torch.tensor([total_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_s = float(t.item())
+        if dist:
+            dist.barrier()
+        t = {"setup": [e[0].elapsed_time(e[1]) for e in ev], "scc": [e[1].elapsed_time(e[2]) for e in ev],
+             "grad": [e[2].elapsed_time(e[3]) for e in ev], "step": [e[0].elapsed_time(e[3]) for e in ev]}
+        total = sum(t["step"]) / 1e3
+        if dist:
+            tt = torch.tensor([total], dtype=torch.float64, device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            total = float(tt.item())
+        return t, total, rb.download(), rb.launches
+
+    with ClockSampler(local) as clk:
+        rb.set_guess(None)
+        t_plain, total_plain, res_plain, _ = timed("plain")
+        rb.set_guess(guess)
+        t_learn, total_s, res, launches = timed("learned")
     value = args.nmol * world * args.steps / total_s
+    plain_value = args.nmol * world * args.steps / total_plain
+    dE_learned = float(np.max(np.abs(res.energy - res_plain.energy)))
+    setup_ms, scc_ms, grad_ms = t_learn["setup"], t_learn["scc"], t_learn["grad"]
 
     # ---- roofline of the dominant kernel (SCC)
     peak = fp64_peak_tflops(torch, dev)
@@ -304,7 +320,8 @@ def main():
                 "peak_source": "cuBLAS FP64 DGEMM 8192^3 burst measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
                 "work": "sum over molecules of iterations*(12N^3+2N^2+2nsh^2)+14N^3 (algorithmic FLOPs)"}
 
-    # ---- end to end through the public C ABI with host buffers
+    # ---- end to end through the public C ABI with host buffers (learned guess)
+    guess.attach()
     e2e_times = []
     for k in range(args.warmup + args.steps):
         torch.cuda.synchronize()
@@ -333,13 +350,24 @@ def main():
         cfg["kernel_ms"] = {"setup": statistics.mean(setup_ms), "scc": statistics.mean(scc_ms),
                             "grad": statistics.mean(grad_ms)}
         cfg["scc_iterations_mean"] = float(res.iterations.mean())
+        cfg["plain"] = {"value": plain_value, "unit": UNIT, "ms_per_step": 1e3 * total_plain / args.steps,
+                        "scc_iterations_mean": float(res_plain.iterations.mean()),
+                        "kernel_ms": {"setup": statistics.mean(t_plain["setup"]),
+                                      "scc": statistics.mean(t_plain["scc"]),
+                                      "grad": statistics.mean(t_plain["grad"])}}
+        cfg["learned_vs_plain"] = value / plain_value
+        cfg["max_abs_dE_learned_vs_plain"] = dE_learned
+        cfg["scc_iterations_p95"] = {"learned": float(np.percentile(res.iterations, 95)),
+                                     "plain": float(np.percentile(res_plain.iterations, 95))}
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded clusters)",
                "config": cfg, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-               "gpu_launches": int(rb.launches * args.steps), "clocks": clk.summary()}
+               "gpu_launches": int(launches * args.steps), "clocks": clk.summary()}
         print(json.dumps(out), flush=True)
     rb.close()
+    guess.detach()
+    guess.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

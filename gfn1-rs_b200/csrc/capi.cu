@@ -19,6 +19,7 @@
 
 #include "../../include/gfn1_b200.h"
 #include "common.cuh"
+#include "guess.cuh"
 #include "model.cuh"
 
 namespace gfn1 {
@@ -207,6 +208,13 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct gfn1_batch;
 
+// A learned initial-guess model on the engine's device (FP32 parameters and
+// BF16 weight copies).
+struct gfn1_guess {
+  gfn1_engine* eng = nullptr;
+  GuessModel model{};
+};
+
 struct gfn1_engine {
   int device = 0;
   int num_sms = 148;
@@ -221,6 +229,7 @@ struct gfn1_engine {
   double* d_c6 = nullptr;
   cudaStream_t stream = nullptr;
   gfn1_batch* oneshot = nullptr;  // reused by gfn1_batch_energy_gradient / gfn1_run
+  gfn1_guess* guess = nullptr;    // default initial guess of new batches (not owned)
   Model model() const {
     Model m;
     m.elem = d_elem;
@@ -254,6 +263,9 @@ struct gfn1_batch {
   gfn1_options opt;
   bool has_init_q = false;
   bool profiling = false;
+  gfn1_guess* guess = nullptr;       // learned guess used when no initial charges are set
+  DevBuf<float> gx, gy;              // guess features [natoms x 100] and outputs [natoms x 2]
+  DevBuf<double> gq;                 // guessed initial shell charges [nshells]
   BlobLayout lay;
   HostBuf h_in, h_out;               // pinned staging
   DevBuf<unsigned char> d_in, d_out; // device blobs
@@ -283,7 +295,7 @@ struct gfn1_batch {
     B.z = din<int>(lay.z);
     B.xyz = din<double>(lay.xyz);
     B.charge = din<double>(lay.charge);
-    B.init_q = has_init_q ? din<double>(lay.init_q) : nullptr;
+    B.init_q = has_init_q ? din<double>(lay.init_q) : (guess ? gq.p : nullptr);
     B.S = S.p;
     B.H0 = H0.p;
     B.P = P.p;
@@ -319,6 +331,9 @@ struct gfn1_batch {
     for (DevBuf<double>* d : {&S, &H0, &P, &W, &ws, &gam, &pairbuf, &cn, &shell_pot, &se, &grad_classic}) d->release();
     queue.release();
     stage.release();
+    gx.release();
+    gy.release();
+    gq.release();
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
     if (side) cudaStreamDestroy(side);
@@ -699,6 +714,11 @@ int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t*
             b->pairbuf.ensure(8 * std::max<long long>(pair_total, 1)) && b->cn.ensure(natoms) &&
             b->shell_pot.ensure(nshells) && b->se.ensure(nshells) && b->grad_classic.ensure(3 * natoms);
   if (!ok) return fail(eng, GFN1_E_DEVICE, "device allocation failed for the batch workspace");
+  b->guess = eng->guess;
+  if (b->guess && !(b->gx.ensure((size_t)kGuessIn * std::max<long long>(natoms, 1)) &&
+                    b->gy.ensure((size_t)kGuessOut * std::max<long long>(natoms, 1)) &&
+                    b->gq.ensure((size_t)std::max<long long>(nshells, 1))))
+    return fail(eng, GFN1_E_DEVICE, "device allocation failed for the learned guess");
   return GFN1_OK;
 }
 
@@ -722,6 +742,15 @@ int launch_stage(gfn1_batch* b, int stage, cudaStream_t st) {
       return cuda_fail(eng, e, "batch reset");
     if (b->profiling && (e = cudaMemsetAsync(b->stage.p, 0, sizeof(unsigned long long) * kStages, st)) != cudaSuccess)
       return cuda_fail(eng, e, "batch reset");
+    if (b->guess && !b->has_init_q) {  // learned initial shell charges from the device coordinates
+      const GuessModel& g = b->guess->model;
+      if ((e = launch_guess_features(b->nmol, B.atom_off, B.z, B.xyz, g.params, g.params + kGuessDesc, b->gx.p, st)) !=
+              cudaSuccess ||
+          (e = launch_guess_infer(g, b->natoms, b->gx.p, b->gy.p, st)) != cudaSuccess ||
+          (e = launch_guess_project(b->nmol, B.atom_off, B.shell_off, B.z, b->gy.p, B.charge, b->gq.p, st)) !=
+              cudaSuccess)
+        return cuda_fail(eng, e, "learned guess");
+    }
     const size_t smem = sizeof(double) * (16 * (size_t)b->max_nat + 32) +
                         sizeof(int) * (3 * (size_t)b->max_nat + 2 + 2 * (size_t)b->max_nsh);
     if (smem > 48 * 1024) cudaFuncSetAttribute(setup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -819,6 +848,12 @@ bool finite_all(const double* x, long long n) {
   return true;
 }
 
+bool finite_all_f(const float* x, long long n) {
+  for (long long i = 0; i < n; ++i)
+    if (!std::isfinite(x[i])) return false;
+  return true;
+}
+
 }  // namespace
 
 // ============================================================== C ABI
@@ -877,6 +912,7 @@ int gfn1_engine_create(const char* param_spec, int device, gfn1_engine** out) {
 void gfn1_engine_destroy(gfn1_engine* eng) {
   if (!eng) return;
   if (eng->oneshot) gfn1_batch_destroy(eng->oneshot);
+  if (eng->guess) eng->guess->eng = nullptr;
   if (eng->d_elem) cudaFree(eng->d_elem);
   if (eng->d_pair) cudaFree(eng->d_pair);
   if (eng->d_c6) cudaFree(eng->d_c6);
@@ -992,7 +1028,9 @@ int gfn1_batch_info(const gfn1_batch* b, int64_t* natoms, int64_t* nshells, int6
   if (natoms) *natoms = b->natoms;
   if (nshells) *nshells = b->nshells;
   if (naos) *naos = b->naos;
-  if (launches) *launches = b->opt.compute_gradient ? 3 : 2;
+  if (launches)  // setup, one SCC launch per non-empty size class, gradient, learned guess
+    *launches = 1 + (b->cls[0].n_cta > 0) + (b->cls[1].n_cta > 0) + (b->opt.compute_gradient ? 1 : 0) +
+                (b->guess && !b->has_init_q ? 3 : 0);
   return GFN1_OK;
 }
 
@@ -1064,6 +1102,80 @@ int gfn1_run(gfn1_engine* eng, int nat, const uint8_t* z, const double* xyz_bohr
              const double* init_shell_q, const gfn1_options* opt, const gfn1_outputs* out) {
   int32_t off[2] = {0, nat};
   return gfn1_batch_energy_gradient(eng, 1, off, z, xyz_bohr, &charge, init_shell_q, opt, out);
+}
+
+int gfn1_guess_create(gfn1_engine* eng, const float* params, int64_t nparams, gfn1_guess** out) {
+  if (!eng || !params || !out) return fail(eng, GFN1_E_INVALID_INPUT, "invalid arguments");
+  *out = nullptr;
+  if (nparams != kGuessParams)
+    return fail(eng, GFN1_E_INVALID_INPUT,
+                "guess parameter vector has " + std::to_string(nparams) + " values, expected " +
+                    std::to_string(kGuessParams));
+  if (!finite_all_f(params, nparams)) return fail(eng, GFN1_E_NAN, "non-finite guess parameter");
+  for (int f = 0; f < kGuessDesc; ++f)
+    if (!(params[kGuessDesc + f] > 0.0f)) return fail(eng, GFN1_E_INVALID_INPUT, "guess feature scale must be positive");
+  cudaSetDevice(eng->device);
+  gfn1_guess* g = new gfn1_guess();
+  g->eng = eng;
+  cudaError_t e = guess_model_upload(params, g->model);
+  if (e != cudaSuccess) {
+    delete g;
+    return cuda_fail(eng, e, "guess upload");
+  }
+  *out = g;
+  return GFN1_OK;
+}
+
+void gfn1_guess_destroy(gfn1_guess* g) {
+  if (!g) return;
+  if (g->eng && g->eng->guess == g) g->eng->guess = nullptr;
+  if (g->eng && g->eng->oneshot && g->eng->oneshot->guess == g) g->eng->oneshot->guess = nullptr;
+  guess_model_free(g->model);
+  delete g;
+}
+
+int gfn1_engine_set_guess(gfn1_engine* eng, gfn1_guess* g) {
+  if (!eng) return fail(nullptr, GFN1_E_INVALID_INPUT, "null engine");
+  if (g && g->eng != eng) return fail(eng, GFN1_E_INVALID_INPUT, "guess belongs to another engine");
+  eng->guess = g;
+  return GFN1_OK;
+}
+
+int gfn1_batch_set_guess(gfn1_batch* b, gfn1_guess* g) {
+  if (!b) return fail(nullptr, GFN1_E_INVALID_INPUT, "null batch");
+  if (g && g->eng != b->eng) return fail(b->eng, GFN1_E_INVALID_INPUT, "guess belongs to another engine");
+  b->guess = g;
+  if (g && !(b->gx.ensure((size_t)kGuessIn * std::max<long long>(b->natoms, 1)) &&
+             b->gy.ensure((size_t)kGuessOut * std::max<long long>(b->natoms, 1)) &&
+             b->gq.ensure((size_t)std::max<long long>(b->nshells, 1)))) {
+    b->guess = nullptr;
+    return fail(b->eng, GFN1_E_DEVICE, "device allocation failed for the learned guess");
+  }
+  return GFN1_OK;
+}
+
+int gfn1_guess_infer_device(gfn1_guess* g, int64_t natoms, const float* x, float* y, void* stream) {
+  if (!g || natoms < 0 || (natoms > 0 && (!x || !y))) return fail(g ? g->eng : nullptr, GFN1_E_INVALID_INPUT, "invalid arguments");
+  cudaError_t e = launch_guess_infer(g->model, natoms, x, y, (cudaStream_t)stream);
+  return e == cudaSuccess ? GFN1_OK : cuda_fail(g->eng, e, "guess inference");
+}
+
+int gfn1_guess_predict_device(gfn1_guess* g, int nmol, const int32_t* atom_off, const int32_t* shell_off,
+                              const int32_t* z, const double* xyz, const double* charge, float* x_scratch,
+                              float* y_scratch, double* init_q, void* stream) {
+  if (!g || nmol < 0 || (nmol > 0 && (!atom_off || !shell_off || !z || !xyz || !x_scratch || !y_scratch || !init_q)))
+    return fail(g ? g->eng : nullptr, GFN1_E_INVALID_INPUT, "invalid arguments");
+  if (nmol == 0) return GFN1_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  int32_t n32 = 0;  // total atom count, read back once from the device offsets
+  cudaError_t e = cudaMemcpyAsync(&n32, atom_off + nmol, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  const int64_t natoms = n32;
+  const GuessModel& m = g->model;
+  if (e == cudaSuccess) e = launch_guess_features(nmol, atom_off, z, xyz, m.params, m.params + kGuessDesc, x_scratch, st);
+  if (e == cudaSuccess) e = launch_guess_infer(m, natoms, x_scratch, y_scratch, st);
+  if (e == cudaSuccess) e = launch_guess_project(nmol, atom_off, shell_off, z, y_scratch, charge, init_q, st);
+  return e == cudaSuccess ? GFN1_OK : cuda_fail(g->eng, e, "guess prediction");
 }
 
 }  // extern "C"

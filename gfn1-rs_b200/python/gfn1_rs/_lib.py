@@ -101,6 +101,31 @@ def load():
         L.gfn1_batch_io_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
         L.gfn1_run_noalloc.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_uint8), _dp, ctypes.c_double, _dp,
                                        ctypes.POINTER(Options), ctypes.POINTER(Outputs), vp]
+        fp = ctypes.POINTER(ctypes.c_float)
+        i64 = ctypes.c_int64
+        L.gfn1_guess_param_count.argtypes = []
+        L.gfn1_guess_param_count.restype = i64
+        L.gfn1_guess_create.argtypes = [vp, fp, i64, ctypes.POINTER(vp)]
+        L.gfn1_guess_destroy.argtypes = [vp]
+        L.gfn1_guess_destroy.restype = None
+        L.gfn1_engine_set_guess.argtypes = [vp, vp]
+        L.gfn1_batch_set_guess.argtypes = [vp, vp]
+        L.gfn1_guess_features_device.argtypes = [ctypes.c_int, vp, vp, vp, vp, vp, vp, vp]
+        L.gfn1_guess_infer_device.argtypes = [vp, i64, vp, vp, vp]
+        L.gfn1_guess_predict_device.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.gfn1_mlp_gemm.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    vp, ctypes.c_int, vp, ctypes.c_int, vp, vp, ctypes.c_int, vp, vp, ctypes.c_int,
+                                    ctypes.c_int, vp]
+        L.gfn1_mlp_gemm_splits.argtypes = [ctypes.c_int, ctypes.c_int]
+        L.gfn1_mlp_reduce.argtypes = [ctypes.c_int, i64, vp, vp, i64, vp]
+        L.gfn1_mlp_colsum.argtypes = [ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int, vp, vp]
+        L.gfn1_mlp_project_loss.argtypes = [ctypes.c_int, vp, vp, vp, vp, ctypes.c_double, vp, vp, vp, vp]
+        L.gfn1_mlp_adam.argtypes = [i64, vp, vp, vp, vp, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                    ctypes.c_float, ctypes.c_float, ctypes.c_float, vp]
+        for name in ("gfn1_guess_create", "gfn1_engine_set_guess", "gfn1_batch_set_guess", "gfn1_guess_features_device",
+                     "gfn1_guess_infer_device", "gfn1_guess_predict_device", "gfn1_mlp_gemm", "gfn1_mlp_gemm_splits",
+                     "gfn1_mlp_reduce", "gfn1_mlp_colsum", "gfn1_mlp_project_loss", "gfn1_mlp_adam"):
+            getattr(L, name).restype = ctypes.c_int
         for name in ("gfn1_run_noalloc", "gfn1_batch_launch_stage", "gfn1_batch_stage_cycles", "gfn1_batch_io_bytes",
                      "gfn1_engine_create", "gfn1_basis_size", "gfn1_run", "gfn1_batch_energy_gradient",
                      "gfn1_batch_create", "gfn1_batch_set_positions", "gfn1_batch_set_initial_charges",

@@ -50,8 +50,15 @@ def _options(opts: dict, compute_gradient: bool) -> _lib.Options:
 class BatchCalculator:
     def __init__(self, param_path=None, device=0, max_scc=250, energy_tolerance=1.0e-6, charge_tolerance=2.0e-5,
                  mixing=0.4, scc_broyden=True, scc_broyden_size=250, electronic_temperature=300.0,
-                 enable_dispersion=True):
+                 enable_dispersion=True, learned_guess=None):
+        """learned_guess: None/False for the reference's zero initial guess, True for
+        the packaged trained network, or a path to a parameter file."""
         self.engine = _lib.Engine(param_path, device)
+        self.guess = None
+        if learned_guess:
+            from .guess import DEFAULT_PATH, LearnedGuess
+            self.guess = LearnedGuess.from_file(self.engine, DEFAULT_PATH if learned_guess is True else learned_guess)
+            self.guess.attach()
         self.opts = dict(max_scc=max_scc, energy_tolerance=energy_tolerance, charge_tolerance=charge_tolerance,
                          mixing=mixing, scc_broyden=int(bool(scc_broyden)), scc_broyden_size=scc_broyden_size,
                          electronic_temperature=electronic_temperature,
@@ -60,9 +67,13 @@ class BatchCalculator:
     def shell_offsets(self, atom_offsets, numbers) -> np.ndarray:
         """Prefix sums of the shell counts, laid out as the C side does (atoms of
         unsupported elements contribute no shells)."""
+        return self.shell_offsets_for(self.engine, atom_offsets, numbers)
+
+    @staticmethod
+    def shell_offsets_for(engine, atom_offsets, numbers) -> np.ndarray:
         off = np.asarray(atom_offsets, dtype=np.int64)
         z = np.asarray(numbers, dtype=np.int64)
-        nsh_z = self.engine.element_sizes()[1]
+        nsh_z = engine.element_sizes()[1]
         per_atom = np.where((z >= 1) & (z <= 86), nsh_z[np.clip(z, 0, 86)], 0)
         cum = np.concatenate([[0], np.cumsum(np.maximum(per_atom, 0))])
         return cum[off]
@@ -150,6 +161,16 @@ class ResidentBatch:
             self._xyz_keep = arr
             p = arr.ctypes.data_as(ctypes.c_void_p)
         _lib.check(_lib.load().gfn1_batch_set_positions(self.handle, p, int(on_device)), self.calc.engine.handle)
+
+    def set_guess(self, guess):
+        """Learned initial guess for launches without initial charges (None: zero guess)."""
+        _lib.check(_lib.load().gfn1_batch_set_guess(self.handle, None if guess is None else guess.handle),
+                   self.calc.engine.handle)
+        self._guess = guess
+        na, ns, no = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        nl = ctypes.c_int32()
+        _lib.load().gfn1_batch_info(self.handle, ctypes.byref(na), ctypes.byref(ns), ctypes.byref(no), ctypes.byref(nl))
+        self.launches = nl.value
 
     def set_initial_charges(self, q, on_device: bool = False):
         if q is None:

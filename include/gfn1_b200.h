@@ -34,6 +34,7 @@ enum {
 
 typedef struct gfn1_engine gfn1_engine;
 typedef struct gfn1_batch gfn1_batch;
+typedef struct gfn1_guess gfn1_guess;
 
 /* Plain-path subset of ElectronicOptions (gfn1-rs src/electronic.rs:157-453,
  * defaults :395-452) plus the gradient switch of AnalyticGradientOptions
@@ -147,6 +148,64 @@ int gfn1_batch_info(const gfn1_batch* b, int64_t* natoms, int64_t* nshells, int6
  * engine's stream.  Synchronous. */
 int gfn1_run_noalloc(gfn1_engine* eng, int nat, const uint8_t* z, const double* xyz_bohr, double charge,
                      const double* init_shell_q, const gfn1_options* opt, const gfn1_outputs* out, void* stream);
+
+/* ---- Learned SCC initial guess.  No counterpart in the reference, whose SCC
+ * starts from zero shell charges or a caller-supplied vector (the Rust
+ * `init_shell_q` hook, gfn1-rs src/electronic.rs:1231-1239); the guess fills
+ * that vector on the device.  Per H/C/N/O atom: 64 radial + 32 angular
+ * descriptors (cutoff 6 bohr) and the element one-hot feed three SiLU layers
+ * of 128 and a linear layer to the atom's two shell charges; each molecule's
+ * charges are shifted to sum to its total charge.  Molecules with other
+ * elements get the zero guess.  Inference runs with BF16 weights and
+ * activations (FP32 accumulation); the converged SCC always judges the result.
+ *
+ * Parameters (float32, gfn1_guess_param_count() values): feature mean[96],
+ * feature scale[96], W1[100x128], b1[128], W2[128x128], b2[128],
+ * W3[128x128], b3[128], W4[128x2], b4[2], weights row-major [in][out]. */
+int64_t gfn1_guess_param_count(void);
+int gfn1_guess_create(gfn1_engine* eng, const float* params, int64_t nparams, gfn1_guess** out);
+void gfn1_guess_destroy(gfn1_guess* g);
+/* Default guess of batches prepared from now on (NULL restores the zero guess).
+ * The guess must outlive its use by the engine. */
+int gfn1_engine_set_guess(gfn1_engine* eng, gfn1_guess* g);
+/* Guess of a resident batch; used by launches while no initial charges are set. */
+int gfn1_batch_set_guess(gfn1_batch* b, gfn1_guess* g);
+/* Device-pointer entry points (stream = cudaStream_t or NULL):
+ * features x[natoms x 100] (raw descriptors and one-hot when mean/scale are
+ * NULL), inference y[natoms x 2] = MLP(x), and the whole prediction into
+ * init_q[nshells] in the engine's shell layout (x, y are caller scratch). */
+int gfn1_guess_features_device(int nmol, const int32_t* atom_off, const int32_t* z, const double* xyz,
+                               const float* mean, const float* scale, float* x, void* stream);
+int gfn1_guess_infer_device(gfn1_guess* g, int64_t natoms, const float* x, float* y, void* stream);
+int gfn1_guess_predict_device(gfn1_guess* g, int nmol, const int32_t* atom_off, const int32_t* shell_off,
+                              const int32_t* z, const double* xyz, const double* charge, float* x_scratch,
+                              float* y_scratch, double* init_q, void* stream);
+
+/* ---- Training primitives of the guess network (FP32, device pointers,
+ * asynchronous on `stream`).  No reference counterpart.
+ * gfn1_mlp_gemm: C[MxN] = op(A)[MxK] op(B)[KxN], op(A)(m,k) = ta ? A[k*lda+m] :
+ * A[m*lda+k], op(B)(k,n) = tb ? B[n*ldb+k] : B[k*ldb+n], with epilogue
+ *   0: partial sums of K-split z into C + z*M*ldc (ksplit >= 1; see
+ *      gfn1_mlp_gemm_splits for the number of slices written),
+ *   1: Z = acc + bias[n], C = SiLU(Z),   2: C = acc + bias[n],
+ *   3: C = acc * SiLU'(zprev[m*ldz+n]).
+ * Supported (ta, tb, epi): (0,0,1) (0,0,2) (0,1,3) (0,1,0) (1,0,0) (0,0,0). */
+int gfn1_mlp_gemm(int ta, int tb, int epi, int M, int N, int K, const float* A, int lda, const float* B, int ldb,
+                  const float* bias, const float* zprev, int ldz, float* C, float* Z, int ldc, int ksplit,
+                  void* stream);
+int gfn1_mlp_gemm_splits(int K, int ksplit);
+/* out[i] = sum_z part[z*stride + i], z = 0..nz-1 in order. */
+int gfn1_mlp_reduce(int nz, int64_t stride, const float* part, float* out, int64_t n, void* stream);
+/* part[c*N + n] = sum of Y[m*ldy + n] over rows m of chunk c (ceil(M/mchunk) chunks). */
+int gfn1_mlp_colsum(int M, int N, const float* Y, int ldy, int mchunk, float* part, void* stream);
+/* Per molecule (2 shells per atom): q = y + (charge - sum y)/nshells; with a
+ * label, loss_mol[m] = sum (q - label)^2 * inv_nsh and gy = d loss / d y. */
+int gfn1_mlp_project_loss(int nmol, const int32_t* atom_off, const float* y, const double* charge,
+                          const float* label, double inv_nsh, float* gy, float* q, double* loss_mol, void* stream);
+/* Adam step: m = b1 m + (1-b1) g, v = b2 v + (1-b2) g^2,
+ * p -= lr (m c1) / (sqrt(v c2) + eps), c1 = 1/(1-b1^t), c2 = 1/(1-b2^t). */
+int gfn1_mlp_adam(int64_t n, float* p, const float* g, float* m, float* v, float lr, float beta1, float beta2,
+                  float eps, float c1, float c2, void* stream);
 
 #ifdef __cplusplus
 }
