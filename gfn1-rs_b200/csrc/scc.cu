@@ -144,8 +144,7 @@ __device__ __forceinline__ int sturm_poly(const double* d, const double* esq, in
     dp = -kGuardScale;
   }
   int c = p <= 0.0;
-  for (int i = 1; i < n; ++i) {
-    const double t = d[i] - x, e2 = esq[i - 1];
+  auto step = [&](double t, double e2) {
     double pn = t * p - e2 * pm;
     double dpn = t * dp - p - e2 * dpm;
     double ddpn = t * ddp - 2.0 * dp - e2 * ddpm;
@@ -165,16 +164,25 @@ __device__ __forceinline__ int sturm_poly(const double* d, const double* esq, in
     dp = dpn;
     ddpm = ddp;
     ddp = ddpn;
-    if ((i & 3) == 0) {
-      const double sc = pow2_inv_scale(fmax(fabs(p), fabs(pm)));
-      p *= sc;
-      pm *= sc;
-      dp *= sc;
-      dpm *= sc;
-      ddp *= sc;
-      ddpm *= sc;
-    }
+  };
+  int i = 1;
+  // groups of four steps with the loads issued first, then a rescale
+  for (; i + 3 < n; i += 4) {
+    const double t0 = d[i] - x, t1 = d[i + 1] - x, t2 = d[i + 2] - x, t3 = d[i + 3] - x;
+    const double e0 = esq[i - 1], e1 = esq[i], e2 = esq[i + 1], e3 = esq[i + 2];
+    step(t0, e0);
+    step(t1, e1);
+    step(t2, e2);
+    step(t3, e3);
+    const double sc = pow2_inv_scale(fmax(fabs(p), fabs(pm)));
+    p *= sc;
+    pm *= sc;
+    dp *= sc;
+    dpm *= sc;
+    ddp *= sc;
+    ddpm *= sc;
   }
+  for (; i < n; ++i) step(d[i] - x, esq[i - 1]);
   pout = p;
   dpout = dp;
   ddpout = ddp;
@@ -232,12 +240,35 @@ __device__ void tri_factor(const double* d, const double* e, int n, double lam, 
 }
 
 // Solves (T - lam I) x = b in place with the factors of tri_factor.  The
-// running entries are carried in registers, so the loads of x and of the
-// factors do not wait on the stores of the previous step.
+// running entries are carried in registers and the loads of x and of the
+// factors are issued four steps ahead of their use, so the serial recurrences
+// do not wait on memory at every step.
 __device__ void tri_solve(const double* w, int n, int ldw, double* x, long long stride) {
   const long long s = (long long)n * ldw;
   double cur = x[0];
-  for (int k = 0; k < n - 1; ++k) {
+  int k = 0;
+  for (; k + 4 <= n - 1; k += 4) {
+    double fl[4], mu[4], xn[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double* wk = w + (long long)(k + q) * ldw;
+      fl[q] = wk[4 * s];
+      mu[q] = wk[3 * s];
+      xn[q] = x[(k + q + 1) * stride];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      double xk = cur, xk1 = xn[q];
+      if (fl[q] != 0.0) {
+        xk = xn[q];
+        xk1 = cur;
+      }
+      xk1 -= mu[q] * xk;
+      x[(k + q) * stride] = xk;
+      cur = xk1;
+    }
+  }
+  for (; k < n - 1; ++k) {
     const double* wk = w + (long long)k * ldw;
     double xk = cur, xk1 = x[(k + 1) * stride];
     if (wk[4 * s] != 0.0) {
@@ -255,7 +286,26 @@ __device__ void tri_solve(const double* w, int n, int ldw, double* x, long long 
   const double* w2 = w + (long long)(n - 2) * ldw;
   double x1 = (x[(n - 2) * stride] - w2[s] * x2) * w2[0];  // x[n-2]
   x[(n - 2) * stride] = x1;
-  for (int k = n - 3; k >= 0; --k) {
+  k = n - 3;
+  for (; k >= 3; k -= 4) {
+    double rh[4], u1[4], u2[4], rp[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double* wk = w + (long long)(k - q) * ldw;
+      rh[q] = x[(k - q) * stride];
+      u1[q] = wk[s];
+      u2[q] = wk[2 * s];
+      rp[q] = wk[0];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double x0 = (rh[q] - u1[q] * x1 - u2[q] * x2) * rp[q];
+      x[(k - q) * stride] = x0;
+      x2 = x1;
+      x1 = x0;
+    }
+  }
+  for (; k >= 0; --k) {
     const double* wk = w + (long long)k * ldw;
     const double x0 = (x[k * stride] - wk[s] * x1 - wk[2 * s] * x2) * wk[0];
     x[k * stride] = x0;
@@ -271,10 +321,30 @@ __device__ void tri_solve(const double* w, int n, int ldw, double* x, long long 
 // with its factor in tau[k] (H_k = I - tau_k v v^T).  Two barriers per column:
 // the matrix-vector product and the p.v partial sums, then the rank-2 update,
 // during which warp 0 also forms the norm of the next pivot row.
+// Four interleaved warp reductions (their shuffle latencies overlap).
+__device__ __forceinline__ void warp_sum4(double& a, double& b, double& c, double& d) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+    d += __shfl_xor_sync(0xffffffffu, d, o);
+  }
+}
+
+// Householder reduction of the symmetric A (full storage, leading dimension
+// lda) to tridiagonal form: d, e, reflector scalars tau, and the reflector of
+// column k in row k (entries k+1..N-1).  Per column: p = beta A22 v by warps
+// over rows (four rows at a time, lanes over columns), one barrier, then the
+// rank-2 update A22 -= v w^T + w v^T with w = p - K v, which also yields the
+// norm of the next column; a second barrier.  While the trailing size is at
+// most 32 * kCols, each lane keeps v_j and w_j of its columns in registers, so
+// the update reads and writes each element once.
 template <int NT>
 __device__ void tridiagonalize(double* A, int lda, int N, double* d, double* e, double* tau, double* pvec,
                                SccShared& sh) {
   constexpr int NW = NT / 32;
+  constexpr int kCols = 6;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   double part = 0.0;
   if (N >= 3)
@@ -283,6 +353,7 @@ __device__ void tridiagonalize(double* A, int lda, int N, double* d, double* e, 
   for (int k = 0; k < N - 2; ++k) {
     const int m = N - k - 1;
     double* rowk = A + (long long)k * lda + (k + 1);
+    double* a22 = A + (long long)(k + 1) * lda + (k + 1);
     const double x0 = rowk[0];
     const double tail = xn2 - x0 * x0;
     if (tail == 0.0) {  // column already reduced
@@ -302,15 +373,50 @@ __device__ void tridiagonalize(double* A, int lda, int N, double* d, double* e, 
     const double alpha = x0 >= 0.0 ? -xn : xn;
     const double v0 = x0 - alpha;
     const double beta = 2.0 / (v0 * v0 + tail);
+    const bool cached = m <= 32 * kCols;
+    double vreg[kCols], wreg[kCols];
+#pragma unroll
+    for (int c = 0; c < kCols; ++c) {
+      const int j = lane + 32 * c;
+      vreg[c] = (cached && j < m) ? (j == 0 ? v0 : rowk[j]) : 0.0;
+    }
+    // p = beta A22 v
     double pv_part = 0.0;
-    for (int i = wid; i < m; i += NW) {
-      const double* brow = A + (long long)(k + 1 + i) * lda + (k + 1);
-      double s = 0.0;
-      for (int j = lane; j < m; j += 32) s += brow[j] * (j == 0 ? v0 : rowk[j]);
-      s = warp_sum(s) * beta;
+    for (int i0 = wid; i0 < m; i0 += 4 * NW) {
+      double s[4] = {0.0, 0.0, 0.0, 0.0};
+      if (cached) {
+#pragma unroll
+        for (int c = 0; c < kCols; ++c) {
+          const int j = lane + 32 * c;
+          if (j < m) {
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+              const int i = i0 + r * NW;
+              if (i < m) s[r] += a22[(long long)i * lda + j] * vreg[c];
+            }
+          }
+        }
+      } else {
+        for (int j = lane; j < m; j += 32) {
+          const double v = (j == 0) ? v0 : rowk[j];
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const int i = i0 + r * NW;
+            if (i < m) s[r] += a22[(long long)i * lda + j] * v;
+          }
+        }
+      }
+      warp_sum4(s[0], s[1], s[2], s[3]);
       if (lane == 0) {
-        pvec[i] = s;
-        pv_part += s * (i == 0 ? v0 : rowk[i]);
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int i = i0 + r * NW;
+          if (i < m) {
+            const double pi = beta * s[r];
+            pvec[i] = pi;
+            pv_part += pi * (i == 0 ? v0 : rowk[i]);
+          }
+        }
       }
     }
     if (lane == 0) sh.red[wid] = pv_part;
@@ -323,19 +429,36 @@ __device__ void tridiagonalize(double* A, int lda, int N, double* d, double* e, 
       d[k] = A[(long long)k * lda + k];
       e[k] = alpha;
       tau[k] = beta;
-      rowk[0] = v0;
     }
+#pragma unroll
+    for (int c = 0; c < kCols; ++c) {
+      const int j = lane + 32 * c;
+      wreg[c] = (cached && j < m) ? pvec[j] - K * vreg[c] : 0.0;
+    }
+    // A22 -= v w^T + w v^T; warp 0 also takes the norm of the next column (row 1 of A22 from entry 1)
     double nrm = 0.0;
     for (int i = wid; i < m; i += NW) {
-      double* brow = A + (long long)(k + 1 + i) * lda + (k + 1);
+      double* brow = a22 + (long long)i * lda;
       const double vi = (i == 0) ? v0 : rowk[i];
       const double wi = pvec[i] - K * vi;
-      for (int j = lane; j < m; j += 32) {
-        const double vj = (j == 0) ? v0 : rowk[j];
-        const double wj = pvec[j] - K * vj;
-        const double nb = brow[j] - (vi * wj + wi * vj);
-        brow[j] = nb;
-        if (i == 0 && j >= 1) nrm += nb * nb;
+      if (cached) {
+#pragma unroll
+        for (int c = 0; c < kCols; ++c) {
+          const int j = lane + 32 * c;
+          if (j < m) {
+            const double nb = brow[j] - (vi * wreg[c] + wi * vreg[c]);
+            brow[j] = nb;
+            if (i == 0 && j >= 1) nrm += nb * nb;
+          }
+        }
+      } else {
+        for (int j = lane; j < m; j += 32) {
+          const double vj = (j == 0) ? v0 : rowk[j];
+          const double wj = pvec[j] - K * vj;
+          const double nb = brow[j] - (vi * wj + wi * vj);
+          brow[j] = nb;
+          if (i == 0 && j >= 1) nrm += nb * nb;
+        }
       }
     }
     if (wid == 0) {
@@ -343,8 +466,10 @@ __device__ void tridiagonalize(double* A, int lda, int N, double* d, double* e, 
       if (lane == 0) sh.scal[3] = nrm;
     }
     __syncthreads();
+    if (tid == 0) rowk[0] = v0;  // the reflector of column k is row k from entry k+1
     xn2 = sh.scal[3];
   }
+  __syncthreads();
   if (tid == 0) {
     if (N >= 2) {
       d[N - 2] = A[(long long)(N - 2) * lda + (N - 2)];
@@ -613,6 +738,7 @@ __device__ void back_transform(const double* A, int lda, const double* tau, int 
       const int j = idx / ncol, c = idx - j * ncol;
       const double* vj = A + (long long)(kb + j) * lda;
       double s = 0.0;
+#pragma unroll 8
       for (int r = kb + j + 1; r < N; ++r) s += vj[r] * Z[(long long)r * ldz + c];
       W1[j * ncol + c] = s;
     }
@@ -629,6 +755,7 @@ __device__ void back_transform(const double* A, int lda, const double* tau, int 
       const int r = kb + 1 + rr;
       const int jmax = min(nb, rr + 1);
       double s = 0.0;
+#pragma unroll 4
       for (int j = 0; j < jmax; ++j) s += A[(long long)(kb + j) * lda + r] * W2[j * ncol + c];
       Z[(long long)r * ldz + c] -= s;
     }
@@ -898,6 +1025,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
         lam_prev = lam;
         tri_factor(d, e, N, lam, tiny, ws, N);
         double* x = Z + jj;  // column jj, stride N
+#pragma unroll 4
         for (int i = 0; i < N; ++i) x[(long long)i * N] = hash_unit(i, jj) + 1e-3;
         const int nit = (jend - j > 1) ? 4 : 2;
         for (int it = 0; it < nit; ++it) {
@@ -908,8 +1036,10 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
             for (int i = 0; i < N; ++i) x[(long long)i * N] -= dot * Z[(long long)i * N + q];
           }
           double nrm = 0.0;
+#pragma unroll 8
           for (int i = 0; i < N; ++i) nrm += x[(long long)i * N] * x[(long long)i * N];
           const double inv = 1.0 / sqrt(fmax(nrm, 1e-300));
+#pragma unroll 8
           for (int i = 0; i < N; ++i) x[(long long)i * N] *= inv;
         }
       }
@@ -920,23 +1050,40 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     back_transform<NT>(A, lda, tau, N, Z, N, nocc, w.W1, w.W2, sh);
     clk.mark(kStBackTr);
     // (8) C = L^-T Z, D = L Z and the AO populations (S P)_mu,mu; warps own
-    //     4-row groups, lanes eigenvectors
+    //     4-row groups, lanes eigenvectors.  L is lower triangular, so row mu
+    //     of D needs k <= mu and row mu of C (column mu of L^-1) needs k >= mu.
     for (int rg = wid; rg * 4 < N; rg += NW) {
       const int m0 = rg * 4;
       const int mmax = min(m0 + 3, N - 1);
+      int mu_r[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) mu_r[r] = min(m0 + r, mmax);
       double pp[4] = {0.0, 0.0, 0.0, 0.0};
       for (int i0 = 0; i0 < nocc; i0 += 32) {
         const int i = i0 + lane;
         if (i < nocc) {
           double c[4] = {0.0, 0.0, 0.0, 0.0}, dd[4] = {0.0, 0.0, 0.0, 0.0};
-          for (int k = 0; k < N; ++k) {
-            const double z = Z[(long long)k * N + i];
+          const double* zc = Z + i;
+#pragma unroll 4
+          for (int k = 0; k < m0; ++k) {  // D only
+            const double z = zc[(long long)k * N];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) dd[r] += L[(long long)mu_r[r] * N + k] * z;
+          }
+          for (int k = m0; k <= mmax; ++k) {  // the diagonal block: both, triangular
+            const double z = zc[(long long)k * N];
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
-              const int mu_ = min(m0 + r, mmax);
-              c[r] += Li[(long long)k * N + mu_] * z;  // zero for k < mu
-              dd[r] += L[(long long)mu_ * N + k] * z;  // zero for k > mu
+              if (k <= mu_r[r]) dd[r] += L[(long long)mu_r[r] * N + k] * z;
+              if (k >= mu_r[r]) c[r] += Li[(long long)k * N + mu_r[r]] * z;
             }
+          }
+#pragma unroll 4
+          for (int k = mmax + 1; k < N; ++k) {  // C only
+            const double z = zc[(long long)k * N];
+            const double* lik = Li + (long long)k * N;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) c[r] += lik[mu_r[r]] * z;
           }
 #pragma unroll
           for (int r = 0; r < 4; ++r) {
