@@ -6,7 +6,9 @@
 // primitive-count rule (src/basis.rs:251-279), same-centre orthogonalisation of
 // a second shell of the same angular momentum (src/basis.rs:318-344), the CN
 // shift (src/basis.rs:281-293) and the legacy eV->Eh factor (src/basis.rs:18).
+#include <cublas_v2.h>
 #include <cuda_runtime.h>
+#include <cusolverDn.h>
 
 #include <algorithm>
 #include <cmath>
@@ -30,6 +32,12 @@ size_t scc_smem_bytes(int maxnsh, int maxn, int maxnat, int matrix_n);
 size_t scc_max_dynamic_smem(int nt);
 cudaError_t launch_scc(int nt, int grid, size_t smem, cudaStream_t st, const Batch& B, const Model& M,
                        const SccOptions& opt, const SccLaunch& SL);
+long long dense_ws_doubles(int maxnsh, int cap, int maxnat);
+size_t dense_smem_bytes(int maxnsh, int maxn, int maxnat);
+size_t dense_state_bytes();
+long long dense_solver_lwork(void* solver, int N);
+cudaError_t run_dense_molecule(const Batch& B, const Model& M, const SccOptions& opt, int m, int N, long long mo,
+                               DenseWork& dw, cudaStream_t st);
 }  // namespace gfn1
 
 using namespace gfn1;
@@ -266,6 +274,15 @@ struct gfn1_batch {
   gfn1_guess* guess = nullptr;       // learned guess used when no initial charges are set
   DevBuf<float> gx, gy;              // guess features [natoms x 100] and outputs [natoms x 2]
   DevBuf<double> gq;                 // guessed initial shell charges [nshells]
+  // molecules above kDenseN AOs: library-backed SCC on their own stream, one at a time
+  std::vector<int> dense_ids;
+  std::vector<int> dense_n;
+  std::vector<long long> dense_mo;
+  DenseWork dw;
+  DevBuf<double> dense_buf;
+  DevBuf<int> dense_info;
+  cudaStream_t dense_stream = nullptr;
+  cudaEvent_t ev_djoin = nullptr;
   BlobLayout lay;
   HostBuf h_in, h_out;               // pinned staging
   DevBuf<unsigned char> d_in, d_out; // device blobs
@@ -334,6 +351,16 @@ struct gfn1_batch {
     gx.release();
     gy.release();
     gq.release();
+    dense_buf.release();
+    dense_info.release();
+    if (dw.blas) cublasDestroy((cublasHandle_t)dw.blas);
+    if (dw.solver) cusolverDnDestroy((cusolverDnHandle_t)dw.solver);
+    if (dw.h_state) cudaFreeHost(dw.h_state);
+    dw = DenseWork();
+    if (ev_djoin) cudaEventDestroy(ev_djoin);
+    if (dense_stream) cudaStreamDestroy(dense_stream);
+    ev_djoin = nullptr;
+    dense_stream = nullptr;
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
     if (side) cudaStreamDestroy(side);
@@ -676,12 +703,34 @@ int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t*
   // size classes over the sorted order: N > kLargeN runs 512-thread CTAs, one
   // per SM, with up to 227 KB of shared memory; the rest 256-thread CTAs, two per SM
   const int kLargeN = 96;
-  int n_large = 0;
+  // above kDenseN AOs one SM per molecule is too slow: library-backed path.
+  // GFN1_DENSE_N overrides the threshold (used by the tests to run both paths
+  // on the same molecules).
+  int kDenseN = 1024;
+  if (const char* dn = std::getenv("GFN1_DENSE_N"))
+    if (*dn) kDenseN = std::max(2, std::atoi(dn));
+  int n_dense = 0;
+  while (n_dense < nmol && n_m[h_order[n_dense]] > kDenseN) ++n_dense;
+  b->dense_ids.clear();
+  b->dense_n.clear();
+  b->dense_mo.clear();
+  int dmaxn = 0, dmaxnsh = 0, dmaxnat = 0;
+  for (int q = 0; q < n_dense; ++q) {
+    const int mm = h_order[q];
+    if (st_m[mm] != GFN1_OK) continue;
+    b->dense_ids.push_back(mm);
+    b->dense_n.push_back(n_m[mm]);
+    b->dense_mo.push_back(h_mat[mm]);
+    dmaxn = std::max(dmaxn, n_m[mm]);
+    dmaxnsh = std::max(dmaxnsh, nsh_m[mm]);
+    dmaxnat = std::max(dmaxnat, atom_offsets[mm + 1] - atom_offsets[mm]);
+  }
+  int n_large = n_dense;
   while (n_large < nmol && n_m[h_order[n_large]] > kLargeN) ++n_large;
   long long ws_total = 0;
   for (int c = 0; c < 2; ++c) {
     gfn1_batch::SccClass& K = b->cls[c];
-    K.q_begin = c == 0 ? 0 : n_large;
+    K.q_begin = c == 0 ? n_dense : n_large;
     K.q_end = c == 0 ? n_large : nmol;
     K.nt = c == 0 ? 512 : 256;
     K.maxn = K.maxnsh = K.maxnat = 0;
@@ -714,6 +763,52 @@ int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t*
             b->pairbuf.ensure(8 * std::max<long long>(pair_total, 1)) && b->cn.ensure(natoms) &&
             b->shell_pot.ensure(nshells) && b->se.ensure(nshells) && b->grad_classic.ensure(3 * natoms);
   if (!ok) return fail(eng, GFN1_E_DEVICE, "device allocation failed for the batch workspace");
+  if (!b->dense_ids.empty()) {
+    DenseWork& dw = b->dw;
+    if (!dw.blas) {
+      cublasHandle_t hb;
+      cusolverDnHandle_t hs;
+      if (cublasCreate(&hb) != CUBLAS_STATUS_SUCCESS) return fail(eng, GFN1_E_DEVICE, "cublasCreate failed");
+      dw.blas = hb;
+      if (cusolverDnCreate(&hs) != CUSOLVER_STATUS_SUCCESS) return fail(eng, GFN1_E_DEVICE, "cusolverDnCreate failed");
+      dw.solver = hs;
+      if (cudaHostAlloc(&dw.h_state, 4 * sizeof(int), cudaHostAllocDefault) != cudaSuccess)
+        return fail(eng, GFN1_E_DEVICE, "pinned host allocation failed");
+      if (cudaStreamCreateWithFlags(&b->dense_stream, cudaStreamNonBlocking) != cudaSuccess ||
+          cudaEventCreateWithFlags(&b->ev_djoin, cudaEventDisableTiming) != cudaSuccess)
+        return fail(eng, GFN1_E_DEVICE, "stream creation failed");
+    }
+    const long long lwork = dense_solver_lwork(dw.solver, dmaxn);
+    if (lwork < 0) return fail(eng, GFN1_E_DEVICE, "cuSOLVER workspace query failed");
+    const long long n2 = (long long)dmaxn * dmaxn;
+    const long long wsd = dense_ws_doubles(dmaxnsh, b->cap, dmaxnat);
+    const long long stated = ((long long)dense_state_bytes() + 7) / 8;
+    const long long total = 6 * n2 + 4LL * dmaxn + lwork + wsd + stated + 64;
+    if (!b->dense_buf.ensure((size_t)total) || !b->dense_info.ensure(4))
+      return fail(eng, GFN1_E_DEVICE, "device allocation failed for the large-molecule path");
+    if (dense_smem_bytes(dmaxnsh, dmaxn, dmaxnat) > 200 * 1024)
+      return fail(eng, GFN1_E_INVALID_INPUT, "molecule too large for the large-molecule path's index tables");
+    double* p = b->dense_buf.p;
+    dw.maxn = dmaxn;
+    dw.maxnsh = dmaxnsh;
+    dw.maxnat = dmaxnat;
+    dw.cap = b->cap;
+    dw.L = p; p += n2;
+    dw.Hp = p; p += n2;
+    dw.Mm = p; p += n2;
+    dw.F = p; p += n2;
+    dw.C = p; p += n2;
+    dw.D = p; p += n2;
+    dw.eps = p; p += dmaxn;
+    dw.occ = p; p += dmaxn;
+    dw.pop = p; p += dmaxn;
+    dw.vao = p; p += dmaxn;
+    dw.solver_work = p; p += lwork;
+    dw.lwork = lwork;
+    dw.ws = p; p += wsd;
+    dw.state = p;
+    dw.info = b->dense_info.p;
+  }
   b->guess = eng->guess;
   if (b->guess && !(b->gx.ensure((size_t)kGuessIn * std::max<long long>(natoms, 1)) &&
                     b->gy.ensure((size_t)kGuessOut * std::max<long long>(natoms, 1)) &&
@@ -787,6 +882,18 @@ int launch_stage(gfn1_batch* b, int stage, cudaStream_t st) {
     }
     if ((e = cudaEventRecord(b->ev_join, b->side)) != cudaSuccess || (e = cudaStreamWaitEvent(st, b->ev_join, 0)) != cudaSuccess)
       return cuda_fail(eng, e, "stream join");
+    if (!b->dense_ids.empty()) {  // large molecules: host-driven, one at a time, next to the class launches
+      // wait for the setup kernel only (ev_fork was recorded before the class launches)
+      if ((e = cudaStreamWaitEvent(b->dense_stream, b->ev_fork, 0)) != cudaSuccess)
+        return cuda_fail(eng, e, "stream fork");
+      for (size_t q = 0; q < b->dense_ids.size(); ++q)
+        if ((e = run_dense_molecule(B, M, so, b->dense_ids[q], b->dense_n[q], b->dense_mo[q], b->dw, b->dense_stream)) !=
+            cudaSuccess)
+          return cuda_fail(eng, e, "large-molecule SCC");
+      if ((e = cudaEventRecord(b->ev_djoin, b->dense_stream)) != cudaSuccess ||
+          (e = cudaStreamWaitEvent(st, b->ev_djoin, 0)) != cudaSuccess)
+        return cuda_fail(eng, e, "stream join");
+    }
   } else if (stage == 2) {
     if (!b->opt.compute_gradient) return GFN1_OK;
     const size_t smem = sizeof(double) * 7 * (size_t)b->max_nat + sizeof(int) * (3 * (size_t)b->max_nat + 2);

@@ -27,6 +27,8 @@
 // Fermi smearing (bisection to the bracket fixed point, :3853-3921), the
 // convergence test (:1881), Broyden mixing (:3203-3309, :3759-3806) and the final
 // energy assembly (:1957-2053) follow the reference step by step.
+#include <cublas_v2.h>
+#include <cusolverDn.h>
 #include <float.h>
 
 #include "common.cuh"
@@ -763,6 +765,315 @@ __device__ void back_transform(const double* A, int lda, const double* tau, int 
   }
 }
 
+// Index tables of one molecule (one thread): shell -> atom, shell -> index
+// within its atom, shell -> first AO, AO -> shell, atom -> first shell.
+__device__ void build_index_tables(const Batch& B, const Model& M, int a0, int nat, int* sh_atom, int* sh_k,
+                                   int* sh_ao0, int* ao_sh, int* atom_sh) {
+  int s = 0, o = 0;
+  for (int a = 0; a < nat; ++a) {
+    const ElemTable& el = M.elem[B.z[a0 + a]];
+    atom_sh[a] = s;
+    for (int k = 0; k < el.nsh; ++k) {
+      sh_atom[s + k] = a;
+      sh_k[s + k] = k;
+      sh_ao0[s + k] = o + el.ao_first[k];
+      for (int q = 0; q < 2 * el.l[k] + 1; ++q) ao_sh[o + el.ao_first[k] + q] = s + k;
+    }
+    s += el.nsh;
+    o += el.nao;
+  }
+  atom_sh[nat] = s;
+}
+
+// Per-molecule view shared by the SCC stages: sizes, offsets and the index
+// tables (shell -> atom, shell -> shell index within its atom, shell -> first
+// AO, AO -> shell, atom -> first shell), plus the molecule's Coulomb matrix.
+struct MolCtx {
+  int m, a0, nat, sh0, nsh, N;
+  const int *sh_atom, *sh_k, *sh_ao0, *ao_sh, *atom_sh;
+  const double* G;
+};
+
+// (1) Shell potential of the input charges (src/coulomb.rs:140-193):
+// w.qat, w.vsh and the AO potential vao.
+template <int NT>
+__device__ void stage_potential(const Batch& B, const Model& M, const MolCtx& c, CtaWs& w, double* vao) {
+  const int tid = threadIdx.x;
+  const int a0 = c.a0, nat = c.nat, nsh = c.nsh, N = c.N;
+  const int *sh_atom = c.sh_atom, *ao_sh = c.ao_sh, *atom_sh = c.atom_sh;
+  const double* G = c.G;
+  for (int a = tid; a < nat; a += NT) {
+    double q = 0.0;
+    for (int s = atom_sh[a]; s < atom_sh[a + 1]; ++s) q += w.qin[s];
+    w.qat[a] = q;
+  }
+  __syncthreads();
+  for (int i = tid; i < nsh; i += NT) {
+    double v = 0.0;
+    for (int j = 0; j < nsh; ++j) v += G[(long long)i * nsh + j] * w.qin[j];
+    const int a = sh_atom[i];
+    const double qa = w.qat[a];
+    v += qa * qa * M.elem[B.z[a0 + a]].gam3;
+    w.vsh[i] = v;
+  }
+  __syncthreads();
+  for (int i = tid; i < N; i += NT) vao[i] = w.vsh[ao_sh[i]];
+  __syncthreads();
+}
+
+// (9) Output shell and atomic charges, electronic energy, second- and
+// third-order energies and the charge rms (src/electronic.rs:2173-2191,
+// :3160-3200); also the output potential w.vout.
+template <int NT>
+__device__ void stage_charges_energy(const Batch& B, const Model& M, const MolCtx& c, CtaWs& w, const double* pop,
+                                     const double* occ, const double* eps, const double* vao, int nocc, SccShared& sh,
+                                     double& e_el, double& e2, double& e3, double& rms) {
+  const int tid = threadIdx.x;
+  const int a0 = c.a0, nat = c.nat, nsh = c.nsh, N = c.N;
+  const int *sh_atom = c.sh_atom, *sh_k = c.sh_k, *sh_ao0 = c.sh_ao0, *atom_sh = c.atom_sh;
+  const double* G = c.G;
+  for (int s = tid; s < nsh; s += NT) {
+    const ElemTable& el = M.elem[B.z[a0 + sh_atom[s]]];
+    const int k = sh_k[s];
+    double p = 0.0;
+    for (int q = 0; q < 2 * el.l[k] + 1; ++q) p += pop[sh_ao0[s] + q];
+    w.qout[s] = el.refocc[k] - p;
+  }
+  double part = 0.0;
+  for (int i = tid; i < N; i += NT) part += (i < nocc ? occ[i] * eps[i] : 0.0) + vao[i] * pop[i];
+  e_el = block_sum(part, sh.red);
+  for (int a = tid; a < nat; a += NT) {
+    double q = 0.0;
+    for (int s = atom_sh[a]; s < atom_sh[a + 1]; ++s) q += w.qout[s];
+    w.qat[a] = q;
+  }
+  __syncthreads();
+  double p2 = 0.0, p3 = 0.0, pr = 0.0;
+  for (int i = tid; i < nsh; i += NT) {
+    double v = 0.0;
+    for (int j = 0; j < nsh; ++j) v += G[(long long)i * nsh + j] * w.qout[j];
+    p2 += w.qout[i] * v;
+    const int a = sh_atom[i];
+    const double qa = w.qat[a];
+    const double g3 = M.elem[B.z[a0 + a]].gam3;
+    w.vout[i] = v + qa * qa * g3;
+    const double r = w.qout[i] - w.qin[i];
+    pr += r * r;
+  }
+  for (int a = tid; a < nat; a += NT) {
+    const double qa = w.qat[a];
+    p3 += qa * qa * qa * M.elem[B.z[a0 + a]].gam3 / 3.0;
+  }
+  e2 = 0.5 * block_sum(p2, sh.red);
+  e3 = block_sum(p3, sh.red);
+  rms = nsh ? sqrt(block_sum(pr, sh.red) / nsh) : 0.0;
+}
+
+// (10) Charge mixing: modified Broyden (src/electronic.rs:3203-3309), linear
+// damped step on the first iteration, a singular solve or an untrusted vector
+// (:3311-3316, :3759-3761); the next input charges land in w.qin.
+template <int NT>
+__device__ void stage_mix(const SccOptions& opt, const MolCtx& c, CtaWs& w, int cap, int& bro_iter, SccShared& sh) {
+  constexpr int NW = NT / 32;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int nsh = c.nsh;
+  const double mixing = fmin(1.0, fmax(0.01, opt.mixing));
+  const int memory = max(opt.broyden_size, 2);
+  bool have_next = false;
+  if (opt.broyden) {
+    bro_iter += 1;
+    if (bro_iter == 1) {
+      for (int s = tid; s < nsh; s += NT) {
+        const double r = w.qout[s] - w.qin[s];
+        w.dqlast[s] = r;
+        w.qlast[s] = w.qin[s];
+        w.qnext[s] = w.qin[s] + mixing * r;
+      }
+      have_next = true;
+      __syncthreads();
+    } else {
+      const int itn = bro_iter - 1;
+      const int it1 = (itn - 1) % memory;
+      const int slot = it1 % cap;
+      double pn = 0.0, pd = 0.0;
+      for (int s = tid; s < nsh; s += NT) {
+        const double r = w.qout[s] - w.qin[s];
+        pn += r * r;
+        const double dfv = r - w.dqlast[s];
+        pd += dfv * dfv;
+      }
+      const double dqn = sqrt(block_sum(pn, sh.red));
+      const double dfn = sqrt(block_sum(pd, sh.red));
+      const double inv = 1.0 / fmax(dfn, DBL_EPSILON);
+      double* dfs = w.df + (long long)slot * nsh;
+      double* us = w.u + (long long)slot * nsh;
+      for (int s = tid; s < nsh; s += NT) {
+        const double r = w.qout[s] - w.qin[s];
+        const double dfv = (r - w.dqlast[s]) * inv;
+        dfs[s] = dfv;
+        us[s] = mixing * dfv + inv * (w.qin[s] - w.qlast[s]);
+      }
+      if (tid == 0) {
+        double om = dqn > 0.01 / 100000.0 ? 0.01 / dqn : 100000.0;
+        if (om < 1.0) om = 1.0;
+        w.omega[slot] = om;
+      }
+      __syncthreads();
+      const int start = itn > memory ? itn - memory + 1 : 1;
+      const int mact = itn - start + 1;
+      // dot products df_new . df_j for every active slot, and c_j = omega_j df_j . dq
+      for (int r = wid; r < mact; r += NW) {
+        const int sj = ((start + r - 1) % memory) % cap;
+        const double* dj = w.df + (long long)sj * nsh;
+        double s1 = 0.0, s2 = 0.0;
+        for (int s = lane; s < nsh; s += 32) {
+          s1 += dfs[s] * dj[s];
+          s2 += dj[s] * (w.qout[s] - w.qin[s]);
+        }
+        s1 = warp_sum(s1);
+        s2 = warp_sum(s2);
+        if (lane == 0) {
+          w.dots[(long long)slot * cap + sj] = s1;
+          w.dots[(long long)sj * cap + slot] = s1;
+          w.cvec[r] = s2;
+        }
+      }
+      __syncthreads();
+      for (int idx = tid; idx < mact * mact; idx += NT) {
+        const int r = idx / mact, c = idx % mact;
+        const int si = ((start + r - 1) % memory) % cap, sj = ((start + c - 1) % memory) % cap;
+        double b = w.omega[si] * w.omega[sj] * w.dots[(long long)si * cap + sj];
+        if (r == c) b += 0.01 * 0.01;
+        w.beta[(long long)r * mact + c] = b;
+      }
+      for (int r = tid; r < mact; r += NT) {
+        const int si = ((start + r - 1) % memory) % cap;
+        w.cvec[r] *= w.omega[si];
+      }
+      __syncthreads();
+      // Gauss-Jordan with partial pivoting (src/electronic.rs:3767-3806)
+      bool ok = true;
+      for (int col = 0; col < mact; ++col) {
+        if (tid == 0) {
+          int piv = col;
+          double pabs = fabs(w.beta[(long long)col * mact + col]);
+          for (int r = col + 1; r < mact; ++r) {
+            const double v = fabs(w.beta[(long long)r * mact + col]);
+            if (v > pabs) {
+              piv = r;
+              pabs = v;
+            }
+          }
+          sh.iscal[1] = (pabs < 1e-18) ? -1 : piv;
+        }
+        __syncthreads();
+        const int piv = sh.iscal[1];
+        if (piv < 0) {
+          ok = false;
+          break;
+        }
+        if (piv != col) {
+          for (int j = tid; j < mact; j += NT) {
+            const double t = w.beta[(long long)piv * mact + j];
+            w.beta[(long long)piv * mact + j] = w.beta[(long long)col * mact + j];
+            w.beta[(long long)col * mact + j] = t;
+          }
+          if (tid == 0) {
+            const double t = w.cvec[piv];
+            w.cvec[piv] = w.cvec[col];
+            w.cvec[col] = t;
+          }
+          __syncthreads();
+        }
+        const double dg = w.beta[(long long)col * mact + col];
+        __syncthreads();
+        for (int j = col + tid; j < mact; j += NT) w.beta[(long long)col * mact + j] /= dg;
+        if (tid == 0) w.cvec[col] /= dg;
+        __syncthreads();
+        for (int idx = tid; idx < mact * (mact - col); idx += NT) {
+          const int r = idx / (mact - col), j = col + idx % (mact - col);
+          if (r == col) continue;
+          const double f = w.beta[(long long)r * mact + col];
+          if (f == 0.0 || j == col) continue;
+          w.beta[(long long)r * mact + j] -= f * w.beta[(long long)col * mact + j];
+        }
+        for (int r = tid; r < mact; r += NT) {
+          if (r == col) continue;
+          const double f = w.beta[(long long)r * mact + col];
+          if (f != 0.0) w.cvec[r] -= f * w.cvec[col];
+        }
+        __syncthreads();
+        for (int r = tid; r < mact; r += NT)
+          if (r != col) w.beta[(long long)r * mact + col] = 0.0;
+        __syncthreads();
+      }
+      if (ok) {
+        for (int s = tid; s < nsh; s += NT) {
+          const double r = w.qout[s] - w.qin[s];
+          double qn = w.qin[s] + mixing * r;
+          for (int rr = 0; rr < mact; ++rr) {
+            const int si = ((start + rr - 1) % memory) % cap;
+            qn -= w.omega[si] * w.cvec[rr] * w.u[(long long)si * nsh + s];
+          }
+          w.qnext[s] = qn;
+          w.dqlast[s] = r;
+          w.qlast[s] = w.qin[s];
+        }
+        have_next = true;
+      }
+      __syncthreads();
+    }
+    if (have_next) {  // trusted_charge_vector (src/electronic.rs:3759-3761)
+      int bad = 0;
+      for (int s = tid; s < nsh; s += NT)
+        if (!isfinite(w.qnext[s]) || fabs(w.qnext[s]) >= 10.0) bad = 1;
+      if (block_max((double)bad, sh.red) > 0.0) have_next = false;
+    }
+  }
+  if (!have_next)
+    for (int s = tid; s < nsh; s += NT) w.qnext[s] = w.qin[s] + mixing * (w.qout[s] - w.qin[s]);
+  __syncthreads();
+  for (int s = tid; s < nsh; s += NT) w.qin[s] = w.qnext[s];
+}
+
+// Results of a finished SCC: energy terms, iterations, status, Fermi level,
+// Mulliken dipole, shell charges and potential, atomic charges.
+template <int NT>
+__device__ void stage_results(const Batch& B, const MolCtx& c, CtaWs& w, int iter, bool converged, double e_el,
+                              double e2, double e3, double ts, double mu) {
+  const int tid = threadIdx.x;
+  const int a0 = c.a0, nat = c.nat, nsh = c.nsh;
+  const int m = c.m, sh0 = c.sh0;
+  if (tid == 0) {
+    double* t = B.terms + (long long)m * kTerms;
+    const double erep = t[2], edisp = t[7];
+    const double total_internal = e_el + e2 + e3 + erep + edisp;
+    t[0] = total_internal + ts;
+    t[1] = total_internal;
+    t[3] = e_el;
+    t[4] = e2;
+    t[5] = e3;
+    t[14] = ts;
+    B.iterations[m] = iter;
+    B.status[m] = converged ? kOk : kErrSccNotConverged;
+    B.fermi[m] = mu;
+    double dx = 0, dy = 0, dz = 0;
+    for (int a = 0; a < nat; ++a) {
+      dx += w.qat[a] * B.xyz[3 * (a0 + a)];
+      dy += w.qat[a] * B.xyz[3 * (a0 + a) + 1];
+      dz += w.qat[a] * B.xyz[3 * (a0 + a) + 2];
+    }
+    B.dipole[3 * m] = dx;
+    B.dipole[3 * m + 1] = dy;
+    B.dipole[3 * m + 2] = dz;
+  }
+  for (int s = tid; s < nsh; s += NT) {
+    B.shell_q[sh0 + s] = w.qout[s];
+    B.shell_pot[sh0 + s] = w.vout[s];
+  }
+  for (int a = tid; a < nat; a += NT) B.atom_q[a0 + a] = w.qat[a];
+}
+
 template <int NT>
 __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& opt, const SccLaunch& SL, int m,
                              SccShared& sh, int* sh_atom, int* sh_k, int* ao_sh, int* atom_sh, int* sh_ao0,
@@ -799,25 +1110,13 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
 
   // ---- index tables
   if (tid == 0) {
-    int s = 0, o = 0;
-    for (int a = 0; a < nat; ++a) {
-      const ElemTable& el = M.elem[B.z[a0 + a]];
-      atom_sh[a] = s;
-      for (int k = 0; k < el.nsh; ++k) {
-        sh_atom[s + k] = a;
-        sh_k[s + k] = k;
-        sh_ao0[s + k] = o + el.ao_first[k];
-        for (int q = 0; q < 2 * el.l[k] + 1; ++q) ao_sh[o + el.ao_first[k] + q] = s + k;
-      }
-      s += el.nsh;
-      o += el.nao;
-    }
-    atom_sh[nat] = s;
+    build_index_tables(B, M, a0, nat, sh_atom, sh_k, sh_ao0, ao_sh, atom_sh);
     sh.iscal[0] = kOk;
   }
   __syncthreads();
 
   StageClock clk(B.stage_cycles);
+  const MolCtx mc{m, a0, nat, sh0, nsh, N, sh_atom, sh_k, sh_ao0, ao_sh, atom_sh, G};
   // ---- Cholesky S = L L^T (right-looking, in place on L)
   for (long long i = tid; i < (long long)N * N; i += NT) L[i] = S[i];
   __syncthreads();
@@ -886,8 +1185,6 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
   const double nelec = nref - B.charge[m];
   const double kt = fmax(opt.etemp, 0.0) * kBoltzmann;
   for (int s = tid; s < nsh; s += NT) w.qin[s] = B.init_q ? B.init_q[sh0 + s] : 0.0;
-  const double mixing = fmin(1.0, fmax(0.01, opt.mixing));
-  const int memory = max(opt.broyden_size, 2);
   const int nneed0 = min(N, max(1, (int)ceil(0.5 * nelec) + 8));
   int bro_iter = 0;
   double last_e = 0.0;
@@ -900,24 +1197,8 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
   clk.mark(kStPrologue);
 
   for (iter = 1; iter <= opt.max_scc; ++iter) {
-    // (1) shell potential from the input charges (src/coulomb.rs:140-193)
-    for (int a = tid; a < nat; a += NT) {
-      double q = 0.0;
-      for (int s = atom_sh[a]; s < atom_sh[a + 1]; ++s) q += w.qin[s];
-      w.qat[a] = q;
-    }
-    __syncthreads();
-    for (int i = tid; i < nsh; i += NT) {
-      double v = 0.0;
-      for (int j = 0; j < nsh; ++j) v += G[(long long)i * nsh + j] * w.qin[j];
-      const int a = sh_atom[i];
-      const double qa = w.qat[a];
-      v += qa * qa * M.elem[B.z[a0 + a]].gam3;
-      w.vsh[i] = v;
-    }
-    __syncthreads();
-    for (int i = tid; i < N; i += NT) vao[i] = w.vsh[ao_sh[i]];
-    __syncthreads();
+    // (1) shell potential from the input charges
+    stage_potential<NT>(B, M, mc, w, vao);
     // (2) F' = H0' - 1/2 (M + M^T), M = L^-1 diag(v) L; warps own 4-row groups,
     //     lanes 32 columns; L rows are read coalesced, L^-1 entries broadcast
     for (int rg = wid; rg * 4 < N; rg += NW) {
@@ -1104,42 +1385,8 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     }
     __syncthreads();
     clk.mark(kStPop);
-    // (9) output charges, energies (src/electronic.rs:2173-2191)
-    for (int s = tid; s < nsh; s += NT) {
-      const ElemTable& el = M.elem[B.z[a0 + sh_atom[s]]];
-      const int k = sh_k[s];
-      double p = 0.0;
-      for (int q = 0; q < 2 * el.l[k] + 1; ++q) p += pop[sh_ao0[s] + q];
-      w.qout[s] = el.refocc[k] - p;
-    }
-    double part = 0.0;
-    for (int i = tid; i < N; i += NT) part += (i < nocc ? occ[i] * eps[i] : 0.0) + vao[i] * pop[i];
-    e_el = block_sum(part, sh.red);
-    for (int a = tid; a < nat; a += NT) {
-      double q = 0.0;
-      for (int s = atom_sh[a]; s < atom_sh[a + 1]; ++s) q += w.qout[s];
-      w.qat[a] = q;
-    }
-    __syncthreads();
-    double p2 = 0.0, p3 = 0.0, pr = 0.0;
-    for (int i = tid; i < nsh; i += NT) {
-      double v = 0.0;
-      for (int j = 0; j < nsh; ++j) v += G[(long long)i * nsh + j] * w.qout[j];
-      p2 += w.qout[i] * v;
-      const int a = sh_atom[i];
-      const double qa = w.qat[a];
-      const double g3 = M.elem[B.z[a0 + a]].gam3;
-      w.vout[i] = v + qa * qa * g3;
-      const double r = w.qout[i] - w.qin[i];
-      pr += r * r;
-    }
-    for (int a = tid; a < nat; a += NT) {
-      const double qa = w.qat[a];
-      p3 += qa * qa * qa * M.elem[B.z[a0 + a]].gam3 / 3.0;
-    }
-    e2 = 0.5 * block_sum(p2, sh.red);
-    e3 = block_sum(p3, sh.red);
-    rms = nsh ? sqrt(block_sum(pr, sh.red) / nsh) : 0.0;
+    // (9) output charges, energies
+    stage_charges_energy<NT>(B, M, mc, w, pop, occ, eps, vao, nocc, sh, e_el, e2, e3, rms);
     const double escc = e_el + e2 + e3 + ts;
     const double err = have_e ? fabs(escc - last_e) : INFINITY;
     if (err < opt.energy_tol && rms < opt.charge_tol) {
@@ -1148,161 +1395,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     }
     clk.mark(kStEnergy);
     // (10) charge mixing
-    bool have_next = false;
-    if (opt.broyden) {
-      bro_iter += 1;
-      if (bro_iter == 1) {
-        for (int s = tid; s < nsh; s += NT) {
-          const double r = w.qout[s] - w.qin[s];
-          w.dqlast[s] = r;
-          w.qlast[s] = w.qin[s];
-          w.qnext[s] = w.qin[s] + mixing * r;
-        }
-        have_next = true;
-        __syncthreads();
-      } else {
-        const int itn = bro_iter - 1;
-        const int it1 = (itn - 1) % memory;
-        const int slot = it1 % cap;
-        double pn = 0.0, pd = 0.0;
-        for (int s = tid; s < nsh; s += NT) {
-          const double r = w.qout[s] - w.qin[s];
-          pn += r * r;
-          const double dfv = r - w.dqlast[s];
-          pd += dfv * dfv;
-        }
-        const double dqn = sqrt(block_sum(pn, sh.red));
-        const double dfn = sqrt(block_sum(pd, sh.red));
-        const double inv = 1.0 / fmax(dfn, DBL_EPSILON);
-        double* dfs = w.df + (long long)slot * nsh;
-        double* us = w.u + (long long)slot * nsh;
-        for (int s = tid; s < nsh; s += NT) {
-          const double r = w.qout[s] - w.qin[s];
-          const double dfv = (r - w.dqlast[s]) * inv;
-          dfs[s] = dfv;
-          us[s] = mixing * dfv + inv * (w.qin[s] - w.qlast[s]);
-        }
-        if (tid == 0) {
-          double om = dqn > 0.01 / 100000.0 ? 0.01 / dqn : 100000.0;
-          if (om < 1.0) om = 1.0;
-          w.omega[slot] = om;
-        }
-        __syncthreads();
-        const int start = itn > memory ? itn - memory + 1 : 1;
-        const int mact = itn - start + 1;
-        // dot products df_new . df_j for every active slot, and c_j = omega_j df_j . dq
-        for (int r = wid; r < mact; r += NW) {
-          const int sj = ((start + r - 1) % memory) % cap;
-          const double* dj = w.df + (long long)sj * nsh;
-          double s1 = 0.0, s2 = 0.0;
-          for (int s = lane; s < nsh; s += 32) {
-            s1 += dfs[s] * dj[s];
-            s2 += dj[s] * (w.qout[s] - w.qin[s]);
-          }
-          s1 = warp_sum(s1);
-          s2 = warp_sum(s2);
-          if (lane == 0) {
-            w.dots[(long long)slot * cap + sj] = s1;
-            w.dots[(long long)sj * cap + slot] = s1;
-            w.cvec[r] = s2;
-          }
-        }
-        __syncthreads();
-        for (int idx = tid; idx < mact * mact; idx += NT) {
-          const int r = idx / mact, c = idx % mact;
-          const int si = ((start + r - 1) % memory) % cap, sj = ((start + c - 1) % memory) % cap;
-          double b = w.omega[si] * w.omega[sj] * w.dots[(long long)si * cap + sj];
-          if (r == c) b += 0.01 * 0.01;
-          w.beta[(long long)r * mact + c] = b;
-        }
-        for (int r = tid; r < mact; r += NT) {
-          const int si = ((start + r - 1) % memory) % cap;
-          w.cvec[r] *= w.omega[si];
-        }
-        __syncthreads();
-        // Gauss-Jordan with partial pivoting (src/electronic.rs:3767-3806)
-        bool ok = true;
-        for (int col = 0; col < mact; ++col) {
-          if (tid == 0) {
-            int piv = col;
-            double pabs = fabs(w.beta[(long long)col * mact + col]);
-            for (int r = col + 1; r < mact; ++r) {
-              const double v = fabs(w.beta[(long long)r * mact + col]);
-              if (v > pabs) {
-                piv = r;
-                pabs = v;
-              }
-            }
-            sh.iscal[1] = (pabs < 1e-18) ? -1 : piv;
-          }
-          __syncthreads();
-          const int piv = sh.iscal[1];
-          if (piv < 0) {
-            ok = false;
-            break;
-          }
-          if (piv != col) {
-            for (int j = tid; j < mact; j += NT) {
-              const double t = w.beta[(long long)piv * mact + j];
-              w.beta[(long long)piv * mact + j] = w.beta[(long long)col * mact + j];
-              w.beta[(long long)col * mact + j] = t;
-            }
-            if (tid == 0) {
-              const double t = w.cvec[piv];
-              w.cvec[piv] = w.cvec[col];
-              w.cvec[col] = t;
-            }
-            __syncthreads();
-          }
-          const double dg = w.beta[(long long)col * mact + col];
-          __syncthreads();
-          for (int j = col + tid; j < mact; j += NT) w.beta[(long long)col * mact + j] /= dg;
-          if (tid == 0) w.cvec[col] /= dg;
-          __syncthreads();
-          for (int idx = tid; idx < mact * (mact - col); idx += NT) {
-            const int r = idx / (mact - col), j = col + idx % (mact - col);
-            if (r == col) continue;
-            const double f = w.beta[(long long)r * mact + col];
-            if (f == 0.0 || j == col) continue;
-            w.beta[(long long)r * mact + j] -= f * w.beta[(long long)col * mact + j];
-          }
-          for (int r = tid; r < mact; r += NT) {
-            if (r == col) continue;
-            const double f = w.beta[(long long)r * mact + col];
-            if (f != 0.0) w.cvec[r] -= f * w.cvec[col];
-          }
-          __syncthreads();
-          for (int r = tid; r < mact; r += NT)
-            if (r != col) w.beta[(long long)r * mact + col] = 0.0;
-          __syncthreads();
-        }
-        if (ok) {
-          for (int s = tid; s < nsh; s += NT) {
-            const double r = w.qout[s] - w.qin[s];
-            double qn = w.qin[s] + mixing * r;
-            for (int rr = 0; rr < mact; ++rr) {
-              const int si = ((start + rr - 1) % memory) % cap;
-              qn -= w.omega[si] * w.cvec[rr] * w.u[(long long)si * nsh + s];
-            }
-            w.qnext[s] = qn;
-            w.dqlast[s] = r;
-            w.qlast[s] = w.qin[s];
-          }
-          have_next = true;
-        }
-        __syncthreads();
-      }
-      if (have_next) {  // trusted_charge_vector (src/electronic.rs:3759-3761)
-        int bad = 0;
-        for (int s = tid; s < nsh; s += NT)
-          if (!isfinite(w.qnext[s]) || fabs(w.qnext[s]) >= 10.0) bad = 1;
-        if (block_max((double)bad, sh.red) > 0.0) have_next = false;
-      }
-    }
-    if (!have_next)
-      for (int s = tid; s < nsh; s += NT) w.qnext[s] = w.qin[s] + mixing * (w.qout[s] - w.qin[s]);
-    __syncthreads();
-    for (int s = tid; s < nsh; s += NT) w.qin[s] = w.qnext[s];
+    stage_mix<NT>(opt, mc, w, cap, bro_iter, sh);
     last_e = escc;
     have_e = true;
     __syncthreads();
@@ -1311,34 +1404,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
   if (iter > opt.max_scc) iter = opt.max_scc;
 
   // ---- results
-  if (tid == 0) {
-    double* t = B.terms + (long long)m * kTerms;
-    const double erep = t[2], edisp = t[7];
-    const double total_internal = e_el + e2 + e3 + erep + edisp;
-    t[0] = total_internal + ts;
-    t[1] = total_internal;
-    t[3] = e_el;
-    t[4] = e2;
-    t[5] = e3;
-    t[14] = ts;
-    B.iterations[m] = iter;
-    B.status[m] = converged ? kOk : kErrSccNotConverged;
-    B.fermi[m] = mu;
-    double dx = 0, dy = 0, dz = 0;
-    for (int a = 0; a < nat; ++a) {
-      dx += w.qat[a] * B.xyz[3 * (a0 + a)];
-      dy += w.qat[a] * B.xyz[3 * (a0 + a) + 1];
-      dz += w.qat[a] * B.xyz[3 * (a0 + a) + 2];
-    }
-    B.dipole[3 * m] = dx;
-    B.dipole[3 * m + 1] = dy;
-    B.dipole[3 * m + 2] = dz;
-  }
-  for (int s = tid; s < nsh; s += NT) {
-    B.shell_q[sh0 + s] = w.qout[s];
-    B.shell_pot[sh0 + s] = w.vout[s];
-  }
-  for (int a = tid; a < nat; a += NT) B.atom_q[a0 + a] = w.qat[a];
+  stage_results<NT>(B, mc, w, iter, converged, e_el, e2, e3, ts, mu);
   // density and energy-weighted density of the last diagonalisation
   // (src/linalg.rs:243-273), kept per molecule for the gradient kernel
   for (int i = wid; i < N; i += NW)
@@ -1382,6 +1448,310 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) scc_kernel(Batch B, M
     if (B.status[m] != kOk) continue;  // rejected during setup
     scc_molecule<NT>(B, M, opt, SL, m, sh, sh_atom, sh_k, ao_sh, atom_sh, sh_ao0, vec, As, as_cap);
   }
+}
+
+// ============================================================ large molecules
+// Molecules too large for one SM run the same SCC (same stage functions for
+// potential, charges, energies, mixing and results) with the matrix algebra
+// spread over the whole GPU: cuSOLVER Cholesky and symmetric eigensolver,
+// cuBLAS triangular products and GEMMs, and element-wise kernels.  All
+// matrices are column-major; S, H0, P and W are symmetric, so the batch's
+// row-major copies are used as they are.
+
+struct DenseState {
+  int status, nocc, converged, iter, bro_iter, have_e;
+  double last_e, e_el, e2, e3, ts, mu, rms, nelec, kt;
+};
+constexpr int kDenseNT = 512;
+
+__host__ __device__ inline size_t dense_table_bytes(int maxnsh, int maxn, int maxnat) {
+  return ((size_t)4 * scc_ints(maxnsh, maxn, maxnat) + 15) & ~(size_t)15;
+}
+
+struct DenseTables {
+  int *sh_atom, *sh_k, *sh_ao0, *ao_sh, *atom_sh;
+};
+__device__ DenseTables dense_tables(unsigned char* raw, int maxnsh, int maxn) {
+  DenseTables t;
+  t.sh_atom = (int*)raw;
+  t.sh_k = t.sh_atom + maxnsh;
+  t.sh_ao0 = t.sh_k + maxnsh;
+  t.ao_sh = t.sh_ao0 + maxnsh;
+  t.atom_sh = t.ao_sh + maxn;
+  return t;
+}
+
+// Index tables in shared memory and the molecule context, for the one-CTA
+// kernels of the large path.
+__device__ MolCtx dense_context(const Batch& B, const Model& M, int m, const DenseWork& dw, unsigned char* raw) {
+  const int a0 = B.atom_off[m], nat = B.atom_off[m + 1] - a0;
+  const int sh0 = B.shell_off[m], nsh = B.shell_off[m + 1] - sh0;
+  const int N = B.ao_off[m + 1] - B.ao_off[m];
+  DenseTables t = dense_tables(raw, dw.maxnsh, dw.maxn);
+  if (threadIdx.x == 0) build_index_tables(B, M, a0, nat, t.sh_atom, t.sh_k, t.sh_ao0, t.ao_sh, t.atom_sh);
+  __syncthreads();
+  return MolCtx{m, a0, nat, sh0, nsh, N, t.sh_atom, t.sh_k, t.sh_ao0, t.ao_sh, t.atom_sh, B.gam + B.gam_off[m]};
+}
+
+__global__ void __launch_bounds__(kDenseNT, 1) dense_init_kernel(Batch B, Model M, SccOptions opt, int m, DenseWork dw) {
+  extern __shared__ __align__(16) unsigned char raw[];
+  const MolCtx c = dense_context(B, M, m, dw, raw);
+  DenseState* st = (DenseState*)dw.state;
+  CtaWs w = cta_ws(dw.ws, 1, dw.maxnsh, dw.cap);
+  for (int s = threadIdx.x; s < c.nsh; s += kDenseNT) w.qin[s] = B.init_q ? B.init_q[c.sh0 + s] : 0.0;
+  if (threadIdx.x == 0) {
+    double nref = 0.0;
+    for (int s = 0; s < c.nsh; ++s) nref += M.elem[B.z[c.a0 + c.sh_atom[s]]].refocc[c.sh_k[s]];
+    // the reference rejects overlaps with an eigenvalue <= 1e-12; here a Cholesky pivot <= 1e-12
+    bool ok = dw.info[0] == 0;
+    for (int k = 0; k < c.N && ok; ++k) {
+      const double l = dw.L[(long long)k * c.N + k];
+      ok = l * l > 1e-12;
+    }
+    st->status = ok ? kOk : kErrInvalidInput;
+    st->nocc = 0;
+    st->converged = 0;
+    st->iter = 0;
+    st->bro_iter = 0;
+    st->have_e = 0;
+    st->last_e = st->e_el = st->e2 = st->e3 = st->ts = st->mu = st->rms = 0.0;
+    st->nelec = nref - B.charge[m];
+    st->kt = fmax(opt.etemp, 0.0) * kBoltzmann;
+    if (!ok) {
+      B.status[m] = kErrInvalidInput;
+      B.iterations[m] = 0;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kDenseNT, 1) dense_potential_kernel(Batch B, Model M, int m, DenseWork dw) {
+  extern __shared__ __align__(16) unsigned char raw[];
+  const MolCtx c = dense_context(B, M, m, dw, raw);
+  CtaWs w = cta_ws(dw.ws, 1, dw.maxnsh, dw.cap);
+  stage_potential<kDenseNT>(B, M, c, w, dw.vao);
+}
+
+// Mm = diag(v) L (lower triangle of L, column-major)
+__global__ void dense_scale_rows_kernel(int N, const double* __restrict__ L, const double* __restrict__ v,
+                                        double* __restrict__ Mm) {
+  const long long n2 = (long long)N * N;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n2; idx += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(idx % N), j = (int)(idx / N);
+    Mm[idx] = i >= j ? v[i] * L[idx] : 0.0;
+  }
+}
+
+// F' = H0' - (Mm + Mm^T)/2 with Mm = L^-1 diag(v) L
+__global__ void dense_fock_kernel(int N, const double* __restrict__ Hp, const double* __restrict__ Mm,
+                                  double* __restrict__ F) {
+  const long long n2 = (long long)N * N;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n2; idx += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(idx % N), j = (int)(idx / N);
+    F[idx] = Hp[idx] - 0.5 * (Mm[idx] + Mm[(long long)i * N + j]);
+  }
+}
+
+__global__ void __launch_bounds__(kDenseNT, 1) dense_fermi_kernel(int N, DenseWork dw) {
+  __shared__ SccShared sh;
+  DenseState* st = (DenseState*)dw.state;
+  const double nelec = st->nelec, kt = st->kt;
+  const int tid = threadIdx.x;
+  if (kt > 0.0 && nelec > 0.0 && nelec < 2.0 * N) {
+    double fm, ft;
+    bool amb;
+    fermi_cta<kDenseNT>(dw.eps, N, N, nelec, kt, dw.occ, sh, fm, ft, amb);
+    if (tid == 0) {
+      sh.scal[1] = fm;
+      sh.scal[2] = ft;
+    }
+  } else if (tid < 32) {
+    double fm, ft;
+    bool amb;
+    fermi_warp(dw.eps, N, N, nelec, kt, dw.occ, fm, ft, amb);
+    if (tid == 0) {
+      sh.scal[1] = fm;
+      sh.scal[2] = ft;
+    }
+  }
+  __syncthreads();
+  int nocc_loc = 0;
+  for (int i = tid; i < N; i += kDenseNT)
+    if (dw.occ[i] > 1e-30) nocc_loc = max(nocc_loc, i + 1);
+  const int nocc = (int)block_max((double)nocc_loc, sh.red);
+  if (tid == 0) {
+    st->mu = sh.scal[1];
+    st->ts = sh.scal[2];
+    st->nocc = nocc;
+  }
+}
+
+// pop_mu = sum_i occ_i C_mu,i D_mu,i, C = L^-T Z, D = L Z (column-major, ld N)
+__global__ void dense_pop_kernel(int N, int nocc, const double* __restrict__ occ, const double* __restrict__ C,
+                                 const double* __restrict__ D, double* __restrict__ pop) {
+  const int mu = blockIdx.x * blockDim.x + threadIdx.x;
+  if (mu >= N) return;
+  double p = 0.0;
+  for (int i = 0; i < nocc; ++i) p += occ[i] * C[(long long)i * N + mu] * D[(long long)i * N + mu];
+  pop[mu] = p;
+}
+
+__global__ void __launch_bounds__(kDenseNT, 1) dense_energy_mix_kernel(Batch B, Model M, SccOptions opt, int m,
+                                                                       int iter, DenseWork dw) {
+  extern __shared__ __align__(16) unsigned char raw[];
+  __shared__ SccShared sh;
+  const MolCtx c = dense_context(B, M, m, dw, raw);
+  CtaWs w = cta_ws(dw.ws, 1, dw.maxnsh, dw.cap);
+  DenseState* st = (DenseState*)dw.state;
+  double e_el, e2, e3, rms;
+  stage_charges_energy<kDenseNT>(B, M, c, w, dw.pop, dw.occ, dw.eps, dw.vao, st->nocc, sh, e_el, e2, e3, rms);
+  const double escc = e_el + e2 + e3 + st->ts;
+  const double err = st->have_e ? fabs(escc - st->last_e) : INFINITY;
+  const bool converged = err < opt.energy_tol && rms < opt.charge_tol;
+  __syncthreads();
+  if (!converged) {
+    int bro = st->bro_iter;
+    stage_mix<kDenseNT>(opt, c, w, dw.cap, bro, sh);
+    if (threadIdx.x == 0) st->bro_iter = bro;
+  }
+  if (threadIdx.x == 0) {
+    st->e_el = e_el;
+    st->e2 = e2;
+    st->e3 = e3;
+    st->rms = rms;
+    st->iter = iter;
+    st->converged = converged ? 1 : 0;
+    if (!converged) {
+      st->last_e = escc;
+      st->have_e = 1;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kDenseNT, 1) dense_results_kernel(Batch B, Model M, int m, DenseWork dw) {
+  extern __shared__ __align__(16) unsigned char raw[];
+  const MolCtx c = dense_context(B, M, m, dw, raw);
+  CtaWs w = cta_ws(dw.ws, 1, dw.maxnsh, dw.cap);
+  const DenseState* st = (const DenseState*)dw.state;
+  stage_results<kDenseNT>(B, c, w, st->iter, st->converged != 0, st->e_el, st->e2, st->e3, st->ts, st->mu);
+}
+
+// out[:, i] = scale_i * in[:, i] with scale = occ (weight 0) or occ * eps (weight 1)
+__global__ void dense_scale_cols_kernel(int N, int nocc, const double* __restrict__ in, const double* __restrict__ occ,
+                                        const double* __restrict__ eps, int weight, double* __restrict__ out) {
+  const long long n2 = (long long)N * nocc;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n2; idx += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(idx / N);
+    out[idx] = in[idx] * (weight ? occ[i] * eps[i] : occ[i]);
+  }
+}
+
+long long dense_ws_doubles(int maxnsh, int cap, int maxnat) { return cta_ws_size(1, maxnsh, cap, maxnat); }
+size_t dense_smem_bytes(int maxnsh, int maxn, int maxnat) { return dense_table_bytes(maxnsh, maxn, maxnat); }
+size_t dense_state_bytes() { return sizeof(DenseState); }
+
+// Solver workspace (doubles) for N: max of potrf and syevd.
+long long dense_solver_lwork(void* solver, int N) {
+  cusolverDnHandle_t hs = (cusolverDnHandle_t)solver;
+  int l1 = 0, l2 = 0;
+  if (cusolverDnDpotrf_bufferSize(hs, CUBLAS_FILL_MODE_LOWER, N, nullptr, N, &l1) != CUSOLVER_STATUS_SUCCESS) return -1;
+  if (cusolverDnDsyevd_bufferSize(hs, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, N, nullptr, N, nullptr, &l2) !=
+      CUSOLVER_STATUS_SUCCESS)
+    return -1;
+  return (long long)(l1 > l2 ? l1 : l2);
+}
+
+// One large molecule, start to finish, on stream st.  Synchronises st once per
+// SCC iteration (the occupied count and the convergence flag).  Returns
+// cudaErrorUnknown when a library call fails.
+cudaError_t run_dense_molecule(const Batch& B, const Model& M, const SccOptions& opt, int m, int N, long long mo,
+                               DenseWork& dw, cudaStream_t st) {
+  cublasHandle_t hb = (cublasHandle_t)dw.blas;
+  cusolverDnHandle_t hs = (cusolverDnHandle_t)dw.solver;
+  if (cublasSetStream(hb, st) != CUBLAS_STATUS_SUCCESS || cusolverDnSetStream(hs, st) != CUSOLVER_STATUS_SUCCESS)
+    return cudaErrorUnknown;
+  const size_t n2b = sizeof(double) * (size_t)N * N;
+  const size_t smem = dense_table_bytes(dw.maxnsh, dw.maxn, dw.maxnat);
+  const int ew_blocks = 4 * 148, ew_threads = 256;
+  const double one = 1.0, zero = 0.0;
+  cudaError_t e;
+  static int configured_dev = -1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (configured_dev != dev) {
+    for (const void* k : {(const void*)dense_init_kernel, (const void*)dense_potential_kernel,
+                          (const void*)dense_energy_mix_kernel, (const void*)dense_results_kernel})
+      if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024)) != cudaSuccess)
+        return e;
+    configured_dev = dev;
+  }
+  if (smem > 200 * 1024) return cudaErrorInvalidValue;
+  // orthogonaliser: S = L L^T, H0' = L^-1 H0 L^-T
+  if ((e = cudaMemcpyAsync(dw.L, B.S + mo, n2b, cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(dw.Hp, B.H0 + mo, n2b, cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e;
+  if (cusolverDnDpotrf(hs, CUBLAS_FILL_MODE_LOWER, N, dw.L, N, dw.solver_work, (int)dw.lwork, dw.info) !=
+      CUSOLVER_STATUS_SUCCESS)
+    return cudaErrorUnknown;
+  if (cublasDtrsm(hb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, N, N, &one, dw.L, N,
+                  dw.Hp, N) != CUBLAS_STATUS_SUCCESS ||
+      cublasDtrsm(hb, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, N, N, &one, dw.L,
+                  N, dw.Hp, N) != CUBLAS_STATUS_SUCCESS)
+    return cudaErrorUnknown;
+  // status, nocc, converged: the first three ints of DenseState, read back at each sync point
+  auto read_flags = [&]() -> cudaError_t {
+    cudaError_t r = cudaGetLastError();
+    if (r == cudaSuccess) r = cudaMemcpyAsync(dw.h_state, dw.state, 3 * sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (r == cudaSuccess) r = cudaStreamSynchronize(st);
+    return r;
+  };
+  dense_init_kernel<<<1, kDenseNT, smem, st>>>(B, M, opt, m, dw);
+  if ((e = read_flags()) != cudaSuccess) return e;
+  if (dw.h_state[0] != kOk) return cudaSuccess;  // status already written
+  int iter = 1;
+  for (; iter <= opt.max_scc; ++iter) {
+    dense_potential_kernel<<<1, kDenseNT, smem, st>>>(B, M, m, dw);
+    dense_scale_rows_kernel<<<ew_blocks, ew_threads, 0, st>>>(N, dw.L, dw.vao, dw.Mm);
+    if (cublasDtrsm(hb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, N, N, &one, dw.L,
+                    N, dw.Mm, N) != CUBLAS_STATUS_SUCCESS)
+      return cudaErrorUnknown;
+    dense_fock_kernel<<<ew_blocks, ew_threads, 0, st>>>(N, dw.Hp, dw.Mm, dw.F);
+    if (cusolverDnDsyevd(hs, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, N, dw.F, N, dw.eps, dw.solver_work,
+                         (int)dw.lwork, dw.info) != CUSOLVER_STATUS_SUCCESS)
+      return cudaErrorUnknown;
+    dense_fermi_kernel<<<1, kDenseNT, 0, st>>>(N, dw);
+    if ((e = read_flags()) != cudaSuccess) return e;
+    const int nocc = dw.h_state[1];
+    if (nocc > 0) {
+      if ((e = cudaMemcpyAsync(dw.C, dw.F, sizeof(double) * (size_t)N * nocc, cudaMemcpyDeviceToDevice, st)) !=
+          cudaSuccess)
+        return e;
+      if (cublasDtrsm(hb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, N, nocc, &one,
+                      dw.L, N, dw.C, N) != CUBLAS_STATUS_SUCCESS ||
+          cublasDtrmm(hb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, N, nocc, &one,
+                      dw.L, N, dw.F, N, dw.D, N) != CUBLAS_STATUS_SUCCESS)
+        return cudaErrorUnknown;
+    }
+    dense_pop_kernel<<<(N + 255) / 256, 256, 0, st>>>(N, nocc, dw.occ, dw.C, dw.D, dw.pop);
+    dense_energy_mix_kernel<<<1, kDenseNT, smem, st>>>(B, M, opt, m, iter, dw);
+    if ((e = read_flags()) != cudaSuccess) return e;
+    if (dw.h_state[2]) break;
+  }
+  dense_results_kernel<<<1, kDenseNT, smem, st>>>(B, M, m, dw);
+  // P = C diag(f) C^T and W = C diag(f eps) C^T of the last diagonalisation
+  const int nocc = dw.h_state[1];
+  if (nocc > 0) {
+    dense_scale_cols_kernel<<<ew_blocks, ew_threads, 0, st>>>(N, nocc, dw.C, dw.occ, dw.eps, 0, dw.D);
+    if (cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, N, N, nocc, &one, dw.D, N, dw.C, N, &zero, B.P + mo, N) !=
+        CUBLAS_STATUS_SUCCESS)
+      return cudaErrorUnknown;
+    dense_scale_cols_kernel<<<ew_blocks, ew_threads, 0, st>>>(N, nocc, dw.C, dw.occ, dw.eps, 1, dw.D);
+    if (cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, N, N, nocc, &one, dw.D, N, dw.C, N, &zero, B.W + mo, N) !=
+        CUBLAS_STATUS_SUCCESS)
+      return cudaErrorUnknown;
+  } else {
+    if ((e = cudaMemsetAsync(B.P + mo, 0, n2b, st)) != cudaSuccess || (e = cudaMemsetAsync(B.W + mo, 0, n2b, st)) != cudaSuccess)
+      return e;
+  }
+  return cudaGetLastError();
 }
 
 long long scc_workspace_doubles(int maxn, int maxnsh, int cap, int maxnat) {

@@ -1,0 +1,95 @@
+"""The large-molecule path (cuSOLVER eigensolver, cuBLAS triangular products,
+the same SCC stage functions) against the one-CTA-per-molecule path and the
+oracle.
+
+Tolerances: between the two device paths |dE| <= 1e-9 Eh, |dg| <= 1e-8 Eh/bohr,
+|dq| <= 1e-8 e at tight convergence; against the oracle the parity bar
+(1e-6 Eh, 1e-5 Eh/bohr, 1e-5 e)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+A2B = 1.8897261246257702
+TIGHT = dict(energy_tolerance=1e-10, charge_tolerance=1e-8)
+LARGE = os.path.join(os.path.dirname(__file__), "golden", "large_systems.json")
+
+
+def _run(off, z, x, dense_n=None, **opts):
+    from gfn1_rs import BatchCalculator
+    old = os.environ.get("GFN1_DENSE_N")
+    if dense_n is not None:
+        os.environ["GFN1_DENSE_N"] = str(dense_n)
+    try:
+        calc = BatchCalculator(**opts)
+        return calc.calculate_flat(off, z, x)
+    finally:
+        if old is None:
+            os.environ.pop("GFN1_DENSE_N", None)
+        else:
+            os.environ["GFN1_DENSE_N"] = old
+
+
+def test_dense_path_matches_cta_path(gpu_calc):
+    from gfn1_rs import workloads
+    zs, xs, off = [], [], [0]
+    for seed in (3, 11, 42):
+        z, x = workloads.water_cluster(16 + seed % 5, seed)
+        zs.append(z), xs.append(x * A2B), off.append(off[-1] + len(z))
+    z2, x2 = workloads.mixed_molecule(1007)
+    zs.append(z2), xs.append(x2 * A2B), off.append(off[-1] + len(z2))
+    off = np.asarray(off, np.int32)
+    z = np.concatenate(zs)
+    x = np.concatenate(xs)
+    ref = _run(off, z, x, **TIGHT)
+    got = _run(off, z, x, dense_n=64, **TIGHT)
+    assert np.all(ref.status == 0) and np.all(got.status == 0)
+    assert np.abs(got.energy - ref.energy).max() <= 1e-9
+    assert np.abs(got.gradient - ref.gradient).max() <= 1e-8
+    assert np.abs(got.shell_charges - ref.shell_charges).max() <= 1e-8
+    assert np.array_equal(got.iterations, ref.iterations)
+    for k in (0, 1, 3, 4, 5, 14):
+        assert np.abs(got.terms[:, k] - ref.terms[:, k]).max() <= 1e-9
+
+
+def test_dense_path_zero_and_learned_guess_agree(gpu_calc):
+    from gfn1_rs import BatchCalculator, workloads
+    z, x = workloads.water_cluster(20, 7)
+    off = np.array([0, len(z)], np.int32)
+    old = os.environ.get("GFN1_DENSE_N")
+    os.environ["GFN1_DENSE_N"] = "64"
+    try:
+        plain = BatchCalculator(**TIGHT).calculate_flat(off, z, x * A2B)
+        learned = BatchCalculator(learned_guess=True, **TIGHT).calculate_flat(off, z, x * A2B)
+    finally:
+        if old is None:
+            os.environ.pop("GFN1_DENSE_N", None)
+        else:
+            os.environ["GFN1_DENSE_N"] = old
+    assert abs(plain.energy[0] - learned.energy[0]) <= 1e-8
+    assert learned.iterations[0] <= plain.iterations[0]
+
+
+@pytest.mark.skipif(not os.path.exists(LARGE), reason="large-system oracle fixtures not generated")
+def test_large_systems_match_oracle(gpu_calc):
+    from gfn1_rs import BatchCalculator
+    fx = json.load(open(LARGE))
+    opts = fx["options"]
+    calc = BatchCalculator(**opts)
+    cases = list(fx.get("water96_traj", []))
+    if "water300" in fx:
+        cases.append(fx["water300"])
+    assert cases
+    for rec in cases:
+        z = np.array(rec["numbers"])
+        x = np.array(rec["positions_angstrom"]) * A2B
+        r = calc.calculate_flat([0, len(z)], z, x)
+        assert r.status[0] == 0
+        de = abs(r.energy[0] - rec["energy"])
+        dg = np.abs(r.gradient - np.array(rec["gradient"])).max()
+        dq = np.abs(r.shell_charges - np.array(rec["shell_charges"])).max()
+        print(f"{len(z)} atoms: dE {de:.2e} dg {dg:.2e} dq {dq:.2e} iterations {r.iterations[0]} vs {rec['iterations']}")
+        assert de <= 1e-6 and dg <= 1e-5 and dq <= 1e-5
