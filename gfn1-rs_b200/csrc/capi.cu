@@ -260,7 +260,7 @@ struct gfn1_batch {
   int nmol = 0;
   long long natoms = 0, nshells = 0, naos = 0, mat_total = 0, gam_total = 0, pair_total = 0;
   int max_nat = 0, max_nsh = 0, max_n = 0, cap = 0;
-  // SCC size classes: [0] large molecules (512 threads, 1 CTA/SM), [1] the rest
+  // SCC size classes: [0] molecules above the split size, [1] the rest
   struct SccClass {
     int q_begin = 0, q_end = 0, n_cta = 0, nt = 256, maxn = 0, maxnsh = 0, maxnat = 0;
     long long ws_offset = 0, ws_stride = 0;
@@ -700,9 +700,15 @@ int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t*
   for (int m = 0; m < nmol; ++m) h_order[m] = m;
   std::stable_sort(h_order, h_order + nmol, [&](int x, int y) { return n_m[x] > n_m[y]; });
   b->cap = std::max(1, std::min(std::max(o.scc_broyden_size, 2), o.max_scc));
-  // size classes over the sorted order: N > kLargeN runs 512-thread CTAs, one
-  // per SM, with up to 227 KB of shared memory; the rest 256-thread CTAs, two per SM
-  const int kLargeN = 96;
+  // two size classes over the sorted order (class 0: N > kSplitN), each with its
+  // CTA size; 512 / nt CTAs share an SM, so several molecules interleave on it.
+  // Measured on the 4096-molecule batch (SCC stage, zero guess): one 512-thread
+  // CTA per SM above 96 AOs 141 ms, 256 threads 126 ms, 128 threads 113 ms,
+  // 64 threads 139 ms: four molecules per SM hide each other's barrier and
+  // latency stalls, while smaller CTAs lose too much per-molecule parallelism.
+  // A class whose vectors do not fit the per-CTA shared memory gets larger CTAs.
+  const int kSplitN = 96;
+  const int kClassNt[2] = {128, 128};
   // above kDenseN AOs one SM per molecule is too slow: library-backed path.
   // GFN1_DENSE_N overrides the threshold (used by the tests to run both paths
   // on the same molecules).
@@ -726,13 +732,13 @@ int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t*
     dmaxnat = std::max(dmaxnat, atom_offsets[mm + 1] - atom_offsets[mm]);
   }
   int n_large = n_dense;
-  while (n_large < nmol && n_m[h_order[n_large]] > kLargeN) ++n_large;
+  while (n_large < nmol && n_m[h_order[n_large]] > kSplitN) ++n_large;
   long long ws_total = 0;
   for (int c = 0; c < 2; ++c) {
     gfn1_batch::SccClass& K = b->cls[c];
     K.q_begin = c == 0 ? n_dense : n_large;
     K.q_end = c == 0 ? n_large : nmol;
-    K.nt = c == 0 ? 512 : 256;
+    K.nt = kClassNt[c];
     K.maxn = K.maxnsh = K.maxnat = 0;
     for (int q = K.q_begin; q < K.q_end; ++q) {
       const int mm = h_order[q];
@@ -741,13 +747,14 @@ int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t*
       K.maxnat = std::max(K.maxnat, atom_offsets[mm + 1] - atom_offsets[mm]);
     }
     const int count = K.q_end - K.q_begin;
-    K.n_cta = count == 0 ? 0 : std::max(1, std::min(count, (c == 0 ? 1 : 2) * eng->num_sms));
+    const size_t fixed = scc_smem_bytes(K.maxnsh, K.maxn, K.maxnat, 0);
+    while (K.nt < 512 && fixed > scc_max_dynamic_smem(K.nt)) K.nt *= 2;  // vectors of big molecules need room
+    K.n_cta = count == 0 ? 0 : std::max(1, std::min(count, (512 / K.nt) * eng->num_sms));
     K.ws_stride = count == 0 ? 0 : scc_workspace_doubles(std::max(K.maxn, 1), std::max(K.maxnsh, 1), b->cap,
                                                            std::max(K.maxnat, 1));
     K.ws_offset = ws_total;
     ws_total += K.ws_stride * K.n_cta;
     const size_t full = scc_smem_bytes(K.maxnsh, K.maxn, K.maxnat, K.maxn);
-    const size_t fixed = scc_smem_bytes(K.maxnsh, K.maxn, K.maxnat, 0);
     const size_t limit = scc_max_dynamic_smem(K.nt);
     K.smem = std::max(fixed, std::min(full, limit));
   }

@@ -1425,7 +1425,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
 }
 
 template <int NT>
-__global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) scc_kernel(Batch B, Model M, SccOptions opt, SccLaunch SL) {
+__global__ void __launch_bounds__(NT, 512 / NT) scc_kernel(Batch B, Model M, SccOptions opt, SccLaunch SL) {
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ SccShared sh;
   __shared__ int next;
@@ -1765,33 +1765,36 @@ size_t scc_smem_bytes(int maxnsh, int maxn, int maxnat, int matrix_n) {
   return matrix_n > 0 ? fixed + sizeof(double) * (size_t)matrix_n * work_lda(matrix_n) : fixed;
 }
 
-// Largest dynamic shared memory a CTA of the class may request: the 227 KB per
-// CTA limit less the kernel's static shared memory (two CTAs per SM for nt = 256
-// share the SM's 228 KB, 1 KB of which each CTA reserves).
+// Largest dynamic shared memory a CTA of the class may request: the SM's
+// 228 KB shared by its 512 / nt CTAs (1 KB of which each CTA reserves), less
+// the kernel's static shared memory.
 size_t scc_max_dynamic_smem(int nt) {
   cudaFuncAttributes a;
-  const cudaError_t e = nt == 512 ? cudaFuncGetAttributes(&a, scc_kernel<512>) : cudaFuncGetAttributes(&a, scc_kernel<256>);
+  const cudaError_t e = nt == 512   ? cudaFuncGetAttributes(&a, scc_kernel<512>)
+                        : nt == 256 ? cudaFuncGetAttributes(&a, scc_kernel<256>)
+                                    : cudaFuncGetAttributes(&a, scc_kernel<128>);
   const size_t stat = e == cudaSuccess ? a.sharedSizeBytes : 8192;
-  const size_t per_cta = nt == 512 ? 232448 : (233472 / 2 - 1024);
+  const size_t per_cta = 233472 / (512 / nt) - 1024;  // the SM's 228 KB shared by 512/nt CTAs
   return per_cta - stat - 256;
 }
 
-// Host launcher of one size class (nt = 512 or 256 threads per CTA).
+template <int NT>
+static cudaError_t launch_scc_nt(int grid, size_t smem, cudaStream_t st, const Batch& B, const Model& M,
+                                 const SccOptions& opt, const SccLaunch& SL) {
+  cudaError_t e = cudaFuncSetAttribute(scc_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  scc_kernel<NT><<<grid, NT, smem, st>>>(B, M, opt, SL);
+  return cudaGetLastError();
+}
+
+// Host launcher of one size class (nt = 512, 256 or 128 threads per CTA;
+// 512 / nt CTAs share an SM).
 cudaError_t launch_scc(int nt, int grid, size_t smem, cudaStream_t st, const Batch& B, const Model& M,
                        const SccOptions& opt, const SccLaunch& SL) {
-  cudaError_t e;
-  if (nt == 512) {
-    if ((e = cudaFuncSetAttribute(scc_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
-        cudaSuccess)
-      return e;
-    scc_kernel<512><<<grid, 512, smem, st>>>(B, M, opt, SL);
-  } else {
-    if ((e = cudaFuncSetAttribute(scc_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
-        cudaSuccess)
-      return e;
-    scc_kernel<256><<<grid, 256, smem, st>>>(B, M, opt, SL);
-  }
-  return cudaGetLastError();
+  if (nt == 512) return launch_scc_nt<512>(grid, smem, st, B, M, opt, SL);
+  if (nt == 256) return launch_scc_nt<256>(grid, smem, st, B, M, opt, SL);
+  if (nt == 128) return launch_scc_nt<128>(grid, smem, st, B, M, opt, SL);
+  return cudaErrorInvalidValue;
 }
 
 }  // namespace gfn1
