@@ -905,7 +905,7 @@ int launch_stage(gfn1_batch* b, int stage, cudaStream_t st) {
     if (!b->opt.compute_gradient) return GFN1_OK;
     const size_t smem = sizeof(double) * 7 * (size_t)b->max_nat + sizeof(int) * (3 * (size_t)b->max_nat + 2);
     if (smem > 48 * 1024) cudaFuncSetAttribute(grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    grad_kernel<<<b->nmol, nt, smem, st>>>(B, M);
+    grad_kernel<<<b->nmol, kGradThreads, smem, st>>>(B, M);
   } else {
     return fail(eng, GFN1_E_INVALID_INPUT, "unknown stage");
   }
@@ -1485,7 +1485,7 @@ extern "C" int gfn1_run_noalloc(gfn1_engine* eng, int nat, const uint8_t* z, con
   SL.smem_bytes = (int)sm_scc;
   if ((e = launch_scc(n > 96 ? 512 : 256, 1, sm_scc, st, B, M, so, SL)) != cudaSuccess)
     return cuda_fail(eng, e, "scc launch");
-  if (o.compute_gradient) grad_kernel<<<1, 256, sm_grad, st>>>(B, M);
+  if (o.compute_gradient) grad_kernel<<<1, kGradThreads, sm_grad, st>>>(B, M);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(eng, e, "kernel launch");
   if ((e = cudaMemcpyAsync(hout, base + o_terms, out_end - o_terms, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
     return cuda_fail(eng, e, "device to host copy");

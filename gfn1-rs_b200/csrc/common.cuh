@@ -31,6 +31,10 @@ constexpr int kMaxShAtom = 3;  // shells per atom on the device path
 constexpr int kMaxPrim = 8;    // H 2s after orthogonalisation to 1s has 7
 constexpr int kMaxRef = 5;     // D3 references per element for Z <= 86
 constexpr int kTerms = 15;     // EnergyTerms::named_values (src/electronic.rs:681-699)
+// Gradient kernel: threads per CTA (one CTA per molecule) and the CTAs per SM
+// its register budget is sized for.
+constexpr int kGradThreads = 128;
+constexpr int kGradMinBlocks = 4;
 
 // Per-element data, indexed by Z.  nsh == 0 marks an element the device path
 // does not support (d/f shells).  Values are already converted to the model

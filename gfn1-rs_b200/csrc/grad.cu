@@ -21,7 +21,36 @@
 
 namespace gfn1 {
 
-__global__ void __launch_bounds__(256) grad_kernel(Batch B, Model M) {
+// Overlap-derivative contraction of one shell pair (mu shell of angular
+// momentum LB on atom b, nu shell LA on atom a), src/gradient.rs:358-455:
+// gmu += dS/dR_b [P (2 h - v_mu - v_nu) - 2 W] + R 2 P h S dlnPi/dR, plus the
+// dE/dCN accumulation of both atoms.  xs = {h, v_mu + v_nu, dlnPi/dR factor,
+// -kcn_mu hscale Pi, -kcn_nu hscale Pi}.
+template <int LB, int LA>
+__device__ __forceinline__ void grad_shell_pair(const ElemTable& eb, int kb, const double* xb, const ElemTable& ea,
+                                                int ka, const double* xa, const double* P, const double* W, int N,
+                                                int mu0, int nu0, const double (&xs)[5], const double (&rv)[3],
+                                                double (&gmu)[3], double& dcmu, double& dcnu) {
+  double Sb[2 * LB + 1][2 * LA + 1], dA[2 * LB + 1][2 * LA + 1][3];
+  overlap_block_t<LB, LA, true>(eb.nprim[kb], eb.alpha[kb], eb.coef[kb], xb, ea.nprim[ka], ea.alpha[ka], ea.coef[ka],
+                                xa, 3, Sb, dA);
+  const double hij = xs[0], vsum = xs[1], dlog = xs[2];
+#pragma unroll
+  for (int x = 0; x < 2 * LB + 1; ++x)
+#pragma unroll
+    for (int y = 0; y < 2 * LA + 1; ++y) {
+      const long long idx = (long long)(mu0 + x) * N + (nu0 + y);
+      const double pp = P[idx], ww = W[idx];
+      const double coeff = pp * (2.0 * hij - vsum) - 2.0 * ww;
+      const double pg = dlog * (2.0 * pp * hij * Sb[x][y]);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) gmu[c] += dA[x][y][c] * coeff + rv[c] * pg;
+      dcmu += xs[3] * pp * Sb[x][y];
+      dcnu += xs[4] * pp * Sb[x][y];
+    }
+}
+
+__global__ void __launch_bounds__(kGradThreads, kGradMinBlocks) grad_kernel(Batch B, Model M) {
   extern __shared__ double gsm[];
   const int m = blockIdx.x;
   if (B.status[m] != kOk) return;
@@ -73,7 +102,7 @@ __global__ void __launch_bounds__(256) grad_kernel(Batch B, Model M) {
     const ElemTable& eb = M.elem[zb];
     const double rv[3] = {xyz[3 * b] - xyz[3 * a], xyz[3 * b + 1] - xyz[3 * a + 1], xyz[3 * b + 2] - xyz[3 * a + 2]};
     const double r2 = rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2];
-    double gmu[3] = {0, 0, 0}, gnu[3] = {0, 0, 0};  // mu on atom b, nu on atom a
+    double gmu[3] = {0, 0, 0};  // derivative with respect to atom b (mu on b, nu on a)
     double dcmu = 0.0, dcnu = 0.0;
     if (r2 <= 900.0 && r2 > 1e-24 && r2 > 1e-12) {
       const double r = sqrt(r2);
@@ -92,24 +121,14 @@ __global__ void __launch_bounds__(256) grad_kernel(Batch B, Model M) {
           const double hij = 0.5 * (semu + senu) * hs;
           double dlog = 0.0;  // src/gradient.rs:1157-1175 (scalar factor of rvec)
           if (fabs(poly) > 1e-18) dlog = (fi * ea.poly[ka] + fj * eb.poly[kb]) * 0.5 * rr / r2 / poly;
-          double Sb[3][3], dA[3][3][3], dB[3][3][3];
-          overlap_block<true>(eb.l[kb], eb.nprim[kb], eb.alpha[kb], eb.coef[kb], &xyz[3 * b], ea.l[ka], ea.nprim[ka],
-                              ea.alpha[ka], ea.coef[ka], &xyz[3 * a], 3, Sb, dA, dB);
           const int mu0 = atom_ao[b] + eb.ao_first[kb], nu0 = atom_ao[a] + ea.ao_first[ka];
-          const int nmu = 2 * eb.l[kb] + 1, nnu = 2 * ea.l[ka] + 1;
-          for (int x = 0; x < nmu; ++x)
-            for (int y = 0; y < nnu; ++y) {
-              const long long idx = (long long)(mu0 + x) * N + (nu0 + y);
-              const double pp = P[idx], ww = W[idx];
-              const double coeff = pp * (2.0 * hij - (vmu + vnu)) - 2.0 * ww;
-              const double pg = dlog * (2.0 * pp * hij * Sb[x][y]);
-              for (int c = 0; c < 3; ++c) {
-                gmu[c] += dA[x][y][c] * coeff + rv[c] * pg;
-                gnu[c] += dB[x][y][c] * coeff - rv[c] * pg;
-              }
-              dcmu += -eb.kcn[kb] * hs * pp * Sb[x][y];
-              dcnu += -ea.kcn[ka] * hs * pp * Sb[x][y];
-            }
+          const double xs[5] = {hij, vmu + vnu, dlog, -eb.kcn[kb] * hs, -ea.kcn[ka] * hs};
+          switch (eb.l[kb] * 2 + ea.l[ka]) {  // s/p shells only on the device path
+            case 0: grad_shell_pair<0, 0>(eb, kb, &xyz[3 * b], ea, ka, &xyz[3 * a], P, W, N, mu0, nu0, xs, rv, gmu, dcmu, dcnu); break;
+            case 1: grad_shell_pair<0, 1>(eb, kb, &xyz[3 * b], ea, ka, &xyz[3 * a], P, W, N, mu0, nu0, xs, rv, gmu, dcmu, dcnu); break;
+            case 2: grad_shell_pair<1, 0>(eb, kb, &xyz[3 * b], ea, ka, &xyz[3 * a], P, W, N, mu0, nu0, xs, rv, gmu, dcmu, dcnu); break;
+            default: grad_shell_pair<1, 1>(eb, kb, &xyz[3 * b], ea, ka, &xyz[3 * a], P, W, N, mu0, nu0, xs, rv, gmu, dcmu, dcnu); break;
+          }
         }
       }
     }
@@ -123,18 +142,15 @@ __global__ void __launch_bounds__(256) grad_kernel(Batch B, Model M) {
             const double g = harmonic_avg(eb.hard[kb], ea.hard[ka]);
             const double den = r2 + 1.0 / (g * g);
             const double pref = -1.0 / (den * sqrt(den)) * qi * qj;
-            for (int c = 0; c < 3; ++c) {
-              gmu[c] += rv[c] * pref;
-              gnu[c] -= rv[c] * pref;
-            }
+            for (int c = 0; c < 3; ++c) gmu[c] += rv[c] * pref;
           }
         }
       }
     }
-    double* slot = pb + 8LL * p;
-    slot[0] = gnu[0];
-    slot[1] = gnu[1];
-    slot[2] = gnu[2];
+    double* slot = pb + 8LL * p;  // every term is a function of R_b - R_a: the atom a force is -gmu
+    slot[0] = -gmu[0];
+    slot[1] = -gmu[1];
+    slot[2] = -gmu[2];
     slot[3] = gmu[0];
     slot[4] = gmu[1];
     slot[5] = gmu[2];

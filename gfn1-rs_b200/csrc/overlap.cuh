@@ -47,8 +47,17 @@ __device__ __forceinline__ double ipow(double x, int n) {
 // Overlap block S[ka][kb] between shell (la, prims a) at A and shell (lb, prims b)
 // at B; nao = 2l+1 for l <= 1.  `order_extra` is the screening order offset
 // (+2 for the integral build, +3 for the gradient, src/integrals.rs:313-316, :498-501).
-// When `want_deriv`, dA[ka][kb][3] receives dS/dA (bra centre) and dB the ket
-// centre derivative.
+// When `want_deriv`, dA[ka][kb][3] receives dS/dA (bra centre); dB, when not
+// null, the ket-centre derivative (equal to -dA for a two-centre overlap).
+//
+// Screening: the reference evaluates bound = |c_a c_b| kab (pi/p)^3/2
+// (1 + r + p^-1/2)^order with kab = exp(-x), x = ab r^2 / p, and drops the pair
+// when bound < 1e-13.  For x > 64 the exp-free part is checked first: if it is
+// below 1e-13 e^64 the full bound is below 1e-13 too, so the same pairs are
+// dropped without evaluating the exponential.
+constexpr double kSkipExpArg = 64.0;
+constexpr double kSkipPrefBound = 6.235149080811617e14;  // 1e-13 * e^64
+
 template <bool WantDeriv>
 __device__ void overlap_block(int la, int na, const double* alpha_a, const double* coef_a, const double* A, int lb,
                               int nb, const double* alpha_b, const double* coef_b, const double* B, int order_extra,
@@ -58,7 +67,10 @@ __device__ void overlap_block(int la, int na, const double* alpha_a, const doubl
     for (int j = 0; j < 3; ++j) {
       S[i][j] = 0.0;
       if (WantDeriv)
-        for (int k = 0; k < 3; ++k) dA[i][j][k] = dB[i][j][k] = 0.0;
+        for (int k = 0; k < 3; ++k) {
+          dA[i][j][k] = 0.0;
+          if (dB) dB[i][j][k] = 0.0;
+        }
     }
   const double d[3] = {A[0] - B[0], A[1] - B[1], A[2] - B[2]};
   const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
@@ -70,12 +82,14 @@ __device__ void overlap_block(int la, int na, const double* alpha_a, const doubl
       const double be = alpha_b[ib];
       const double p = al + be;
       const double ip = 1.0 / p;
-      const double kab = exp(-al * be * ip * r2);
+      const double xarg = al * be * ip * r2;
       const double gpre = (kPi * ip) * sqrt(kPi * ip);
       const double pref = coef_a[ia] * coef_b[ib];
       // src/integrals.rs:30-45 (component scale is 1 for s and p AOs)
-      const double bound = fabs(pref) * kab * gpre * ipow(1.0 + r + sqrt(ip), order);
-      if (bound < kPrimScreen) continue;
+      const double pbound = fabs(pref) * gpre * ipow(1.0 + r + sqrt(ip), order);
+      if (xarg > kSkipExpArg && pbound < kSkipPrefBound) continue;
+      const double kab = exp(-xarg);
+      if (pbound * kab < kPrimScreen) continue;
       const double c = pref * kab * gpre;
       const double inv2p = 0.5 * ip;
       double E[3][3][3];
@@ -98,9 +112,76 @@ __device__ void overlap_block(int la, int na, const double* alpha_a, const doubl
             for (int x = 0; x < 3; ++x) {
               const double o = e1[(x + 1) % 3] * e1[(x + 2) % 3];
               const double da = 2.0 * al * E[x][a[x] + 1][b[x]] - (a[x] ? E[x][a[x] - 1][b[x]] : 0.0);
-              const double db = 2.0 * be * E[x][a[x]][b[x] + 1] - (b[x] ? E[x][a[x]][b[x] - 1] : 0.0);
               dA[ka][kb][x] += c * da * o;
-              dB[ka][kb][x] += c * db * o;
+              if (dB) {
+                const double db = 2.0 * be * E[x][a[x]][b[x] + 1] - (b[x] ? E[x][a[x]][b[x] - 1] : 0.0);
+                dB[ka][kb][x] += c * db * o;
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
+// The same block with the angular momenta known at compile time (LA, LB in
+// {0, 1}): every loop is unrolled and the block lives in registers.
+template <int LA, int LB, bool WantDeriv>
+__device__ __forceinline__ void overlap_block_t(int na, const double* alpha_a, const double* coef_a, const double* A,
+                                                int nb, const double* alpha_b, const double* coef_b, const double* B,
+                                                int order_extra, double (&S)[2 * LA + 1][2 * LB + 1],
+                                                double (&dA)[2 * LA + 1][2 * LB + 1][3]) {
+  constexpr int NA = 2 * LA + 1, NB = 2 * LB + 1;
+#pragma unroll
+  for (int i = 0; i < NA; ++i)
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+      S[i][j] = 0.0;
+      if (WantDeriv)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) dA[i][j][k] = 0.0;
+    }
+  const double d[3] = {A[0] - B[0], A[1] - B[1], A[2] - B[2]};
+  const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+  const double r = sqrt(r2);
+  const int order = LA + LB + order_extra;
+  for (int ia = 0; ia < na; ++ia) {
+    const double al = alpha_a[ia];
+    for (int ib = 0; ib < nb; ++ib) {
+      const double be = alpha_b[ib];
+      const double p = al + be;
+      const double ip = 1.0 / p;
+      const double xarg = al * be * ip * r2;
+      const double gpre = (kPi * ip) * sqrt(kPi * ip);
+      const double pref = coef_a[ia] * coef_b[ib];
+      const double pbound = fabs(pref) * gpre * ipow(1.0 + r + sqrt(ip), order);
+      if (xarg > kSkipExpArg && pbound < kSkipPrefBound) continue;
+      const double kab = exp(-xarg);
+      if (pbound * kab < kPrimScreen) continue;
+      const double c = pref * kab * gpre;
+      const double inv2p = 0.5 * ip;
+      double E[3][3][3];
+#pragma unroll
+      for (int x = 0; x < 3; ++x) {
+        const double P = (al * A[x] + be * B[x]) * ip;
+        moments1d(P - A[x], P - B[x], inv2p, E[x]);
+      }
+#pragma unroll
+      for (int ka = 0; ka < NA; ++ka) {
+        const int a[3] = {LA == 1 && ka == 0, LA == 1 && ka == 1, LA == 1 && ka == 2};
+#pragma unroll
+        for (int kb = 0; kb < NB; ++kb) {
+          const int b[3] = {LB == 1 && kb == 0, LB == 1 && kb == 1, LB == 1 && kb == 2};
+          const double ex = E[0][a[0]][b[0]], ey = E[1][a[1]][b[1]], ez = E[2][a[2]][b[2]];
+          S[ka][kb] += c * ex * ey * ez;
+          if (WantDeriv) {
+            const double e1[3] = {ex, ey, ez};
+#pragma unroll
+            for (int x = 0; x < 3; ++x) {
+              const double o = e1[(x + 1) % 3] * e1[(x + 2) % 3];
+              const double da = 2.0 * al * E[x][a[x] + 1][b[x]] - (a[x] ? E[x][a[x] - 1][b[x]] : 0.0);
+              dA[ka][kb][x] += c * da * o;
             }
           }
         }

@@ -29,6 +29,31 @@ __device__ __forceinline__ void tri_inverse(long long w, int& i, int& j) {
   j = (int)(w - ii * (ii + 1) / 2);
 }
 
+// S and H0 entries of one shell pair (both triangles); LA, LB are the shells'
+// angular momenta, so the overlap block stays in registers.
+template <int LA, int LB>
+__device__ __forceinline__ void shell_pair_sh0(const ElemTable& ea, int ka, const double* xa, const ElemTable& eb, int kb,
+                                               const double* xb, bool zero, double hij, double* S, double* H0, int N,
+                                               int mu0, int nu0) {
+  double Sb[2 * LA + 1][2 * LB + 1];
+  double dummy[2 * LA + 1][2 * LB + 1][3];
+  if (!zero)
+    overlap_block_t<LA, LB, false>(ea.nprim[ka], ea.alpha[ka], ea.coef[ka], xa, eb.nprim[kb], eb.alpha[kb], eb.coef[kb],
+                                   xb, 2, Sb, dummy);
+#pragma unroll
+  for (int x = 0; x < 2 * LA + 1; ++x)
+#pragma unroll
+    for (int y = 0; y < 2 * LB + 1; ++y) {
+      const double sv = zero ? 0.0 : Sb[x][y];
+      const long long i1 = (long long)(mu0 + x) * N + (nu0 + y);
+      const long long i2 = (long long)(nu0 + y) * N + (mu0 + x);
+      S[i1] = sv;
+      S[i2] = sv;
+      H0[i1] = sv * hij;
+      H0[i2] = sv * hij;
+    }
+}
+
 __global__ void __launch_bounds__(256) setup_kernel(Batch B, Model M, int enable_dispersion, int max_nsh) {
   extern __shared__ double smem[];
   const int m = blockIdx.x;
@@ -115,39 +140,28 @@ __global__ void __launch_bounds__(256) setup_kernel(Batch B, Model M, int enable
     const ElemTable& eb = M.elem[zb];
     const int la = ea.l[ka], lb = eb.l[kb];
     const int mu0 = atom_ao[a] + ea.ao_first[ka], nu0 = atom_ao[b] + eb.ao_first[kb];
-    const int na = 2 * la + 1, nb = 2 * lb + 1;
     const double sei = B.se[sh0 + si], sej = B.se[sh0 + sj];
-    double Sb[3][3];
-    double hij;
+    double hij = 0.0;
     bool zero = false;
     if (a == b) {
-      overlap_block<false>(la, ea.nprim[ka], ea.alpha[ka], ea.coef[ka], &xyz[3 * a], lb, eb.nprim[kb], eb.alpha[kb],
-                           eb.coef[kb], &xyz[3 * b], 2, Sb, nullptr, nullptr);
       hij = 0.5 * (sei + sej);
     } else {
       const double dx = xyz[3 * a] - xyz[3 * b], dy = xyz[3 * a + 1] - xyz[3 * b + 1], dz = xyz[3 * a + 2] - xyz[3 * b + 2];
       const double r2 = dx * dx + dy * dy + dz * dz;
       if (r2 <= 1e-24 || r2 > 900.0) {
         zero = true;
-        hij = 0.0;
       } else {
-        overlap_block<false>(la, ea.nprim[ka], ea.alpha[ka], ea.coef[ka], &xyz[3 * a], lb, eb.nprim[kb], eb.alpha[kb],
-                             eb.coef[kb], &xyz[3 * b], 2, Sb, nullptr, nullptr);
         const double rr = sqrt(sqrt(r2) / (ea.rad + eb.rad));
         const double poly = (1.0 + ea.poly[ka] * rr) * (1.0 + eb.poly[kb] * rr);
         hij = 0.5 * (sei + sej) * hscale(M, za, ka, zb, kb) * poly;
       }
     }
-    for (int x = 0; x < na; ++x)
-      for (int y = 0; y < nb; ++y) {
-        const double s = zero ? 0.0 : Sb[x][y];
-        const long long i1 = (long long)(mu0 + x) * N + (nu0 + y);
-        const long long i2 = (long long)(nu0 + y) * N + (mu0 + x);
-        S[i1] = s;
-        S[i2] = s;
-        H0[i1] = s * hij;
-        H0[i2] = s * hij;
-      }
+    switch (la * 2 + lb) {  // s/p shells only on the device path
+      case 0: shell_pair_sh0<0, 0>(ea, ka, &xyz[3 * a], eb, kb, &xyz[3 * b], zero, hij, S, H0, N, mu0, nu0); break;
+      case 1: shell_pair_sh0<0, 1>(ea, ka, &xyz[3 * a], eb, kb, &xyz[3 * b], zero, hij, S, H0, N, mu0, nu0); break;
+      case 2: shell_pair_sh0<1, 0>(ea, ka, &xyz[3 * a], eb, kb, &xyz[3 * b], zero, hij, S, H0, N, mu0, nu0); break;
+      default: shell_pair_sh0<1, 1>(ea, ka, &xyz[3 * a], eb, kb, &xyz[3 * b], zero, hij, S, H0, N, mu0, nu0); break;
+    }
   }
 
   // ---- Klopman-Ohno matrix
