@@ -707,21 +707,29 @@ __device__ void fermi_cta(const double* eps, int N, int nneed, double nelec, dou
 template <int NT>
 __device__ void back_transform(const double* A, int lda, const double* tau, int N, double* Z, int ldz, int ncol,
                                double* W1, double* W2, SccShared& sh) {
-  constexpr int NW = NT / 32;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int nref = N - 2;
   if (nref <= 0 || ncol <= 0) return;
   for (int kb = ((nref - 1) / kBackNB) * kBackNB; kb >= 0; kb -= kBackNB) {
     const int nb = min(kBackNB, nref - kb);
-    for (int p = wid; p < nb * nb; p += NW) {
-      const int i = p / nb, j = p % nb;
-      if (i >= j) continue;
+    // V^T V, one thread per pair i < j (rows >= kb + j + 1 hold both reflectors)
+    for (int p = tid; p < nb * (nb - 1) / 2; p += NT) {
+      int i = 0, rem = p;
+      while (rem >= nb - 1 - i) {
+        rem -= nb - 1 - i;
+        ++i;
+      }
+      const int j = i + 1 + rem;
       const double* vi = A + (long long)(kb + i) * lda;
       const double* vj = A + (long long)(kb + j) * lda;
-      double s = 0.0;
-      for (int r = kb + j + 1 + lane; r < N; r += 32) s += vi[r] * vj[r];
-      s = warp_sum(s);
-      if (lane == 0) sh.VtV[i][j] = s;
+      double s0 = 0.0, s1 = 0.0;
+      int r = kb + j + 1;
+      for (; r + 1 < N; r += 2) {
+        s0 += vi[r] * vj[r];
+        s1 += vi[r + 1] * vj[r + 1];
+      }
+      if (r < N) s0 += vi[r] * vj[r];
+      sh.VtV[i][j] = s0 + s1;
     }
     __syncthreads();
     if (wid == 0) {  // T upper triangular: T_jj = tau_j, T[0:j,j] = -tau_j T[0:j,0:j] V^T v_j
@@ -1118,6 +1126,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
   StageClock clk(B.stage_cycles);
   const MolCtx mc{m, a0, nat, sh0, nsh, N, sh_atom, sh_k, sh_ao0, ao_sh, atom_sh, G};
   // ---- Cholesky S = L L^T (right-looking, in place on L)
+  double* colk = eps;  // current column of L (the eigenvalue slot is free until the first iteration)
   for (long long i = tid; i < (long long)N * N; i += NT) L[i] = S[i];
   __syncthreads();
   for (int k = 0; k < N; ++k) {
@@ -1131,11 +1140,16 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     }
     __syncthreads();
     const double lkk = sh.scal[0];
-    for (int i = k + 1 + tid; i < N; i += NT) L[(long long)i * N + k] /= lkk;
+    for (int i = k + 1 + tid; i < N; i += NT) {  // column k, also staged in shared memory
+      const double v = L[(long long)i * N + k] / lkk;
+      L[(long long)i * N + k] = v;
+      colk[i] = v;
+    }
     __syncthreads();
     for (int i = k + 1 + wid; i < N; i += NW) {
-      const double lik = L[(long long)i * N + k];
-      for (int j = k + 1 + lane; j <= i; j += 32) L[(long long)i * N + j] -= lik * L[(long long)j * N + k];
+      const double lik = colk[i];
+      double* li = L + (long long)i * N;
+      for (int j = k + 1 + lane; j <= i; j += 32) li[j] -= lik * colk[j];
     }
     __syncthreads();
   }
@@ -1149,32 +1163,52 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
   for (int i = wid; i < N; i += NW)
     for (int j = i + 1 + lane; j < N; j += 32) L[(long long)i * N + j] = 0.0;
   __syncthreads();
-  // L^-1, one thread per column
-  for (int j = tid; j < N; j += NT) {
-    for (int i = 0; i < j; ++i) Li[(long long)i * N + j] = 0.0;
-    Li[(long long)j * N + j] = 1.0 / L[(long long)j * N + j];
-    for (int i = j + 1; i < N; ++i) {
-      double s = 0.0;
-      for (int k = j; k < i; ++k) s += L[(long long)i * N + k] * Li[(long long)k * N + j];
-      Li[(long long)i * N + j] = -s / L[(long long)i * N + i];
+  // L^-1 by forward substitution L X = I, one thread per column; all threads
+  // step through the rows together, so row i of L is a broadcast and the reads
+  // of X[k][c] coalesce (the entries above the diagonal come out as zeros)
+  for (int c0 = 0; c0 < N; c0 += NT) {
+    const int c = c0 + tid;
+    const int cc = min(c, N - 1);
+    for (int i = 0; i < N; ++i) {
+      const double* li = L + (long long)i * N;
+      double s0 = (i == c) ? 1.0 : 0.0, s1 = 0.0;
+      int k = 0;
+      for (; k + 1 < i; k += 2) {
+        s0 -= li[k] * Li[(long long)k * N + cc];
+        s1 -= li[k + 1] * Li[(long long)(k + 1) * N + cc];
+      }
+      if (k < i) s0 -= li[k] * Li[(long long)k * N + cc];
+      if (c < N) Li[(long long)i * N + c] = (s0 + s1) / li[i];
     }
   }
   __syncthreads();
-  // H0' = L^-1 H0 L^-T: T = H0 L^-T into the global work matrix, then H0' = L^-1 T
-  double* T = w.A;
+  // H0' = L^-1 H0 L^-T as U = L^-1 H0, then H0' = U (L^-1)^T with (L^-1)^T
+  // stored explicitly, so both products read rows (lanes over columns) and
+  // broadcast the other factor.  U and the transpose use the eigenvector and
+  // global work matrices, free until the first iteration.
+  double* U = w.A;
+  double* LiT = w.Z;
   for (int i = wid; i < N; i += NW)
+    for (int j = lane; j < N; j += 32) LiT[(long long)j * N + i] = Li[(long long)i * N + j];
+  for (int i = wid; i < N; i += NW) {
+    const double* lir = Li + (long long)i * N;
     for (int j = lane; j < N; j += 32) {
       double s = 0.0;
-      for (int k = 0; k <= j; ++k) s += H0[(long long)i * N + k] * Li[(long long)j * N + k];
-      T[(long long)i * N + j] = s;
+#pragma unroll 4
+      for (int k = 0; k <= i; ++k) s += lir[k] * H0[(long long)k * N + j];
+      U[(long long)i * N + j] = s;
     }
+  }
   __syncthreads();
-  for (int i = wid; i < N; i += NW)
+  for (int i = wid; i < N; i += NW) {
+    const double* ur = U + (long long)i * N;
     for (int j = lane; j <= i; j += 32) {
       double s = 0.0;
-      for (int k = 0; k <= i; ++k) s += Li[(long long)i * N + k] * T[(long long)k * N + j];
+#pragma unroll 4
+      for (int k = 0; k <= j; ++k) s += ur[k] * LiT[(long long)k * N + j];
       Hp[(long long)i * N + j] = s;
     }
+  }
   __syncthreads();
   for (int i = wid; i < N; i += NW)
     for (int j = i + 1 + lane; j < N; j += 32) Hp[(long long)i * N + j] = Hp[(long long)j * N + i];
