@@ -74,10 +74,20 @@ struct CtaWs {
   double *L, *Li, *Hp, *A, *Z, *C, *D, *iw, *W1, *W2;
   double *df, *u, *dots, *omega, *beta, *cvec, *qin, *qout, *vsh, *qlast, *dqlast, *qnext, *vout, *qat;
 };
+// Leading dimension of the working matrix: odd in shared memory (strided
+// column accesses spread over the banks), a multiple of four doubles in global
+// memory (every row starts on a 32-byte sector).
+__host__ __device__ inline int work_lda(int n) { return (n & 1) ? n : n + 1; }
+__host__ __device__ inline int work_lda_global(int n) { return (n + 3) & ~3; }
+
+// Slot sizes in doubles; the slot size is a multiple of four and the working
+// matrix A starts on a multiple of four (slots start 32-byte aligned).
 __host__ __device__ inline long long cta_ws_size(int maxn, int maxnsh, int cap, int maxnat) {
   const long long n2 = (long long)maxn * (maxn + 1);
-  return 12 * n2 + 2LL * kBackNB * maxn + 2LL * cap * maxnsh + 2LL * cap * cap + 2LL * cap + 8LL * maxnsh + maxnat +
-         64;
+  const long long na = (long long)maxn * work_lda_global(maxn);
+  const long long t = 11 * n2 + na + 4 + 2LL * kBackNB * maxn + 2LL * cap * maxnsh + 2LL * cap * cap + 2LL * cap +
+                      8LL * maxnsh + maxnat + 64;
+  return (t + 3) & ~3LL;
 }
 __device__ __forceinline__ CtaWs cta_ws(double* base, int maxn, int maxnsh, int cap) {
   CtaWs w;
@@ -85,8 +95,8 @@ __device__ __forceinline__ CtaWs cta_ws(double* base, int maxn, int maxnsh, int 
   w.L = base;
   w.Li = w.L + n2;
   w.Hp = w.Li + n2;
-  w.A = w.Hp + n2;
-  w.Z = w.A + n2;
+  w.A = base + ((3 * n2 + 3) & ~3LL);
+  w.Z = w.A + (long long)maxn * work_lda_global(maxn);
   w.C = w.Z + n2;
   w.D = w.C + n2;
   w.iw = w.D + n2;  // 5 * n2
@@ -116,9 +126,6 @@ __host__ __device__ inline size_t scc_smem_fixed(int maxnsh, int maxn, int maxna
   const size_t ib = ((size_t)4 * scc_ints(maxnsh, maxn, maxnat) + 15) & ~(size_t)15;
   return ib + sizeof(double) * kVecSlots * (size_t)maxn;
 }
-// Odd leading dimension of the working matrix: strided column accesses then
-// spread over the shared-memory banks.
-__host__ __device__ inline int work_lda(int n) { return (n & 1) ? n : n + 1; }
 
 // Sturm count and characteristic polynomial at x for the symmetric tridiagonal
 // (d, esq = e^2): returns #eigenvalues <= x and the values p, p', p'' of
@@ -1103,8 +1110,9 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
   double* D = w.D;
   double* iw = w.iw;
   const double* G = B.gam + B.gam_off[m];
-  const int lda = work_lda(N);
-  double* A = ((long long)N * lda <= as_cap) ? As : w.A;  // shared memory when it fits
+  const bool a_shared = (long long)N * work_lda(N) <= as_cap;  // shared memory when the launch gave room
+  const int lda = a_shared ? work_lda(N) : work_lda_global(N);
+  double* A = a_shared ? As : w.A;
   double* d = vec;
   double* e = vec + N;
   double* tau = vec + 2 * N;
