@@ -32,6 +32,8 @@ size_t scc_smem_bytes(int maxnsh, int maxn, int maxnat, int matrix_n);
 size_t scc_max_dynamic_smem(int nt);
 cudaError_t launch_scc(int nt, int grid, size_t smem, cudaStream_t st, const Batch& B, const Model& M,
                        const SccOptions& opt, const SccLaunch& SL);
+cudaError_t launch_scc_robust(int nt, int grid, size_t smem, cudaStream_t st, const Batch& B, const Model& M,
+                              const SccOptions& opt, const SccLaunch& SL);
 long long dense_ws_doubles(int maxnsh, int cap, int maxnat);
 size_t dense_smem_bytes(int maxnsh, int maxn, int maxnat);
 size_t dense_state_bytes();
@@ -266,6 +268,8 @@ struct gfn1_batch {
     long long ws_offset = 0, ws_stride = 0;
     size_t smem = 0;
   } cls[2];
+  SccClass robust;  // fallback ladder: workspace for the batch's largest molecule, a few CTAs
+  DevBuf<int> failed;
   cudaStream_t side = nullptr;  // second stream for the concurrent class launch
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   gfn1_options opt;
@@ -337,6 +341,7 @@ struct gfn1_batch {
     B.iterations = dout<int>(lay.iterations);
     B.status = dout<int>(lay.status);
     B.queue = queue.p;
+    B.failed = failed.p;
     B.stage_cycles = profiling ? stage.p : nullptr;
     return B;
   }
@@ -348,6 +353,7 @@ struct gfn1_batch {
     for (DevBuf<double>* d : {&S, &H0, &P, &W, &ws, &gam, &pairbuf, &cn, &shell_pot, &se, &grad_classic}) d->release();
     queue.release();
     stage.release();
+    failed.release();
     gx.release();
     gy.release();
     gq.release();
@@ -760,6 +766,26 @@ int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t*
     // the matrix: 98 vs 105 ms for the SCC stage of the 4096-molecule batch).
     K.smem = fixed;
   }
+  {  // fallback ladder: molecules the rung-0 launches leave unconverged, rerun by a few CTAs
+    gfn1_batch::SccClass& R = b->robust;
+    R.maxn = R.maxnsh = R.maxnat = 0;
+    for (int q = n_dense; q < nmol; ++q) {
+      const int mm = h_order[q];
+      R.maxn = std::max(R.maxn, n_m[mm]);
+      R.maxnsh = std::max(R.maxnsh, nsh_m[mm]);
+      R.maxnat = std::max(R.maxnat, atom_offsets[mm + 1] - atom_offsets[mm]);
+    }
+    const int count = nmol - n_dense;
+    R.nt = 128;
+    const size_t fixed = scc_smem_bytes(R.maxnsh, R.maxn, R.maxnat, 0);
+    while (R.nt < 512 && fixed > scc_max_dynamic_smem(R.nt)) R.nt *= 2;
+    R.n_cta = count == 0 ? 0 : std::min(count, 64);
+    R.ws_stride = count == 0 ? 0 : scc_workspace_doubles(std::max(R.maxn, 1), std::max(R.maxnsh, 1), b->cap,
+                                                           std::max(R.maxnat, 1));
+    R.ws_offset = ws_total;
+    ws_total += R.ws_stride * R.n_cta;
+    R.smem = fixed;
+  }
   if (!b->side) {
     if (cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
@@ -767,6 +793,7 @@ int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t*
       return fail(eng, GFN1_E_DEVICE, "stream creation failed");
   }
   bool ok = b->d_in.ensure(L.in_bytes) && b->d_out.ensure(L.out_bytes) && b->queue.ensure(4) &&
+            b->failed.ensure((size_t)nmol) &&
             b->stage.ensure(kStages) && b->S.ensure(mat_total) && b->H0.ensure(mat_total) && b->P.ensure(mat_total) &&
             b->W.ensure(mat_total) && b->ws.ensure((size_t)std::max<long long>(ws_total, 1)) && b->gam.ensure(gam_total) &&
             b->pairbuf.ensure(8 * std::max<long long>(pair_total, 1)) && b->cn.ensure(natoms) &&
@@ -891,6 +918,22 @@ int launch_stage(gfn1_batch* b, int stage, cudaStream_t st) {
     }
     if ((e = cudaEventRecord(b->ev_join, b->side)) != cudaSuccess || (e = cudaStreamWaitEvent(st, b->ev_join, 0)) != cudaSuccess)
       return cuda_fail(eng, e, "stream join");
+    if (b->robust.n_cta > 0) {  // rungs 1-3 for whatever rung 0 left unconverged (exits at once if nothing)
+      const gfn1_batch::SccClass& R = b->robust;
+      SccLaunch SL;
+      SL.q_begin = 0;
+      SL.q_end = 0;
+      SL.counter = b->queue.p + 2;
+      SL.ws = b->ws.p + R.ws_offset;
+      SL.ws_stride = R.ws_stride;
+      SL.maxn = R.maxn;
+      SL.maxnsh = R.maxnsh;
+      SL.maxnat = R.maxnat;
+      SL.cap = b->cap;
+      SL.smem_bytes = (int)R.smem;
+      if ((e = launch_scc_robust(R.nt, R.n_cta, R.smem, st, B, M, so, SL)) != cudaSuccess)
+        return cuda_fail(eng, e, "scc fallback launch");
+    }
     if (!b->dense_ids.empty()) {  // large molecules: host-driven, one at a time, next to the class launches
       // wait for the setup kernel only (ev_fork was recorded before the class launches)
       if ((e = cudaStreamWaitEvent(b->dense_stream, b->ev_fork, 0)) != cudaSuccess)
@@ -1144,9 +1187,9 @@ int gfn1_batch_info(const gfn1_batch* b, int64_t* natoms, int64_t* nshells, int6
   if (natoms) *natoms = b->natoms;
   if (nshells) *nshells = b->nshells;
   if (naos) *naos = b->naos;
-  if (launches)  // setup, one SCC launch per non-empty size class, gradient, learned guess
-    *launches = 1 + (b->cls[0].n_cta > 0) + (b->cls[1].n_cta > 0) + (b->opt.compute_gradient ? 1 : 0) +
-                (b->guess && !b->has_init_q ? 3 : 0);
+  if (launches)  // setup, one SCC launch per non-empty size class, the fallback ladder, gradient, learned guess
+    *launches = 1 + (b->cls[0].n_cta > 0) + (b->cls[1].n_cta > 0) + (b->robust.n_cta > 0) +
+                (b->opt.compute_gradient ? 1 : 0) + (b->guess && !b->has_init_q ? 3 : 0);
   return GFN1_OK;
 }
 

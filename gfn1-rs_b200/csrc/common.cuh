@@ -130,7 +130,8 @@ struct Batch {
   double* fermi;            // [nmol]
   int* iterations;          // [nmol]
   int* status;              // [nmol]
-  int* queue;               // work counters
+  int* queue;               // work counters: [0], [1] size classes, [2] fallback ladder, [3] failed count
+  int* failed;              // [nmol] molecules whose first SCC attempt did not converge, or null
   unsigned long long* stage_cycles;  // [kStages] per-stage clock totals, or null
 };
 

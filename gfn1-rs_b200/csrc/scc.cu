@@ -1089,7 +1089,7 @@ __device__ void stage_results(const Batch& B, const MolCtx& c, CtaWs& w, int ite
   for (int a = tid; a < nat; a += NT) B.atom_q[a0 + a] = w.qat[a];
 }
 
-template <int NT>
+template <int NT, bool Robust>
 __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& opt, const SccLaunch& SL, int m,
                              SccShared& sh, int* sh_atom, int* sh_k, int* ao_sh, int* atom_sh, int* sh_ao0,
                              double* vec, double* As, long long as_cap) {
@@ -1225,8 +1225,6 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
   double nref = 0.0;
   for (int s = 0; s < nsh; ++s) nref += M.elem[B.z[a0 + sh_atom[s]]].refocc[sh_k[s]];
   const double nelec = nref - B.charge[m];
-  const double kt = fmax(opt.etemp, 0.0) * kBoltzmann;
-  for (int s = tid; s < nsh; s += NT) w.qin[s] = B.init_q ? B.init_q[sh0 + s] : 0.0;
   const int nneed0 = min(N, max(1, (int)ceil(0.5 * nelec) + 8));
   int bro_iter = 0;
   double last_e = 0.0;
@@ -1235,10 +1233,34 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
   int iter = 0;
   int nocc = 0;
   double e_el = 0.0, e2 = 0.0, e3 = 0.0, ts = 0.0, mu = 0.0, rms = 0.0;
+  // The reference's fallback ladder (src/electronic.rs:1390-1447): rung 0 is
+  // the requested options (the main kernel); rungs 1-3 (the Robust kernel,
+  // for molecules rung 0 left unconverged) restart from the initial charges
+  // with linear mixing 0.2 and a 0.2 Eh level shift, then 0.1 / 0.1, then
+  // Broyden at T_el >= 3000 K.
+  const int rung_first = Robust ? 1 : 0, rung_last = Robust ? 3 : 0;
+  for (int rung = rung_first; rung <= rung_last && !converged; ++rung) {
+  SccOptions ro = opt;
+  double lshift = 0.0;  // the plain path has no level shift on rung 0
+  if (rung == 1 || rung == 2) {
+    ro.broyden = 0;
+    ro.mixing = rung == 1 ? 0.20 : 0.10;
+    lshift = rung == 1 ? 0.20 : 0.10;
+    ro.max_scc = max(opt.max_scc, 800);
+  } else if (rung == 3) {
+    ro.etemp = fmax(opt.etemp, 3000.0);
+    ro.max_scc = max(opt.max_scc, 250);
+  }
+  const double kt = fmax(ro.etemp, 0.0) * kBoltzmann;
+  for (int s = tid; s < nsh; s += NT) w.qin[s] = B.init_q ? B.init_q[sh0 + s] : 0.0;
+  bro_iter = 0;
+  last_e = 0.0;
+  have_e = false;
+  bool have_prev = false;  // a previous density to shift against (rungs with a level shift)
   __syncthreads();
   clk.mark(kStPrologue);
 
-  for (iter = 1; iter <= opt.max_scc; ++iter) {
+  for (iter = 1; iter <= ro.max_scc; ++iter) {
     // (1) shell potential from the input charges
     stage_potential<NT>(B, M, mc, w, vao);
     // (2) F' = H0' - 1/2 (M + M^T), M = L^-1 diag(v) L; warps own 4-row groups,
@@ -1269,6 +1291,21 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
       }
     }
     __syncthreads();
+    if (Robust && lshift != 0.0 && have_prev) {
+      // level shift F += lshift (S - S P_prev S / 2) (src/electronic.rs:2125-2137);
+      // in the orthonormal basis F' += lshift (I - Z f Z^T / 2) with the
+      // previous iteration's eigenvectors Z and occupations f
+      for (long long idx = tid; idx < (long long)N * N; idx += NT) {
+        const int i = (int)(idx / N), j = (int)(idx % N);
+        if (j > i) continue;
+        double sp = 0.0;
+        for (int k = 0; k < nocc; ++k) sp += occ[k] * Z[(long long)i * N + k] * Z[(long long)j * N + k];
+        const double val = lshift * ((i == j ? 1.0 : 0.0) - 0.5 * sp);
+        A[(long long)i * lda + j] += val;
+        if (i != j) A[(long long)j * lda + i] += val;
+      }
+      __syncthreads();
+    }
     clk.mark(kStFock);
     // (3) Householder tridiagonalisation
     tridiagonalize<NT>(A, lda, N, d, e, tau, pvec, sh);
@@ -1429,6 +1466,17 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     clk.mark(kStPop);
     // (9) output charges, energies
     stage_charges_energy<NT>(B, M, mc, w, pop, occ, eps, vao, nocc, sh, e_el, e2, e3, rms);
+    if (Robust && lshift != 0.0) {
+      // with a shifted Fock matrix sum(f eps) is not tr(F P): E_el = tr(H0 P) = sum_k f_k z_k^T H0' z_k
+      double part = 0.0;
+      for (long long idx = tid; idx < (long long)N * nocc; idx += NT) {
+        const int i = (int)(idx / nocc), k = (int)(idx % nocc);
+        double hz = 0.0;
+        for (int j = 0; j < N; ++j) hz += Hp[(long long)i * N + j] * Z[(long long)j * N + k];
+        part += occ[k] * Z[(long long)i * N + k] * hz;
+      }
+      e_el = block_sum(part, sh.red);
+    }
     const double escc = e_el + e2 + e3 + ts;
     const double err = have_e ? fabs(escc - last_e) : INFINITY;
     if (err < opt.energy_tol && rms < opt.charge_tol) {
@@ -1437,13 +1485,16 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     }
     clk.mark(kStEnergy);
     // (10) charge mixing
-    stage_mix<NT>(opt, mc, w, cap, bro_iter, sh);
+    stage_mix<NT>(ro, mc, w, cap, bro_iter, sh);
     last_e = escc;
     have_e = true;
+    have_prev = lshift != 0.0;
     __syncthreads();
     clk.mark(kStMix);
   }
-  if (iter > opt.max_scc) iter = opt.max_scc;
+  if (iter > ro.max_scc) iter = ro.max_scc;
+  }  // rungs
+  if (!Robust && !converged && B.failed && tid == 0) B.failed[atomicAdd(B.queue + 3, 1)] = m;
 
   // ---- results
   stage_results<NT>(B, mc, w, iter, converged, e_el, e2, e3, ts, mu);
@@ -1466,7 +1517,10 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
   clk.mark(kStFinal);
 }
 
-template <int NT>
+// Persistent SCC kernel.  Robust = false: molecules q_begin..q_end of the
+// processing order (rung 0 of the fallback ladder); Robust = true: the
+// molecules the rung-0 launches left unconverged (rungs 1-3).
+template <int NT, bool Robust>
 __global__ void __launch_bounds__(NT, 512 / NT) scc_kernel(Batch B, Model M, SccOptions opt, SccLaunch SL) {
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ SccShared sh;
@@ -1480,15 +1534,22 @@ __global__ void __launch_bounds__(NT, 512 / NT) scc_kernel(Batch B, Model M, Scc
   double* vec = (double*)(smraw + ib);
   double* As = vec + (size_t)kVecSlots * SL.maxn;
   const long long as_cap = ((long long)SL.smem_bytes - (long long)scc_smem_fixed(SL.maxnsh, SL.maxn, SL.maxnat)) / 8;
+  const int nfailed = Robust ? B.queue[3] : 0;  // written by the rung-0 launches before this one
   for (;;) {
-    if (threadIdx.x == 0) next = SL.q_begin + atomicAdd(SL.counter, 1);
+    if (threadIdx.x == 0) next = Robust ? atomicAdd(B.queue + 2, 1) : SL.q_begin + atomicAdd(SL.counter, 1);
     __syncthreads();
     const int idx = next;
     __syncthreads();
-    if (idx >= SL.q_end) break;
-    const int m = B.order[idx];
-    if (B.status[m] != kOk) continue;  // rejected during setup
-    scc_molecule<NT>(B, M, opt, SL, m, sh, sh_atom, sh_k, ao_sh, atom_sh, sh_ao0, vec, As, as_cap);
+    int m;
+    if (Robust) {
+      if (idx >= nfailed) break;
+      m = B.failed[idx];
+    } else {
+      if (idx >= SL.q_end) break;
+      m = B.order[idx];
+      if (B.status[m] != kOk) continue;  // rejected during setup
+    }
+    scc_molecule<NT, Robust>(B, M, opt, SL, m, sh, sh_atom, sh_k, ao_sh, atom_sh, sh_ao0, vec, As, as_cap);
   }
 }
 
@@ -1812,20 +1873,20 @@ size_t scc_smem_bytes(int maxnsh, int maxn, int maxnat, int matrix_n) {
 // the kernel's static shared memory.
 size_t scc_max_dynamic_smem(int nt) {
   cudaFuncAttributes a;
-  const cudaError_t e = nt == 512   ? cudaFuncGetAttributes(&a, scc_kernel<512>)
-                        : nt == 256 ? cudaFuncGetAttributes(&a, scc_kernel<256>)
-                                    : cudaFuncGetAttributes(&a, scc_kernel<128>);
+  const cudaError_t e = nt == 512   ? cudaFuncGetAttributes(&a, scc_kernel<512, false>)
+                        : nt == 256 ? cudaFuncGetAttributes(&a, scc_kernel<256, false>)
+                                    : cudaFuncGetAttributes(&a, scc_kernel<128, false>);
   const size_t stat = e == cudaSuccess ? a.sharedSizeBytes : 8192;
   const size_t per_cta = 233472 / (512 / nt) - 1024;  // the SM's 228 KB shared by 512/nt CTAs
   return per_cta - stat - 256;
 }
 
-template <int NT>
+template <int NT, bool Robust>
 static cudaError_t launch_scc_nt(int grid, size_t smem, cudaStream_t st, const Batch& B, const Model& M,
                                  const SccOptions& opt, const SccLaunch& SL) {
-  cudaError_t e = cudaFuncSetAttribute(scc_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(scc_kernel<NT, Robust>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  scc_kernel<NT><<<grid, NT, smem, st>>>(B, M, opt, SL);
+  scc_kernel<NT, Robust><<<grid, NT, smem, st>>>(B, M, opt, SL);
   return cudaGetLastError();
 }
 
@@ -1833,9 +1894,19 @@ static cudaError_t launch_scc_nt(int grid, size_t smem, cudaStream_t st, const B
 // 512 / nt CTAs share an SM).
 cudaError_t launch_scc(int nt, int grid, size_t smem, cudaStream_t st, const Batch& B, const Model& M,
                        const SccOptions& opt, const SccLaunch& SL) {
-  if (nt == 512) return launch_scc_nt<512>(grid, smem, st, B, M, opt, SL);
-  if (nt == 256) return launch_scc_nt<256>(grid, smem, st, B, M, opt, SL);
-  if (nt == 128) return launch_scc_nt<128>(grid, smem, st, B, M, opt, SL);
+  if (nt == 512) return launch_scc_nt<512, false>(grid, smem, st, B, M, opt, SL);
+  if (nt == 256) return launch_scc_nt<256, false>(grid, smem, st, B, M, opt, SL);
+  if (nt == 128) return launch_scc_nt<128, false>(grid, smem, st, B, M, opt, SL);
+  return cudaErrorInvalidValue;
+}
+
+// Host launcher of the fallback-ladder kernel (rungs 1-3 for the molecules
+// listed in B.failed; returns at once when the list is empty).
+cudaError_t launch_scc_robust(int nt, int grid, size_t smem, cudaStream_t st, const Batch& B, const Model& M,
+                              const SccOptions& opt, const SccLaunch& SL) {
+  if (nt == 512) return launch_scc_nt<512, true>(grid, smem, st, B, M, opt, SL);
+  if (nt == 256) return launch_scc_nt<256, true>(grid, smem, st, B, M, opt, SL);
+  if (nt == 128) return launch_scc_nt<128, true>(grid, smem, st, B, M, opt, SL);
   return cudaErrorInvalidValue;
 }
 

@@ -114,11 +114,52 @@ def test_unsupported_element_is_rejected(calc, fixtures):
     assert r.status[0] == 12
 
 
-def test_not_converged_status(calc, fixtures):
-    z, x = smoke_molecule(fixtures, "caffeine")
-    calc.opts.update(max_scc=2, energy_tolerance=1e-12, charge_tolerance=1e-12)
+def test_not_converged_status_matches_oracle(calc, oracle_mod, fixtures):
+    """Zero tolerances (|dE| < 0 never holds): every rung of the fallback ladder
+    runs to its limit and both report SCC not converged."""
+    z, x = smoke_molecule(fixtures, "water")
+    opts = dict(max_scc=2, energy_tolerance=0.0, charge_tolerance=0.0)
+    calc.opts.update(opts)
     r = calc.calculate_flat([0, len(z)], z, x)
+    with pytest.raises(oracle_mod.OracleError) as ei:
+        oracle_mod.run(z, x, options=oracle_mod.make_options(**opts), gradient=False)
+    assert ei.value.code == 8
     assert r.status[0] == 8
+    assert r.iterations[0] == 250  # the last rung's limit, max(max_scc, 250)
+
+
+@pytest.mark.parametrize("name", ["water", "caffeine"])
+def test_fallback_ladder_matches_oracle(calc, oracle_mod, fixtures, name):
+    """max_scc = 1 leaves rung 0 unconverged; the device ladder (linear mixing +
+    level shift, src/electronic.rs:1390-1447) must land where the oracle's does,
+    with the same iteration count."""
+    z, x = smoke_molecule(fixtures, name)
+    calc.opts.update(max_scc=1)
+    r = calc.calculate_flat([0, len(z)], z, x, raise_on_error=True)
+    o = oracle_mod.run(z, x, options=oracle_mod.make_options(max_scc=1))
+    assert r.status[0] == 0 and o.converged
+    assert abs(r.energy[0] - o.energy) <= E_TOL
+    assert np.abs(r.gradient - o.gradient).max() <= G_TOL
+    assert np.abs(r.shell_charges - o.shell_charges).max() <= Q_TOL
+    assert r.iterations[0] == o.iterations
+
+
+def test_fallback_ladder_in_a_batch(calc, oracle_mod, fixtures):
+    """Only the molecules rung 0 leaves unconverged are rerun; the others keep
+    their rung-0 result."""
+    zs, xs, off = [], [], [0]
+    mols = [(np.array(fixtures["xyz"][n]["numbers"]), np.array(fixtures["xyz"][n]["positions_angstrom"]) * ANGSTROM_TO_BOHR)
+            for n in ("water", "ammonia", "methane")]
+    mols.append(smoke_molecule(fixtures, "caffeine"))
+    for z, x in mols:
+        zs.append(z), xs.append(x), off.append(off[-1] + len(z))
+    off = np.array(off, np.int32)
+    calc.opts.update(max_scc=7)  # caffeine needs 10 iterations at rung 0, the others 5-6
+    r = calc.calculate_flat(off, np.concatenate(zs), np.concatenate(xs), raise_on_error=True)
+    for k, (z, x) in enumerate(zip(zs, xs)):
+        o = oracle_mod.run(z, x, options=oracle_mod.make_options(max_scc=7), gradient=False)
+        assert abs(r.energy[k] - o.energy) <= E_TOL
+        assert r.iterations[k] == o.iterations
 
 
 def test_charged_molecule(calc, oracle_mod, fixtures):
