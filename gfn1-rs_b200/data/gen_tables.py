@@ -187,6 +187,8 @@ def main(root: str) -> None:
             v = e.get(key, [default])[0]
             assert v is not None, (z, key)
             w(f"elem.{z}.{key.lower()} 1 {fmt(v)}")
+        if "CXB" in e:  # halogen-bond strength, present for Br, I and At only
+            w(f"elem.{z}.cxb 1 {fmt(e['CXB'][0])}")
     nf = 15
     for ng in range(1, 7):
         alpha = _rust_array(sto, f"P_ALPHA{ng}")

@@ -1125,17 +1125,67 @@ double dispersion(const System& s, std::vector<Vec3>* grad) {
   return e;
 }
 
-// ---------------------------------------------------------------- halogen guard
-// src/halogen.rs:716-770: donors Cl/Br/I/At, acceptors N/O/P/S.  Not restated:
-// molecules that could carry the term are rejected.
-void check_halogen(const System& s) {
-  bool donor = false, acceptor = false;
-  for (int z : s.z) {
-    if (z == 17 || z == 35 || z == 53 || z == 85) donor = true;
-    if (z == 7 || z == 8 || z == 15 || z == 16) acceptor = true;
+// ---------------------------------------------------------------- halogen bonds
+// src/halogen.rs:64-160 (energy and gradient) with the triples of :716-786.
+// Each donor X (Cl, Br, I, At) whose strength c = 0.1 CXB is non-zero pairs
+// with its nearest other atom K and with every acceptor J (N, O, P, S) within
+// 20 bohr (r^2 > 1e-24 and r^2 <= 400).  With T = (r_KX^2 + r_JX^2 - r_JK^2) /
+// (r_KX r_JX) (twice the cosine of the K-X-J angle), b = 1/2 - T/4 and
+// u = (r0 / r_JX)^6, r0 = xbrad (R_X + R_J) in the xTB atomic radii,
+//   E_XJ = c b^6 (u^2 - xbdamp u) / (1 + u^2),
+// where r_JX carries the reference's +1e-18.  The gradient is written as the
+// derivatives of E_XJ with respect to the three squared distances.
+bool is_halogen_donor(int z) { return z == 17 || z == 35 || z == 53 || z == 85; }
+bool is_halogen_acceptor(int z) { return z == 7 || z == 8 || z == 15 || z == 16; }
+
+double halogen(const System& s, std::vector<Vec3>* grad) {
+  const double cutoff2 = 20.0 * 20.0, eps = 1e-18;
+  double e = 0.0;
+  for (int x = 0; x < s.nat(); ++x) {
+    if (!is_halogen_donor(s.z[x])) continue;
+    const std::string key = "elem." + std::to_string(s.z[x]) + ".cxb";
+    const double c = 0.1 * (g_tables.has(key) ? g_tables.get(key)[0] : 0.0);
+    int k = -1;
+    double kr2 = 0.0;
+    for (int j = 0; j < s.nat(); ++j) {  // nearest other atom inside the cutoff
+      if (j == x) continue;
+      const double r2 = (s.pos[j] - s.pos[x]).norm2();
+      if (r2 <= 1e-24 || r2 > cutoff2) continue;
+      if (k < 0 || r2 < kr2) { k = j; kr2 = r2; }
+    }
+    if (k < 0 || c == 0.0) continue;
+    const double damp = g_params.req("xbdamp"), rscale = g_params.req("xbrad");
+    for (int j = 0; j < s.nat(); ++j) {
+      if (j == x || !is_halogen_acceptor(s.z[j])) continue;
+      const Vec3 vjx = s.pos[j] - s.pos[x], vkx = s.pos[k] - s.pos[x], vjk = s.pos[j] - s.pos[k];
+      const double djx = vjx.norm2(), dkx = vkx.norm2(), djk = vjk.norm2();
+      if (djx <= 1e-24 || djx > cutoff2) continue;  // outside the donor's neighbour list
+      if (djx <= eps || dkx <= eps) continue;
+      const double rjx = std::sqrt(djx) + eps, rkx = std::sqrt(dkx) + eps;
+      const double xy = std::sqrt(dkx * djx);
+      if (xy <= eps) continue;
+      const double T = (dkx + djx - djk) / xy;
+      const double b = 0.5 - 0.25 * T;
+      const double b5 = std::pow(b, 5.0), b6 = b5 * b;
+      const double r0 = rscale * (atomic_radius_bohr(s.z[x]) + atomic_radius_bohr(s.z[j]));
+      const double u = std::pow(r0 / rjx, 6.0);
+      const double num = u * u - damp * u, den = 1.0 + u * u;
+      const double L = num / den;
+      e += c * b6 * L;
+      if (!grad) continue;
+      // dL/dr_JX and dE/dT
+      const double dL = (6.0 * u * (damp - 2.0 * u) / den + 12.0 * u * u * num / (den * den)) / rjx;
+      const double dET = -1.5 * c * b5 * L;
+      // dE/d(r^2) for the three squared distances
+      const double gjx = dET * (1.0 / (rkx * rjx) - 0.5 * T / (rjx * rjx)) + 0.5 * c * b6 * dL / rjx;
+      const double gkx = dET * (1.0 / (rkx * rjx) - 0.5 * T / (rkx * rkx));
+      const double gjk = -dET / xy;
+      (*grad)[j] += vjx * (2.0 * gjx) + vjk * (2.0 * gjk);
+      (*grad)[x] -= vjx * (2.0 * gjx) + vkx * (2.0 * gkx);
+      (*grad)[k] += vkx * (2.0 * gkx) - vjk * (2.0 * gjk);
+    }
   }
-  if (donor && acceptor)
-    throw OracleError(E_INVALID_INPUT, "halogen-bond correction is not part of the restated path");
+  return e;
 }
 
 // ---------------------------------------------------------------- SCC
@@ -1167,7 +1217,6 @@ Result run(const System& sys, const Options& opt, const double* init_q, bool wan
     if (!(std::isfinite(sys.pos[a].x) && std::isfinite(sys.pos[a].y) && std::isfinite(sys.pos[a].z)))
       throw OracleError(E_INVALID_INPUT, "non-finite coordinate");
   }
-  check_halogen(sys);
   Basis b = build_basis(sys.z);
   int n = (int)b.aos.size(), nsh = (int)b.shells.size();
   res.nao = n;
@@ -1374,7 +1423,7 @@ Result run(const System& sys, const Options& opt, const double* init_q, bool wan
   // --- final assembly (src/electronic.rs:1957-2053)
   double eel = e_el(last.P);
   Coul sc = coulomb(b, A, last.q, nat);
-  double ehal = 0.0;
+  double ehal = halogen(sys, nullptr);
   double total_internal = eel + sc.e2 + sc.e3 + erep + edisp + ehal;
   double total_free = total_internal + last.ts;
   // named_values order, src/electronic.rs:681-699
@@ -1484,9 +1533,11 @@ Result run(const System& sys, const Options& opt, const double* init_q, bool wan
   }
   for (int a = 0; a < nat; ++a) g[a] += gel[a];
   std::vector<Vec3> grep(nat), gdisp(nat);
+  std::vector<Vec3> ghal(nat);
   repulsion(sys, &grep);
   if (opt.enable_dispersion) dispersion(sys, &gdisp);
-  for (int a = 0; a < nat; ++a) g[a] += grep[a] + gdisp[a];
+  halogen(sys, &ghal);
+  for (int a = 0; a < nat; ++a) g[a] += grep[a] + gdisp[a] + ghal[a];
   res.grad = g;
   return res;
 }
@@ -1546,6 +1597,24 @@ int oracle_sizes(int nat, const int* z, int* nao, int* nsh) {
     Basis b = build_basis(zs);
     *nao = (int)b.aos.size();
     *nsh = (int)b.shells.size();
+    return OK;
+  } catch (const OracleError& e) {
+    t_err = e.what();
+    return e.code;
+  }
+}
+
+// The halogen-bond term alone (src/halogen.rs:64-160): energy and, when grad
+// is not null, its gradient [nat*3].
+int oracle_halogen(int nat, const int* z, const double* xyz_bohr, double* energy, double* grad) {
+  try {
+    System s;
+    s.z.assign(z, z + nat);
+    for (int a = 0; a < nat; ++a) s.pos.push_back(Vec3(xyz_bohr[3 * a], xyz_bohr[3 * a + 1], xyz_bohr[3 * a + 2]));
+    std::vector<Vec3> g(nat);
+    *energy = halogen(s, grad ? &g : nullptr);
+    if (grad)
+      for (int a = 0; a < nat; ++a) { grad[3 * a] = g[a].x; grad[3 * a + 1] = g[a].y; grad[3 * a + 2] = g[a].z; }
     return OK;
   } catch (const OracleError& e) {
     t_err = e.what();

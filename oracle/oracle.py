@@ -100,6 +100,7 @@ def lib():
         L.oracle_sizes.argtypes = [ctypes.c_int, ip, ip, ip]
         L.oracle_run.argtypes = [ctypes.c_int, ip, dp, ctypes.POINTER(OracleOptions), dp, ctypes.c_int,
                                  dp, dp, dp, dp, dp, dp, dp, dp, ip, ip, dp, dp, dp, dp, dp]
+        L.oracle_halogen.argtypes = [ctypes.c_int, ip, dp, dp, dp]
         L.oracle_run_batch.argtypes = [ctypes.c_int, ip, ip, dp, dp, ctypes.POINTER(OracleOptions), ctypes.c_int,
                                        ctypes.c_int, dp, dp, ip, dp, ip, ip]
         rc = L.oracle_init(TABLES_PATH.encode())
@@ -158,6 +159,19 @@ def run(numbers, positions_bohr, options: OracleOptions | None = None, gradient:
                         shell_charges=qsh, atomic_charges=qat, orbital_energies=eps, occupations=occ,
                         dipole=dip, coordination_numbers=cn, iterations=it.value, converged=bool(conv.value),
                         fermi_level=fermi.value, S=mats[0], H0=mats[1], P=mats[2], W=mats[3])
+
+
+def halogen(numbers, positions_bohr, gradient: bool = True):
+    """Halogen-bond energy (Eh) and gradient (Eh/bohr) of one molecule."""
+    L = lib()
+    z = np.ascontiguousarray(numbers, dtype=np.int32)
+    x = np.ascontiguousarray(positions_bohr, dtype=np.float64).reshape(-1, 3)
+    e = np.zeros(1)
+    g = np.zeros((len(z), 3)) if gradient else None
+    rc = L.oracle_halogen(len(z), _ip(z), _dp(x), _dp(e), _dp(g))
+    if rc != 0:
+        raise OracleError(rc, L.oracle_last_error().decode())
+    return float(e[0]), g
 
 
 def run_batch(atom_offsets, numbers, positions_bohr, charges=None, options: OracleOptions | None = None,

@@ -5,7 +5,9 @@ Sources (gfn1-rs v0.5.1):
   stored absolute result in the reference tree);
 * examples/{h2,water,ammonia,methane,water48,water100}.xyz: geometries;
 * the molecules embedded in tests/nonpbc_smoke.rs:14-50 (H/C/N/O/F/B/P subset),
-  read as text.
+  read as text;
+* the halogen-bond test systems embedded in src/halogen.rs (its unit tests,
+  from :788), keyed by their xyz title line.
 
 Run where the reference tree is available:
     python tests/golden/make_golden.py /path/to/gfn1-rs
@@ -34,7 +36,7 @@ def read_engrad(path: Path) -> dict:
 
 
 SYMBOLS = {"H": 1, "He": 2, "Li": 3, "Be": 4, "B": 5, "C": 6, "N": 7, "O": 8, "F": 9, "Ne": 10, "P": 15,
-           "S": 16, "Cl": 17, "Fe": 26}
+           "S": 16, "Cl": 17, "Fe": 26, "Br": 35, "I": 53}
 
 
 def read_xyz_text(text: str) -> dict:
@@ -63,6 +65,16 @@ def main(root: str) -> None:
         rec["gradient_fd"] = m.group(3) == "true"
         mols[m.group(1)] = rec
     out["nonpbc_smoke"] = mols
+    hal = {}
+    src = (root / "src/halogen.rs").read_text()
+    for m in re.finditer(r'from_xyz_str\(\s*"((?:[^"\\]|\\.)*)"', src, re.S):
+        lit = re.sub(r"\\\n\s*", "", m.group(1))  # Rust line continuations
+        text = lit.encode().decode("unicode_escape")
+        title = text.splitlines()[1].strip()
+        if "Lattice=" in title:  # periodic systems are outside the molecular path
+            continue
+        hal.setdefault(title, read_xyz_text(text))
+    out["halogen_tests"] = hal
     dest = Path(__file__).with_name("reference_fixtures.json")
     dest.write_text(json.dumps(out, indent=1) + "\n")
 
