@@ -407,7 +407,7 @@ bool build_elements(gfn1_engine* eng, const Tables& t, std::string& err) {
   g.kexp = t.scalar("glob.kexp", 1.5);
   g.kexplight = t.scalar("glob.kexplight", g.kexp);
   g.s6 = t.scalar("glob.s6", 1.0);
-  for (const char* k : {"glob.a1", "glob.a2", "glob.s8", "glob.s9"}) {
+  for (const char* k : {"glob.a1", "glob.a2", "glob.s8", "glob.s9", "glob.xbdamp", "glob.xbrad"}) {
     if (!t.has(k)) {
       err = std::string("missing required $globpar entry `") + (k + 5) + "`";
       return false;
@@ -416,11 +416,14 @@ bool build_elements(gfn1_engine* eng, const Tables& t, std::string& err) {
   g.a1 = t.scalar("glob.a1", 0);
   g.a2 = t.scalar("glob.a2", 0);
   g.s8 = t.scalar("glob.s8", 0);
+  g.xbdamp = t.scalar("glob.xbdamp", 0);  // src/halogen.rs:68-69
+  g.xbrad = t.scalar("glob.xbrad", 0);
   if (std::fabs(t.scalar("glob.s9", 0.0)) > 1e-15) {
     err = "D3 three-body term (s9 != 0) is outside the device path";
     return false;
   }
   const double cns = t.scalar("glob.cns", 0.6), cnp = t.scalar("glob.cnp", -0.3);
+  const double cnd1 = t.scalar("glob.cnd1", -0.5), cnd2 = t.scalar("glob.cnd2", 0.5);
   auto refocc = t.get("refocc");
   auto radius = t.get("atomic_radius_ang");
   auto covrad = t.get("covrad_ang");
@@ -445,20 +448,21 @@ bool build_elements(gfn1_engine* eng, const Tables& t, std::string& err) {
     const int nsh = (int)ao->size() / 2;
     bool ok = nsh <= kMaxShAtom;
     for (int k = 0; k < nsh && ok; ++k)
-      if ((int)(*ao)[2 * k + 1] > 1) ok = false;  // device path: s and p shells
+      if ((int)(*ao)[2 * k + 1] > 2) ok = false;  // device path: s, p and d shells
     if (!ok) continue;
     ElemTable& e = eng->elem[z];
     e.nsh = nsh;
     const double gam = t.scalar(p + "gam", 0.0);
-    const double lpar[2] = {t.scalar(p + "lpars", 0.0), t.scalar(p + "lparp", 0.0)};
-    const double poly[2] = {t.scalar(p + "polys", 0.0), t.scalar(p + "polyp", 0.0)};
-    bool seen[2] = {false, false};
-    std::vector<Prim> ref[2];
+    const double lpar[3] = {t.scalar(p + "lpars", 0.0), t.scalar(p + "lparp", 0.0), t.scalar(p + "lpard", 0.0)};
+    const double poly[3] = {t.scalar(p + "polys", 0.0), t.scalar(p + "polyp", 0.0), t.scalar(p + "polyd", 0.0)};
+    bool seen[3] = {false, false, false};
+    std::vector<Prim> ref[3];
     int nao = 0;
     for (int k = 0; k < nsh; ++k) {
       const int n = (int)(*ao)[2 * k], l = (int)(*ao)[2 * k + 1];
       const bool valence = !seen[l];
-      const int np = (z <= 2) ? (l == 0 ? (n == 1 ? 4 : 3) : 3) : 6;
+      // src/basis.rs:251-279: d shells take 4 primitives
+      const int np = (z <= 2) ? (l == 0 ? (n == 1 ? 4 : 3) : (l == 1 ? 3 : 4)) : (l <= 1 ? 6 : 4);
       std::vector<Prim> prims;
       if (!sto_ng(t, np, n, l, (*ex)[k], prims)) {
         ok = false;
@@ -482,7 +486,7 @@ bool build_elements(gfn1_engine* eng, const Tables& t, std::string& err) {
       }
       e.hdiag[k] = (*lev)[k] * kEvToHartreeModel;
       const int kind = gfn1_kind(z);
-      const double f = kind == 0 ? 0.0 : (l == 0 ? cns : cnp);
+      const double f = kind == 0 ? 0.0 : (l == 0 ? cns : (l == 1 ? cnp : (kind == 1 ? cnd1 : cnd2)));
       e.kcn[k] = -(*lev)[k] * kEvToHartreeModel * f * 0.01;
       e.poly[k] = poly[l] * 0.01;
       e.refocc[k] = valence ? (*refocc)[3 * z + l] : 0.0;
@@ -498,6 +502,7 @@ bool build_elements(gfn1_engine* eng, const Tables& t, std::string& err) {
     e.gam3 = 0.1 * t.scalar(p + "gam3", 0.0);
     e.repa = t.scalar(p + "repa", 0.0);
     e.repb = t.scalar(p + "repb", 0.0);
+    e.xb = 0.1 * t.scalar(p + "cxb", 0.0);  // src/halogen.rs:775-786
     e.en = (*en)[z];
     e.rad = (*radius)[z] * kAngstromToBohr;
     e.rcov = (4.0 / 3.0) * (*covrad)[z] * kAngstromToBohr;
@@ -611,7 +616,7 @@ int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t*
       }
       if (!eng->device_ok[zz]) {
         st = std::max(st, (int)GFN1_E_UNSUPPORTED);
-        if (first_err.empty()) first_err = "element Z=" + std::to_string(zz) + " has d/f shells; outside the device path";
+        if (first_err.empty()) first_err = "element Z=" + std::to_string(zz) + " is outside the device path";
         continue;
       }
       n += eng->elem[zz].nao;
@@ -992,7 +997,7 @@ int finish(gfn1_batch* b, const gfn1_outputs* out, cudaStream_t st) {
     switch (status[first]) {
       case GFN1_E_SCC_NOT_CONVERGED: msg += "GFN1 SCC did not converge"; break;
       case GFN1_E_INVALID_INPUT: msg += "invalid input (empty molecule, electron count or non-positive-definite overlap)"; break;
-      case GFN1_E_UNSUPPORTED: msg += "element outside the device path (d/f shells)"; break;
+      case GFN1_E_UNSUPPORTED: msg += "element outside the device path (no parameters or f shells)"; break;
       case GFN1_E_MISSING_ELEMENT: msg += "missing GFN1 parameter block"; break;
       default: msg += "error " + std::to_string(status[first]);
     }
@@ -1086,7 +1091,7 @@ int gfn1_basis_size(const gfn1_engine* eng, int nat, const uint8_t* z, int32_t* 
     const int zz = z[a];
     if (zz < 1 || zz > kMaxZ) return fail(eng, GFN1_E_MISSING_ELEMENT, "missing GFN1 parameter block for Z=" + std::to_string(zz));
     if (!eng->device_ok[zz])
-      return fail(eng, GFN1_E_UNSUPPORTED, "element Z=" + std::to_string(zz) + " has d/f shells; outside the device path");
+      return fail(eng, GFN1_E_UNSUPPORTED, "element Z=" + std::to_string(zz) + " is outside the device path");
     n += eng->elem[zz].nao;
     s += eng->elem[zz].nsh;
   }
@@ -1376,7 +1381,7 @@ extern "C" int gfn1_run_noalloc(gfn1_engine* eng, int nat, const uint8_t* z, con
     const int zz = z[a];
     if (zz < 1 || zz > kMaxZ) return fail(eng, GFN1_E_MISSING_ELEMENT, "missing GFN1 parameter block for Z=" + std::to_string(zz));
     if (!eng->device_ok[zz])
-      return fail(eng, GFN1_E_UNSUPPORTED, "element Z=" + std::to_string(zz) + " has d/f shells; outside the device path");
+      return fail(eng, GFN1_E_UNSUPPORTED, "element Z=" + std::to_string(zz) + " is outside the device path");
     n += eng->elem[zz].nao;
     nsh += eng->elem[zz].nsh;
     nref += eng->refocc_total[zz];

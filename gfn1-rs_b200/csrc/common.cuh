@@ -37,7 +37,7 @@ constexpr int kGradThreads = 128;
 constexpr int kGradMinBlocks = 4;
 
 // Per-element data, indexed by Z.  nsh == 0 marks an element the device path
-// does not support (d/f shells).  Values are already converted to the model
+// does not support (f shells, more than three shells).  Values are already converted to the model
 // units (Hartree, bohr) with the reference's conventions.
 struct ElemTable {
   int nsh, nao;
@@ -49,6 +49,7 @@ struct ElemTable {
   double refocc[kMaxShAtom];  // reference occupation of the shell
   double hard[kMaxShAtom];    // shell hardness
   double gam3, repa, repb, en, rad, rcov, r4r2;
+  double xb;                  // halogen-bond strength 0.1 CXB (0 without an entry)
   int d3_nref;
   double d3_cnref[kMaxRef];
 };
@@ -57,6 +58,7 @@ struct ElemTable {
 struct Globals {
   double ks, kp, kd, ksp, kdiff, enscale, kexp, kexplight;
   double a1, a2, s6, s8;
+  double xbdamp, xbrad;  // halogen-bond damping and radius scaling
 };
 
 // SCC options (plain-path subset of ElectronicOptions, src/electronic.rs:157-453).

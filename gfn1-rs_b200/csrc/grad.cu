@@ -32,8 +32,8 @@ __device__ __forceinline__ void grad_shell_pair(const ElemTable& eb, int kb, con
                                                 int mu0, int nu0, const double (&xs)[5], const double (&rv)[3],
                                                 double (&gmu)[3], double& dcmu, double& dcnu) {
   double Sb[2 * LB + 1][2 * LA + 1], dA[2 * LB + 1][2 * LA + 1][3];
-  overlap_block_t<LB, LA, true>(eb.nprim[kb], eb.alpha[kb], eb.coef[kb], xb, ea.nprim[ka], ea.alpha[ka], ea.coef[ka],
-                                xa, 3, Sb, dA);
+  overlap_block_any<LB, LA, true>(eb.nprim[kb], eb.alpha[kb], eb.coef[kb], xb, ea.nprim[ka], ea.alpha[ka],
+                                  ea.coef[ka], xa, 3, Sb, dA);
   const double hij = xs[0], vsum = xs[1], dlog = xs[2];
 #pragma unroll
   for (int x = 0; x < 2 * LB + 1; ++x)
@@ -123,11 +123,16 @@ __global__ void __launch_bounds__(kGradThreads, kGradMinBlocks) grad_kernel(Batc
           if (fabs(poly) > 1e-18) dlog = (fi * ea.poly[ka] + fj * eb.poly[kb]) * 0.5 * rr / r2 / poly;
           const int mu0 = atom_ao[b] + eb.ao_first[kb], nu0 = atom_ao[a] + ea.ao_first[ka];
           const double xs[5] = {hij, vmu + vnu, dlog, -eb.kcn[kb] * hs, -ea.kcn[ka] * hs};
-          switch (eb.l[kb] * 2 + ea.l[ka]) {  // s/p shells only on the device path
+          switch (eb.l[kb] * 3 + ea.l[ka]) {
             case 0: grad_shell_pair<0, 0>(eb, kb, &xyz[3 * b], ea, ka, &xyz[3 * a], P, W, N, mu0, nu0, xs, rv, gmu, dcmu, dcnu); break;
             case 1: grad_shell_pair<0, 1>(eb, kb, &xyz[3 * b], ea, ka, &xyz[3 * a], P, W, N, mu0, nu0, xs, rv, gmu, dcmu, dcnu); break;
-            case 2: grad_shell_pair<1, 0>(eb, kb, &xyz[3 * b], ea, ka, &xyz[3 * a], P, W, N, mu0, nu0, xs, rv, gmu, dcmu, dcnu); break;
-            default: grad_shell_pair<1, 1>(eb, kb, &xyz[3 * b], ea, ka, &xyz[3 * a], P, W, N, mu0, nu0, xs, rv, gmu, dcmu, dcnu); break;
+            case 2: grad_shell_pair<0, 2>(eb, kb, &xyz[3 * b], ea, ka, &xyz[3 * a], P, W, N, mu0, nu0, xs, rv, gmu, dcmu, dcnu); break;
+            case 3: grad_shell_pair<1, 0>(eb, kb, &xyz[3 * b], ea, ka, &xyz[3 * a], P, W, N, mu0, nu0, xs, rv, gmu, dcmu, dcnu); break;
+            case 4: grad_shell_pair<1, 1>(eb, kb, &xyz[3 * b], ea, ka, &xyz[3 * a], P, W, N, mu0, nu0, xs, rv, gmu, dcmu, dcnu); break;
+            case 5: grad_shell_pair<1, 2>(eb, kb, &xyz[3 * b], ea, ka, &xyz[3 * a], P, W, N, mu0, nu0, xs, rv, gmu, dcmu, dcnu); break;
+            case 6: grad_shell_pair<2, 0>(eb, kb, &xyz[3 * b], ea, ka, &xyz[3 * a], P, W, N, mu0, nu0, xs, rv, gmu, dcmu, dcnu); break;
+            case 7: grad_shell_pair<2, 1>(eb, kb, &xyz[3 * b], ea, ka, &xyz[3 * a], P, W, N, mu0, nu0, xs, rv, gmu, dcmu, dcnu); break;
+            default: grad_shell_pair<2, 2>(eb, kb, &xyz[3 * b], ea, ka, &xyz[3 * a], P, W, N, mu0, nu0, xs, rv, gmu, dcmu, dcnu); break;
           }
         }
       }

@@ -1061,8 +1061,8 @@ __device__ void stage_results(const Batch& B, const MolCtx& c, CtaWs& w, int ite
   const int m = c.m, sh0 = c.sh0;
   if (tid == 0) {
     double* t = B.terms + (long long)m * kTerms;
-    const double erep = t[2], edisp = t[7];
-    const double total_internal = e_el + e2 + e3 + erep + edisp;
+    const double erep = t[2], edisp = t[7], ehal = t[8];
+    const double total_internal = e_el + e2 + e3 + erep + edisp + ehal;
     t[0] = total_internal + ts;
     t[1] = total_internal;
     t[3] = e_el;

@@ -11,7 +11,8 @@
 //  * the shell-resolved Klopman-Ohno matrix (src/coulomb.rs:82-107);
 //  * repulsion energy and gradient (src/repulsion.rs:39-59, :139-159);
 //  * D3(BJ) two-body energy and gradient with its CN chain
-//    (src/dispersion.rs:1232-1360, :1629-1692, :1753-1787).
+//    (src/dispersion.rs:1232-1360, :1629-1692, :1753-1787);
+//  * the halogen-bond correction, energy and gradient (src/halogen.rs:64-160).
 //
 // Per-atom sums run one thread per atom over all partners in a fixed order, so
 // the results are bitwise reproducible (no floating-point atomics).
@@ -38,8 +39,8 @@ __device__ __forceinline__ void shell_pair_sh0(const ElemTable& ea, int ka, cons
   double Sb[2 * LA + 1][2 * LB + 1];
   double dummy[2 * LA + 1][2 * LB + 1][3];
   if (!zero)
-    overlap_block_t<LA, LB, false>(ea.nprim[ka], ea.alpha[ka], ea.coef[ka], xa, eb.nprim[kb], eb.alpha[kb], eb.coef[kb],
-                                   xb, 2, Sb, dummy);
+    overlap_block_any<LA, LB, false>(ea.nprim[ka], ea.alpha[ka], ea.coef[ka], xa, eb.nprim[kb], eb.alpha[kb],
+                                     eb.coef[kb], xb, 2, Sb, dummy);
 #pragma unroll
   for (int x = 0; x < 2 * LA + 1; ++x)
 #pragma unroll
@@ -54,7 +55,76 @@ __device__ __forceinline__ void shell_pair_sh0(const ElemTable& ea, int ka, cons
     }
 }
 
-__global__ void __launch_bounds__(256) setup_kernel(Batch B, Model M, int enable_dispersion, int max_nsh) {
+// Halogen-bond energy of one molecule; adds its gradient to gc [nat*3].  For
+// each donor X with strength c = 0.1 CXB, K is the nearest other atom within
+// 20 bohr and every acceptor J (N, O, P, S) within 20 bohr contributes
+//   E = c b^6 (u^2 - xbdamp u) / (1 + u^2),  b = 1/2 - T/4,  u = (r0 / r_JX)^6,
+// T = (r_KX^2 + r_JX^2 - r_JK^2) / (r_KX r_JX), r0 = xbrad (R_X + R_J), with the
+// reference's +1e-18 on r_JX and r_KX.  The gradient is taken through the
+// three squared distances.
+__device__ double halogen_term(const Model& M, const int* zs, const double* xyz, int nat, double* gc) {
+  const double cut2 = 400.0, eps = 1e-18;
+  const double damp = M.g.xbdamp, rscale = M.g.xbrad;
+  double e = 0.0;
+  for (int x = 0; x < nat; ++x) {
+    const int zx = zs[x];
+    const double c = M.elem[zx].xb;
+    if (c == 0.0 || !(zx == 17 || zx == 35 || zx == 53 || zx == 85)) continue;
+    int k = -1;  // nearest other atom inside the cutoff (first of equals)
+    double kr2 = 0.0;
+    for (int j = 0; j < nat; ++j) {
+      if (j == x) continue;
+      const double dx = xyz[3 * j] - xyz[3 * x], dy = xyz[3 * j + 1] - xyz[3 * x + 1], dz = xyz[3 * j + 2] - xyz[3 * x + 2];
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      if (r2 <= 1e-24 || r2 > cut2) continue;
+      if (k < 0 || r2 < kr2) {
+        k = j;
+        kr2 = r2;
+      }
+    }
+    if (k < 0) continue;
+    for (int j = 0; j < nat; ++j) {
+      const int zj = zs[j];
+      if (j == x || !(zj == 7 || zj == 8 || zj == 15 || zj == 16)) continue;
+      double vjx[3], vkx[3], vjk[3];
+      for (int q = 0; q < 3; ++q) {
+        vjx[q] = xyz[3 * j + q] - xyz[3 * x + q];
+        vkx[q] = xyz[3 * k + q] - xyz[3 * x + q];
+        vjk[q] = xyz[3 * j + q] - xyz[3 * k + q];
+      }
+      const double djx = vjx[0] * vjx[0] + vjx[1] * vjx[1] + vjx[2] * vjx[2];
+      const double dkx = vkx[0] * vkx[0] + vkx[1] * vkx[1] + vkx[2] * vkx[2];
+      const double djk = vjk[0] * vjk[0] + vjk[1] * vjk[1] + vjk[2] * vjk[2];
+      if (djx <= 1e-24 || djx > cut2 || djx <= eps || dkx <= eps) continue;
+      const double rjx = sqrt(djx) + eps, rkx = sqrt(dkx) + eps;
+      const double xy = sqrt(dkx * djx);
+      if (xy <= eps) continue;
+      const double T = (dkx + djx - djk) / xy;
+      const double b = 0.5 - 0.25 * T;
+      const double b2 = b * b, b5 = b2 * b2 * b, b6 = b5 * b;
+      const double r0 = rscale * (M.elem[zx].rad + M.elem[zj].rad);
+      const double t1 = r0 / rjx, t3 = t1 * t1 * t1, u = t3 * t3;
+      const double num = u * u - damp * u, den = 1.0 + u * u;
+      const double L = num / den;
+      e += c * b6 * L;
+      const double dL = (6.0 * u * (damp - 2.0 * u) / den + 12.0 * u * u * num / (den * den)) / rjx;
+      const double dET = -1.5 * c * b5 * L;  // dE/dT
+      const double gjx = dET * (1.0 / (rkx * rjx) - 0.5 * T / (rjx * rjx)) + 0.5 * c * b6 * dL / rjx;
+      const double gkx = dET * (1.0 / (rkx * rjx) - 0.5 * T / (rkx * rkx));
+      const double gjk = -dET / xy;
+      for (int q = 0; q < 3; ++q) {
+        gc[3 * j + q] += 2.0 * (gjx * vjx[q] + gjk * vjk[q]);
+        gc[3 * x + q] -= 2.0 * (gjx * vjx[q] + gkx * vkx[q]);
+        gc[3 * k + q] += 2.0 * (gkx * vkx[q] - gjk * vjk[q]);
+      }
+    }
+  }
+  return e;
+}
+
+// Two CTAs per SM (128 registers): the s/p pairs fit, pairs with a d shell
+// (rare) keep part of their blocks in local memory.
+__global__ void __launch_bounds__(256, 2) setup_kernel(Batch B, Model M, int enable_dispersion, int max_nsh) {
   extern __shared__ double smem[];
   const int m = blockIdx.x;
   if (B.status[m] != kOk) return;  // rejected by the host-side validation
@@ -156,11 +226,16 @@ __global__ void __launch_bounds__(256) setup_kernel(Batch B, Model M, int enable
         hij = 0.5 * (sei + sej) * hscale(M, za, ka, zb, kb) * poly;
       }
     }
-    switch (la * 2 + lb) {  // s/p shells only on the device path
+    switch (la * 3 + lb) {
       case 0: shell_pair_sh0<0, 0>(ea, ka, &xyz[3 * a], eb, kb, &xyz[3 * b], zero, hij, S, H0, N, mu0, nu0); break;
       case 1: shell_pair_sh0<0, 1>(ea, ka, &xyz[3 * a], eb, kb, &xyz[3 * b], zero, hij, S, H0, N, mu0, nu0); break;
-      case 2: shell_pair_sh0<1, 0>(ea, ka, &xyz[3 * a], eb, kb, &xyz[3 * b], zero, hij, S, H0, N, mu0, nu0); break;
-      default: shell_pair_sh0<1, 1>(ea, ka, &xyz[3 * a], eb, kb, &xyz[3 * b], zero, hij, S, H0, N, mu0, nu0); break;
+      case 2: shell_pair_sh0<0, 2>(ea, ka, &xyz[3 * a], eb, kb, &xyz[3 * b], zero, hij, S, H0, N, mu0, nu0); break;
+      case 3: shell_pair_sh0<1, 0>(ea, ka, &xyz[3 * a], eb, kb, &xyz[3 * b], zero, hij, S, H0, N, mu0, nu0); break;
+      case 4: shell_pair_sh0<1, 1>(ea, ka, &xyz[3 * a], eb, kb, &xyz[3 * b], zero, hij, S, H0, N, mu0, nu0); break;
+      case 5: shell_pair_sh0<1, 2>(ea, ka, &xyz[3 * a], eb, kb, &xyz[3 * b], zero, hij, S, H0, N, mu0, nu0); break;
+      case 6: shell_pair_sh0<2, 0>(ea, ka, &xyz[3 * a], eb, kb, &xyz[3 * b], zero, hij, S, H0, N, mu0, nu0); break;
+      case 7: shell_pair_sh0<2, 1>(ea, ka, &xyz[3 * a], eb, kb, &xyz[3 * b], zero, hij, S, H0, N, mu0, nu0); break;
+      default: shell_pair_sh0<2, 2>(ea, ka, &xyz[3 * a], eb, kb, &xyz[3 * b], zero, hij, S, H0, N, mu0, nu0); break;
     }
   }
 
@@ -308,11 +383,17 @@ __global__ void __launch_bounds__(256) setup_kernel(Batch B, Model M, int enable
     }
     edisp = block_sum(edisp, red);
   }
+  // ---- halogen bonds (src/halogen.rs:64-160, triples :716-786).  Donors
+  // (Cl, Br, I, At with a CXB entry) are rare, so one thread sums every triple
+  // in atom order and adds the gradient after the per-atom terms above.
+  __syncthreads();
   if (tid == 0) {
+    const double ehal = halogen_term(M, zs, xyz, nat, B.grad_classic + 3LL * a0);
     double* t = B.terms + (long long)m * kTerms;
     for (int k = 0; k < kTerms; ++k) t[k] = 0.0;
     t[2] = erep;
     t[7] = edisp;
+    t[8] = ehal;
   }
 }
 

@@ -29,7 +29,7 @@ enum {
   GFN1_E_DEVICE = 9,            /* CUDA error */
   GFN1_E_TIMEOUT = 10,          /* host-side wait exceeded */
   GFN1_E_NAN = 11,              /* non-finite input or result */
-  GFN1_E_UNSUPPORTED = 12       /* element outside the device path (d/f shells, halogen-bond donors) */
+  GFN1_E_UNSUPPORTED = 12       /* element outside the device path (f shells, missing data) */
 };
 
 typedef struct gfn1_engine gfn1_engine;

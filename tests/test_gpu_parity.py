@@ -108,10 +108,12 @@ def test_translation_invariance_gpu(calc, fixtures):
     assert np.max(np.abs(r0.gradient.sum(axis=0))) < 1e-9
 
 
-def test_unsupported_element_is_rejected(calc, fixtures):
-    z, x = smoke_molecule(fixtures, "phosphine")  # P carries a 3d shell
+def test_element_without_parameters_is_rejected(calc, fixtures):
+    z, x = smoke_molecule(fixtures, "water")
+    z = z.copy()
+    z[0] = 87  # the GFN1 parametrisation ends at Rn
     r = calc.calculate_flat([0, len(z)], z, x)
-    assert r.status[0] == 12
+    assert r.status[0] == 4  # MissingElement
 
 
 def test_not_converged_status_matches_oracle(calc, oracle_mod, fixtures):
