@@ -9,8 +9,8 @@ The tables are published data, not code:
 * Stewart's STO-nG expansion exponents/coefficients (J. Chem. Phys. 52, 431
   (1970)) as tabulated in gfn1-rs ``src/sto.rs:24-788``;
 * the GFN1 reference shell occupations (gfn1-rs ``src/basis.rs:446-531``), the
-  xTB atomic radii, mctc covalent radii and Pauling electronegativities
-  (gfn1-rs ``src/data_tables.rs:14-38, 165-174``);
+  xTB atomic radii, mctc covalent radii, Pauling electronegativities and
+  relative atomic masses (gfn1-rs ``src/data_tables.rs:14-174``);
 * the DFT-D3 reference coordination numbers, C6 table and <r4>/<r2> values from
   simple-dftd3 (LGPL-3.0-or-later), ``third_party/simple-dftd3/src/dftd3/
   {reference.f90,data/r4r2.f90}``.
@@ -205,7 +205,8 @@ def main(root: str) -> None:
     w(f"refocc {len(refocc)} " + " ".join(fmt(v) for v in refocc))
     for key, name in (("atomic_radius_ang", "XTB_ATOMIC_RADII_ANGSTROM"),
                       ("covrad_ang", "MCTC_COVALENT_RADII_2009_ANGSTROM"),
-                      ("pauling_en", "PAULING_EN")):
+                      ("pauling_en", "PAULING_EN"),
+                      ("atomic_mass_amu", "RELATIVE_ATOMIC_MASSES")):
         vals = _rust_array(tables, name)[: MAX_Z + 1]
         assert len(vals) == MAX_Z + 1
         w(f"{key} {len(vals)} " + " ".join(fmt(v) for v in vals))

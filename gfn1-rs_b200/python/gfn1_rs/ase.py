@@ -27,11 +27,13 @@ try:  # pragma: no cover - depends on the environment
     from ase.calculators.calculator import all_changes
     from ase.units import Bohr as _BOHR
     from ase.units import Hartree as _HARTREE
+    from ase.units import invcm as _INVCM_EV
     HAVE_ASE = True
 except ImportError:
     HAVE_ASE = False
     _HARTREE = 27.211386024367243  # ase.units.Hartree (CODATA 2014, ASE's default)
     _BOHR = 0.5291772105638411     # ase.units.Bohr (CODATA 2014)
+    _INVCM_EV = 1.239841973964072e-04  # ase.units.invcm, eV per cm^-1 (CODATA 2014)
     all_changes = ("positions", "numbers", "cell", "pbc", "initial_charges", "initial_magmoms")
 
     class _AseCalculator:  # minimal stand-in with ASE's calculate/results protocol
@@ -193,6 +195,39 @@ class GFN1RSCalculator(_AseCalculator):
         atoms = self.atoms if atoms is None else atoms
         numbers, positions = self._numbers_positions(atoms)
         return np.asarray(self.native_calculator().calculate(numbers.tolist(), positions.tolist()).dipole)
+
+    def get_hessian(self, atoms=None):
+        """Nuclear Hessian d2E/dR_a dR_b as a (3N, 3N) array in eV/Angstrom^2,
+        atom-major (reference ``ase.py:641-672``, non-periodic).  Central
+        differences of the engine's analytic gradient, all 6N displacements in
+        one batched engine call (``gfn1_rs.hessian``)."""
+        from .hessian import hessian_batch
+        from .native import ANGSTROM_TO_BOHR
+
+        atoms = self.atoms if atoms is None else atoms
+        numbers, positions = self._numbers_positions(atoms)
+        out = hessian_batch(self._batch_calc(), [0, len(numbers)], numbers, positions * ANGSTROM_TO_BOHR,
+                            charges=[float(self.parameters["charge"])])
+        if out["hessians"][0] is None:
+            raise RuntimeError(f"Hessian evaluation failed (status {int(out['status'][0])})")
+        return out["hessians"][0] * (_HARTREE / _BOHR ** 2)
+
+    def get_vibrational_frequencies(self, atoms=None):
+        """Harmonic analysis (reference ``ase.py:674-690``): ``wavenumbers`` in
+        cm^-1 (imaginary as negative), ``energies_ev`` (the same quanta in eV)
+        and ``modes`` (Cartesian normal-mode displacements, one per row)."""
+        from .hessian import hessian_batch, vibrational_analysis
+        from .native import ANGSTROM_TO_BOHR
+
+        atoms = self.atoms if atoms is None else atoms
+        numbers, positions = self._numbers_positions(atoms)
+        out = hessian_batch(self._batch_calc(), [0, len(numbers)], numbers, positions * ANGSTROM_TO_BOHR,
+                            charges=[float(self.parameters["charge"])])
+        if out["hessians"][0] is None:
+            raise RuntimeError(f"Hessian evaluation failed (status {int(out['status'][0])})")
+        vib = vibrational_analysis(out["hessians"][0], numbers)
+        vib["energies_ev"] = vib["wavenumbers"] * _INVCM_EV
+        return vib
 
 
 __all__ = ["GFN1RSCalculator", "HAVE_ASE"]
