@@ -109,3 +109,50 @@ def test_every_element_in_one_batch(calc, oracle_mod):
         assert de <= E_TOL and dg <= G_TOL and dq <= Q_TOL, (zm, de, dg, dq)
         worst = tuple(max(w, v) for w, v in zip(worst, (de, dg, dq)))
     print("worst |dE| %.2e  |dg| %.2e  |dq| %.2e" % worst)
+
+
+def test_d_elements_on_the_large_molecule_path(oracle_mod, fixtures):
+    """The same molecules through the cuSOLVER path (size threshold lowered to
+    16 AOs) agree with the one-CTA path and the oracle."""
+    from gfn1_rs import BatchCalculator
+
+    names = ["ferrocene", "phosphine"]
+    mols = [smoke_molecule(fixtures, n) for n in names]
+    rec = fixtures["halogen_tests"]["CH3Br...OH2 halogen bond"]
+    mols.append((np.array(rec["numbers"]), np.array(rec["positions_angstrom"]) * ANGSTROM_TO_BOHR))
+    off = np.concatenate([[0], np.cumsum([len(z) for z, _ in mols])]).astype(np.int32)
+    z = np.concatenate([z for z, _ in mols])
+    x = np.concatenate([x for _, x in mols])
+    old = os.environ.get("GFN1_DENSE_N")
+    os.environ["GFN1_DENSE_N"] = "16"
+    try:
+        got = BatchCalculator(**TIGHT).calculate_flat(off, z, x)
+    finally:
+        if old is None:
+            os.environ.pop("GFN1_DENSE_N", None)
+        else:
+            os.environ["GFN1_DENSE_N"] = old
+    ref = BatchCalculator(**TIGHT).calculate_flat(off, z, x)
+    assert np.all(got.status == 0) and np.all(ref.status == 0)
+    assert np.abs(got.energy - ref.energy).max() <= 1e-9
+    assert np.abs(got.gradient - ref.gradient).max() <= 1e-8
+    for m, (zm, xm) in enumerate(mols):
+        o = oracle_mod.run(zm, xm, options=oracle_mod.make_options(**TIGHT))
+        assert abs(got.energy[m] - o.energy) <= E_TOL
+        assert abs(got.terms[m, 8] - o.terms["halogen"]) <= 1e-12
+
+
+def test_learned_guess_with_other_elements():
+    """Molecules with elements outside the guess network's H/C/N/O start from
+    zero charges; the rest of the batch keeps the learned guess, and every
+    molecule converges to the plain run's energy."""
+    from gfn1_rs import BatchCalculator
+
+    mols = periodic_table_set(seed=11)
+    off = np.concatenate([[0], np.cumsum([len(z) for z, _ in mols])]).astype(np.int32)
+    z = np.concatenate([z for z, _ in mols])
+    x = np.concatenate([x for _, x in mols])
+    plain = BatchCalculator(**TIGHT).calculate_flat(off, z, x)
+    learned = BatchCalculator(learned_guess=True, **TIGHT).calculate_flat(off, z, x)
+    assert np.all(plain.status == 0) and np.all(learned.status == 0)
+    assert np.abs(plain.energy - learned.energy).max() <= 1e-6
