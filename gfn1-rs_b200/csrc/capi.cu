@@ -290,7 +290,7 @@ struct gfn1_batch {
   BlobLayout lay;
   HostBuf h_in, h_out;               // pinned staging
   DevBuf<unsigned char> d_in, d_out; // device blobs
-  DevBuf<double> S, H0, P, W, ws, gam, pairbuf, cn, shell_pot, se, grad_classic;
+  DevBuf<double> S, H0, P, W, ws, gam, pairbuf, cn, shell_pot, se, grad_classic, orb_eps, orb_occ;
   DevBuf<int> queue;
   DevBuf<unsigned long long> stage;
   template <class T>
@@ -340,6 +340,8 @@ struct gfn1_batch {
     B.fermi = dout<double>(lay.fermi);
     B.iterations = dout<int>(lay.iterations);
     B.status = dout<int>(lay.status);
+    B.orb_eps = orb_eps.p;
+    B.orb_occ = orb_occ.p;
     B.queue = queue.p;
     B.failed = failed.p;
     B.stage_cycles = profiling ? stage.p : nullptr;
@@ -350,7 +352,8 @@ struct gfn1_batch {
     h_out.release();
     d_in.release();
     d_out.release();
-    for (DevBuf<double>* d : {&S, &H0, &P, &W, &ws, &gam, &pairbuf, &cn, &shell_pot, &se, &grad_classic}) d->release();
+    for (DevBuf<double>* d : {&S, &H0, &P, &W, &ws, &gam, &pairbuf, &cn, &shell_pot, &se, &grad_classic, &orb_eps, &orb_occ})
+      d->release();
     queue.release();
     stage.release();
     failed.release();
@@ -802,7 +805,8 @@ int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t*
             b->stage.ensure(kStages) && b->S.ensure(mat_total) && b->H0.ensure(mat_total) && b->P.ensure(mat_total) &&
             b->W.ensure(mat_total) && b->ws.ensure((size_t)std::max<long long>(ws_total, 1)) && b->gam.ensure(gam_total) &&
             b->pairbuf.ensure(8 * std::max<long long>(pair_total, 1)) && b->cn.ensure(natoms) &&
-            b->shell_pot.ensure(nshells) && b->se.ensure(nshells) && b->grad_classic.ensure(3 * natoms);
+            b->shell_pot.ensure(nshells) && b->se.ensure(nshells) && b->grad_classic.ensure(3 * natoms) &&
+            b->orb_eps.ensure(std::max<long long>(naos, 1)) && b->orb_occ.ensure(std::max<long long>(naos, 1));
   if (!ok) return fail(eng, GFN1_E_DEVICE, "device allocation failed for the batch workspace");
   if (!b->dense_ids.empty()) {
     DenseWork& dw = b->dw;
@@ -1260,6 +1264,49 @@ int gfn1_batch_energy_gradient(gfn1_engine* eng, int nmol, const int32_t* atom_o
   for (int s = 0; s < 3; ++s)
     if ((rc = launch_stage(b, s, st)) != GFN1_OK) return rc;
   return finish(b, out, st);
+}
+
+// S, H0, P, W (N x N, row-major) and the orbital energies / occupations (N)
+// of molecule m from the batch's device buffers; every pointer may be null.
+static int copy_molecule_matrices(gfn1_batch* b, int m, double* S, double* H0, double* P, double* W, double* eps,
+                                  double* occ) {
+  gfn1_engine* eng = b->eng;
+  if (m < 0 || m >= b->nmol) return fail(eng, GFN1_E_INVALID_INPUT, "molecule index out of range");
+  const int* h_ao = b->hin<int>(b->lay.ao_off);
+  const long long* h_mat = b->hin<long long>(b->lay.mat_off);
+  const size_t n = (size_t)(h_ao[m + 1] - h_ao[m]);
+  struct Part {
+    double* dst;
+    const double* src;
+    size_t count;
+  } parts[6] = {{S, b->S.p + h_mat[m], n * n},       {H0, b->H0.p + h_mat[m], n * n},
+                {P, b->P.p + h_mat[m], n * n},       {W, b->W.p + h_mat[m], n * n},
+                {eps, b->orb_eps.p + h_ao[m], n},    {occ, b->orb_occ.p + h_ao[m], n}};
+  for (const Part& q : parts) {
+    if (!q.dst || q.count == 0) continue;
+    cudaError_t e = cudaMemcpy(q.dst, q.src, sizeof(double) * q.count, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(eng, e, "matrix copy");
+  }
+  return GFN1_OK;
+}
+
+int gfn1_last_molecule_matrices(gfn1_engine* eng, int m, double* S, double* H0, double* P, double* W, double* eps,
+                                double* occ) {
+  if (!eng) return fail(nullptr, GFN1_E_INVALID_INPUT, "null engine");
+  if (!eng->oneshot || eng->oneshot->nmol < 1) return fail(eng, GFN1_E_INVALID_INPUT, "no calculation on this engine");
+  cudaSetDevice(eng->device);
+  cudaError_t e = cudaStreamSynchronize(eng->stream);
+  if (e != cudaSuccess) return cuda_fail(eng, e, "stream synchronise");
+  return copy_molecule_matrices(eng->oneshot, m, S, H0, P, W, eps, occ);
+}
+
+int gfn1_batch_molecule_matrices(gfn1_batch* b, int m, double* S, double* H0, double* P, double* W, double* eps,
+                                 double* occ) {
+  if (!b) return fail(nullptr, GFN1_E_INVALID_INPUT, "null batch");
+  cudaSetDevice(b->eng->device);
+  cudaError_t e = cudaDeviceSynchronize();  // launches may be on any of the caller's streams
+  if (e != cudaSuccess) return cuda_fail(b->eng, e, "device synchronise");
+  return copy_molecule_matrices(b, m, S, H0, P, W, eps, occ);
 }
 
 int gfn1_run(gfn1_engine* eng, int nat, const uint8_t* z, const double* xyz_bohr, double charge,

@@ -132,6 +132,8 @@ struct Batch {
   double* fermi;            // [nmol]
   int* iterations;          // [nmol]
   int* status;              // [nmol]
+  double* orb_eps;          // [naos] orbital energies of the last diagonalisation (offset ao_off[m]), or null
+  double* orb_occ;          // [naos] their occupations, or null
   int* queue;               // work counters: [0], [1] size classes, [2] fallback ladder, [3] failed count
   int* failed;              // [nmol] molecules whose first SCC attempt did not converge, or null
   unsigned long long* stage_cycles;  // [kStages] per-stage clock totals, or null

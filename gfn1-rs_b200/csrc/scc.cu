@@ -1230,6 +1230,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
   double last_e = 0.0;
   bool have_e = false;
   bool converged = false;
+  int nneed_last = nneed0;  // eigenvalues 0..nneed_last-1 and N-1 of the last diagonalisation are known
   int iter = 0;
   int nocc = 0;
   double e_el = 0.0, e2 = 0.0, e3 = 0.0, ts = 0.0, mu = 0.0, rms = 0.0;
@@ -1363,6 +1364,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     }
     mu = sh.scal[1];
     ts = sh.scal[2];
+    nneed_last = nneed;
     // number of orbitals whose occupation matters at FP64 resolution
     int nocc_loc = 0;
     for (int i = tid; i < N; i += NT)
@@ -1498,6 +1500,13 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
 
   // ---- results
   stage_results<NT>(B, mc, w, iter, converged, e_el, e2, e3, ts, mu);
+  if (B.orb_eps) {  // orbital energies (NaN where the eigensolver did not need them) and occupations
+    const int ao0 = B.ao_off[m];
+    for (int i = tid; i < N; i += NT) {
+      B.orb_eps[ao0 + i] = (i < nneed_last || i == N - 1) ? eps[i] : __longlong_as_double(0x7ff8000000000000LL);
+      B.orb_occ[ao0 + i] = occ[i];
+    }
+  }
   // density and energy-weighted density of the last diagonalisation
   // (src/linalg.rs:243-273), kept per molecule for the gradient kernel
   for (int i = wid; i < N; i += NW)
@@ -1736,6 +1745,13 @@ __global__ void __launch_bounds__(kDenseNT, 1) dense_results_kernel(Batch B, Mod
   CtaWs w = cta_ws(dw.ws, 1, dw.maxnsh, dw.cap);
   const DenseState* st = (const DenseState*)dw.state;
   stage_results<kDenseNT>(B, c, w, st->iter, st->converged != 0, st->e_el, st->e2, st->e3, st->ts, st->mu);
+  if (B.orb_eps) {  // the full spectrum from the library eigensolver
+    const int ao0 = B.ao_off[m];
+    for (int i = threadIdx.x; i < c.N; i += blockDim.x) {
+      B.orb_eps[ao0 + i] = dw.eps[i];
+      B.orb_occ[ao0 + i] = dw.occ[i];
+    }
+  }
 }
 
 // out[:, i] = scale_i * in[:, i] with scale = occ (weight 0) or occ * eps (weight 1)

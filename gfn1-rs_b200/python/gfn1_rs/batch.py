@@ -47,6 +47,18 @@ def _options(opts: dict, compute_gradient: bool) -> _lib.Options:
     return _lib.default_options(compute_gradient=int(bool(compute_gradient)), **opts)
 
 
+def _matrices(engine, off, z, m: int, call) -> dict:
+    if not 0 <= m < len(off) - 1:
+        raise IndexError(f"molecule {m} out of range")
+    nao_z = engine.element_sizes()[0]
+    n = int(np.sum(nao_z[np.asarray(z[off[m]:off[m + 1]], dtype=np.int64)]))
+    keys = ("S", "H0", "P", "W", "orbital_energies", "occupations")
+    out = {k: np.zeros((n, n)) for k in keys[:4]}
+    out.update({k: np.zeros(n) for k in keys[4:]})
+    _lib.check(call(*[_lib.ptr(out[k]) for k in keys]), engine.handle)
+    return out
+
+
 class BatchCalculator:
     def __init__(self, param_path=None, device=0, max_scc=250, energy_tolerance=1.0e-6, charge_tolerance=2.0e-5,
                  mixing=0.4, scc_broyden=True, scc_broyden_size=250, electronic_temperature=300.0,
@@ -63,6 +75,7 @@ class BatchCalculator:
                          mixing=mixing, scc_broyden=int(bool(scc_broyden)), scc_broyden_size=scc_broyden_size,
                          electronic_temperature=electronic_temperature,
                          enable_dispersion=int(bool(enable_dispersion)))
+        self._last = None  # (atom_offsets, numbers) of the last calculate_flat call
 
     def shell_offsets(self, atom_offsets, numbers) -> np.ndarray:
         """Prefix sums of the shell counts, laid out as the C side does (atoms of
@@ -106,9 +119,21 @@ class BatchCalculator:
         rc = L.gfn1_batch_energy_gradient(self.engine.handle, nmol, _lib.ptr(off, ctypes.c_int32),
                                           _lib.ptr(z, ctypes.c_uint8), _lib.ptr(xyz), _lib.ptr(ch), _lib.ptr(q0),
                                           ctypes.byref(opt), ctypes.byref(out))
+        self._last = (off, z)
         if rc != 0 and (raise_on_error or rc not in (3, 4, 8, 12)):
             _lib.check(rc, self.engine.handle)
         return BatchResult(energy, terms, grad, qsh, qat, dip, fermi, iters, status, off, shoff)
+
+    def molecule_matrices(self, m: int) -> dict:
+        """S, H0, P, W ([N, N]) and orbital energies / occupations ([N]) of
+        molecule m of the last calculate_flat call: the optional members of the
+        reference's ElectronicResult (gfn1-rs src/electronic.rs:600-612).
+        Orbital energies the eigensolver did not need are NaN."""
+        if self._last is None:
+            raise RuntimeError("no calculation on this calculator yet")
+        off, z = self._last
+        return _matrices(self.engine, off, z, m,
+                         lambda *p: _lib.load().gfn1_last_molecule_matrices(self.engine.handle, int(m), *p))
 
     def calculate(self, molecules, unit="angstrom", charges=None, compute_gradient=True, **kw) -> BatchResult:
         """molecules: iterable of (numbers, positions) in `unit`."""
@@ -140,6 +165,11 @@ class ResidentBatch:
         L.gfn1_batch_info(h, ctypes.byref(na), ctypes.byref(ns), ctypes.byref(no), ctypes.byref(nl))
         self.natoms, self.nshells, self.naos, self.launches = na.value, ns.value, no.value, nl.value
         self.compute_gradient = compute_gradient
+
+    def molecule_matrices(self, m: int) -> dict:
+        """As BatchCalculator.molecule_matrices, after this batch's last launch."""
+        return _matrices(self.calc.engine, self.atom_offsets, self.numbers, m,
+                         lambda *p: _lib.load().gfn1_batch_molecule_matrices(self.handle, int(m), *p))
 
     def close(self):
         if getattr(self, "handle", None):

@@ -99,6 +99,19 @@ int gfn1_batch_energy_gradient(gfn1_engine* eng, int nmol, const int32_t* atom_o
                                const double* xyz_bohr, const double* charge, const double* init_shell_q,
                                const gfn1_options* opt, const gfn1_outputs* out);
 
+/* Matrices and orbitals of molecule m of the last gfn1_run /
+ * gfn1_batch_energy_gradient call on this engine, the optional members of
+ * ElectronicResult (src/electronic.rs:600-612): S = integrals.overlap, H0 = h0,
+ * P = density, W = energy_weighted_density (N x N, row-major, AO order of
+ * BasisSet::build) and orbital_energies / occupations (N).  P, W, the
+ * eigenvalues and occupations are those of the last diagonalisation.  The
+ * one-SM-per-molecule path solves only for the eigenvalues its occupations
+ * need (the lowest ceil(nel/2)+8, the whole spectrum when the Fermi
+ * distribution reaches further, and the highest); the others are NaN.  Above
+ * 1024 AOs the full spectrum is returned.  Any pointer may be NULL. */
+int gfn1_last_molecule_matrices(gfn1_engine* eng, int m, double* S, double* H0, double* P, double* W, double* eps,
+                                double* occ);
+
 /* Resident-batch interface: the topology (atom counts, elements, charges) is
  * uploaded once; coordinates can then be replaced and the batch re-run with
  * inputs already on the device (molecular dynamics, benchmarking).
@@ -126,6 +139,10 @@ int gfn1_batch_stage_cycles(const gfn1_batch* b, uint64_t* cycles, int n);
 int gfn1_batch_io_bytes(const gfn1_batch* b, int64_t* h2d, int64_t* d2h);
 /* Synchronises and copies results to host buffers. */
 int gfn1_batch_download(gfn1_batch* b, const gfn1_outputs* out);
+/* As gfn1_last_molecule_matrices for molecule m of a resident batch after its
+ * last launch (waits for the device first). */
+int gfn1_batch_molecule_matrices(gfn1_batch* b, int m, double* S, double* H0, double* P, double* W, double* eps,
+                                 double* occ);
 /* Device pointers of the batch-owned result arrays (valid until destroy). */
 int gfn1_batch_outputs_device(gfn1_batch* b, gfn1_outputs* out);
 /* Sizes of the batch: natoms, nshells, total AOs; launches = kernels per run. */
