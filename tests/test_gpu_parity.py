@@ -178,3 +178,20 @@ def test_initial_guess_converges_to_same_result(calc, oracle_mod, fixtures):
     r = calc.calculate_flat([0, len(z)], z, x, initial_shell_charges=o.shell_charges, raise_on_error=True)
     assert abs(r.energy[0] - o.energy) < E_TOL
     assert r.iterations[0] <= o.iterations
+
+
+def test_charged_h2_cation_aufbau_on_gpu(calc, oracle_mod):
+    """The charged-doublet case of tests/nonpbc_smoke.rs (charge +1, T_el = 0,
+    no dispersion) through the batch API: parity with the oracle and the
+    reference's assertions on occupations and charges."""
+    x = np.array([[0.0, 0.0, 0.0], [0.74, 0.0, 0.0]]) * ANGSTROM_TO_BOHR
+    calc.opts.update(electronic_temperature=0.0, enable_dispersion=0)
+    r = calc.calculate_flat([0, 2], [1, 1], x, charges=[1.0], raise_on_error=True)
+    o = oracle_mod.run([1, 1], x, options=oracle_mod.make_options(electronic_temperature=0.0, enable_dispersion=False,
+                                                                  charge=1.0))
+    assert r.status[0] == 0
+    assert abs(r.energy[0] - o.energy) <= E_TOL
+    assert np.max(np.abs(r.gradient - o.gradient)) <= G_TOL
+    assert abs(r.atomic_charges.sum() - 1.0) < 1e-6
+    occ = calc.molecule_matrices(0)["occupations"]
+    assert abs(occ.sum() - 1.0) < 1e-10 and np.any(np.abs(occ - 1.0) < 1e-10)

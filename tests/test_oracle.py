@@ -117,3 +117,16 @@ def test_robust_ladder_recovers(oracle_mod, fixtures):
     r = oracle_mod.run(z, x, options=oracle_mod.make_options(max_scc=1), gradient=False)
     assert r.converged and r.iterations > 1
     assert abs(r.energy - ref) < 1e-6
+
+
+def test_charged_h2_cation_aufbau(oracle_mod):
+    """tests/nonpbc_smoke.rs (charged doublet H2+): charge +1, T_el = 0,
+    no dispersion; one electron, a singly occupied orbital, atomic charges
+    summing to +1."""
+    x = np.array([[0.0, 0.0, 0.0], [0.74, 0.0, 0.0]]) * ANGSTROM_TO_BOHR
+    opt = oracle_mod.make_options(electronic_temperature=0.0, enable_dispersion=False, charge=1.0)
+    r = oracle_mod.run([1, 1], x, options=opt)
+    assert r.converged
+    assert abs(r.occupations.sum() - 1.0) < 1e-10
+    assert np.any(np.abs(r.occupations - 1.0) < 1e-10)
+    assert abs(r.atomic_charges.sum() - 1.0) < 1e-6
