@@ -784,6 +784,7 @@ struct Options {
   int enable_dispersion = 1;
   double level_shift = 0.0;
   double eigen_tolerance = 1e-12;
+  int spin_multiplicity = 0;  // 0: None
 };
 
 // ---------------------------------------------------------------- Broyden
@@ -884,23 +885,26 @@ struct Broyden {
 };
 
 // ---------------------------------------------------------------- occupations
-// src/electronic.rs:3853-3921
+// src/electronic.rs:3853-3921 (cap = 2, both spins in one orbital) and the
+// one-spin channels of :3958-4045 (cap = 1): occupation cap / (1 + e^x),
+// aufbau fills of at most cap, entropy cap kT [n ln n + (1-n) ln(1-n)] with
+// n = f / cap.
 struct Occ {
   std::vector<double> f;
   double mu = 0, ts = 0;
 };
-double fermi_occ(double eps, double mu, double kt) {
+double fermi_occ(double eps, double mu, double kt, double cap = 2.0) {
   double x = std::min(80.0, std::max(-80.0, (eps - mu) / kt));
-  return 2.0 / (1.0 + std::exp(x));
+  return cap / (1.0 + std::exp(x));
 }
-Occ occupations(const std::vector<double>& eps, double nelec, double kt) {
+Occ occupations(const std::vector<double>& eps, double nelec, double kt, double cap = 2.0) {
   Occ o;
   int n = (int)eps.size();
   o.f.assign(n, 0.0);
   if (kt <= 0.0) {  // aufbau, src/electronic.rs:3830-3851
     double rem = std::max(0.0, nelec);
     for (int i = 0; i < n; ++i) {
-      double fill = std::min(rem, 2.0);
+      double fill = std::min(rem, cap);
       o.f[i] = fill;
       rem -= fill;
       if (rem <= 0.0) break;
@@ -912,14 +916,14 @@ Occ occupations(const std::vector<double>& eps, double nelec, double kt) {
     return o;
   }
   if (nelec <= 0.0) { o.mu = n ? eps[0] : 0.0; return o; }
-  if (nelec >= 2.0 * n) { o.f.assign(n, 2.0); o.mu = n ? eps[n - 1] : 0.0; return o; }
+  if (nelec >= cap * n) { o.f.assign(n, cap); o.mu = n ? eps[n - 1] : 0.0; return o; }
   double mn = *std::min_element(eps.begin(), eps.end());
   double mx = *std::max_element(eps.begin(), eps.end());
   double lo = mn - 100.0 * kt - 10.0, hi = mx + 100.0 * kt + 10.0;
   for (int it = 0; it < 200; ++it) {
     double mu = 0.5 * (lo + hi);
     double sum = 0.0;
-    for (double e : eps) sum += fermi_occ(e, mu, kt);
+    for (double e : eps) sum += fermi_occ(e, mu, kt, cap);
     double nlo = lo, nhi = hi;
     if (sum < nelec) nlo = mu; else nhi = mu;
     if (nlo == lo && nhi == hi) break;
@@ -929,10 +933,45 @@ Occ occupations(const std::vector<double>& eps, double nelec, double kt) {
   o.mu = 0.5 * (lo + hi);
   o.ts = 0.0;
   for (int i = 0; i < n; ++i) {
-    o.f[i] = fermi_occ(eps[i], o.mu, kt);
-    double nn = std::min(1.0 - 1e-16, std::max(1e-16, 0.5 * o.f[i]));
-    o.ts += 2.0 * kt * (nn * std::log(nn) + (1.0 - nn) * std::log(1.0 - nn));
+    o.f[i] = fermi_occ(eps[i], o.mu, kt, cap);
+    double nn = std::min(1.0 - 1e-16, std::max(1e-16, o.f[i] / cap));
+    o.ts += cap * kt * (nn * std::log(nn) + (1.0 - nn) * std::log(1.0 - nn));
   }
+  return o;
+}
+
+// src/electronic.rs:545-598: alpha and beta electron counts of a requested
+// spin multiplicity (0 = none), with the reference's checks.
+struct SpinChannels {
+  bool on = false;
+  double alpha = 0, beta = 0;
+};
+SpinChannels resolve_spin_channels(double nelec, int mult, int norb) {
+  SpinChannels c;
+  if (mult == 0) return c;
+  if (mult < 1) throw OracleError(E_INVALID_INPUT, "spin multiplicity must be at least 1");
+  const double rounded = std::round(nelec);
+  if (std::fabs(nelec - rounded) > 1e-8)
+    throw OracleError(E_INVALID_INPUT, "spin multiplicity requires an integer electron count");
+  const long long ne = (long long)rounded, unpaired = mult - 1;
+  if (unpaired > ne) throw OracleError(E_INVALID_INPUT, "spin multiplicity needs more unpaired electrons than the system has");
+  if ((ne - unpaired) % 2 != 0) throw OracleError(E_INVALID_INPUT, "spin multiplicity is incompatible with the electron count");
+  const long long a = (ne + unpaired) / 2, b = (ne - unpaired) / 2;
+  if (a > norb || b > norb) throw OracleError(E_INVALID_INPUT, "spin multiplicity needs more orbitals than the basis has");
+  c.on = true;
+  c.alpha = (double)a;
+  c.beta = (double)b;
+  return c;
+}
+
+// src/electronic.rs:3930-3956: each spin channel filled on its own.
+Occ spin_constrained_occupations(const std::vector<double>& eps, const SpinChannels& c, double kt) {
+  Occ a = occupations(eps, c.alpha, kt, 1.0), b = occupations(eps, c.beta, kt, 1.0);
+  Occ o;
+  o.f.resize(eps.size());
+  for (size_t i = 0; i < eps.size(); ++i) o.f[i] = a.f[i] + b.f[i];
+  o.mu = 0.5 * (a.mu + b.mu);
+  o.ts = a.ts + b.ts;
   return o;
 }
 
@@ -1271,6 +1310,7 @@ Result run(const System& sys, const Options& opt, const double* init_q, bool wan
   if (nelec < -1e-8) throw OracleError(E_INVALID_INPUT, "electron count is negative");
   if (nelec > 2.0 * n + 1e-8) throw OracleError(E_INVALID_INPUT, "electron count exceeds basis capacity");
   res.nelec = nelec;
+  const SpinChannels spin = resolve_spin_channels(nelec, opt.spin_multiplicity, n);
   Mat A = coulomb_matrix(sys, b);
   // Lowdin orthogonaliser (src/linalg.rs:193-217)
   std::vector<double> sw;
@@ -1327,7 +1367,7 @@ Result run(const System& sys, const Options& opt, const double* init_q, bool wan
     sym_eig(Fo, st.eps, V);
     Mat C = matmul(X, V);
     double kt = std::max(0.0, etemp) * KB_HARTREE_PER_K;
-    Occ o = occupations(st.eps, nelec, kt);
+    Occ o = spin.on ? spin_constrained_occupations(st.eps, spin, kt) : occupations(st.eps, nelec, kt);
     st.f = o.f;
     st.mu = o.mu;
     st.ts = o.ts;
@@ -1560,6 +1600,7 @@ struct oracle_options {
   int enable_dispersion;
   double charge;
   double level_shift;
+  int spin_multiplicity;  // 0: none
 };
 
 const char* oracle_last_error() { return t_err.c_str(); }
@@ -1587,6 +1628,7 @@ static Options to_opts(const oracle_options* o) {
     opt.electronic_temperature = o->electronic_temperature;
     opt.enable_dispersion = o->enable_dispersion;
     opt.level_shift = o->level_shift;
+    opt.spin_multiplicity = o->spin_multiplicity;
   }
   return opt;
 }

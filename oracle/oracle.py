@@ -38,16 +38,19 @@ class OracleOptions(ctypes.Structure):
         ("enable_dispersion", ctypes.c_int),
         ("charge", ctypes.c_double),
         ("level_shift", ctypes.c_double),
+        ("spin_multiplicity", ctypes.c_int),
     ]
 
 
 def make_options(max_scc=250, energy_tolerance=1e-6, charge_tolerance=2e-5, mixing=0.4,
                  scc_broyden=True, scc_broyden_size=250, electronic_temperature=300.0,
-                 enable_dispersion=True, charge=0.0, level_shift=0.0) -> OracleOptions:
-    """Defaults of ``ElectronicOptions::default`` (src/electronic.rs:395-452)."""
+                 enable_dispersion=True, charge=0.0, level_shift=0.0, spin_multiplicity=None) -> OracleOptions:
+    """Defaults of ``ElectronicOptions::default`` (src/electronic.rs:395-452);
+    spin_multiplicity None is the reference's None."""
     return OracleOptions(int(max_scc), float(energy_tolerance), float(charge_tolerance), float(mixing),
                          int(bool(scc_broyden)), int(scc_broyden_size), float(electronic_temperature),
-                         int(bool(enable_dispersion)), float(charge), float(level_shift))
+                         int(bool(enable_dispersion)), float(charge), float(level_shift),
+                         int(spin_multiplicity or 0))
 
 
 class OracleError(RuntimeError):

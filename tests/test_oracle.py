@@ -130,3 +130,50 @@ def test_charged_h2_cation_aufbau(oracle_mod):
     assert abs(r.occupations.sum() - 1.0) < 1e-10
     assert np.any(np.abs(r.occupations - 1.0) < 1e-10)
     assert abs(r.atomic_charges.sum() - 1.0) < 1e-6
+
+
+def test_spin_multiplicity_triplet_o2(oracle_mod):
+    """Spin-constrained occupations (src/electronic.rs:3930-4045, tests at
+    :4173-4183): O2 as a triplet at T_el = 0 has two singly occupied orbitals;
+    the same count with the wrong parity is rejected as incompatible."""
+    x = np.array([[0.0, 0.0, 0.0], [0.0, 0.0, 1.21]]) * ANGSTROM_TO_BOHR
+    opt = oracle_mod.make_options(electronic_temperature=0.0, spin_multiplicity=3)
+    r = oracle_mod.run([8, 8], x, options=opt)
+    assert r.converged
+    assert int(np.sum(np.abs(r.occupations - 1.0) < 1e-10)) == 2
+    assert abs(r.occupations.sum() - 12.0) < 1e-10
+    with pytest.raises(oracle_mod.OracleError) as ei:
+        oracle_mod.run([8, 8], x, options=oracle_mod.make_options(spin_multiplicity=2))
+    assert ei.value.code == 3 and "incompatible" in str(ei.value)
+    # multiplicity 1 is the closed-shell filling: the same result as no multiplicity
+    a = oracle_mod.run([8, 8], x, options=oracle_mod.make_options(spin_multiplicity=1))
+    b = oracle_mod.run([8, 8], x)
+    assert abs(a.energy - b.energy) < 1e-10
+
+
+def test_spin_multiplicity_doublet_h2_cation(oracle_mod):
+    """tests/nonpbc_smoke.rs charged doublet with spin_multiplicity = 2."""
+    x = np.array([[0.0, 0.0, 0.0], [0.74, 0.0, 0.0]]) * ANGSTROM_TO_BOHR
+    opt = oracle_mod.make_options(electronic_temperature=0.0, enable_dispersion=False, charge=1.0,
+                                  spin_multiplicity=2)
+    r = oracle_mod.run([1, 1], x, options=opt)
+    assert r.converged
+    assert abs(r.occupations.sum() - 1.0) < 1e-10
+    assert np.any(np.abs(r.occupations - 1.0) < 1e-10)
+    assert abs(r.atomic_charges.sum() - 1.0) < 1e-6
+
+
+def test_spin_multiplicity_gradient_is_derivative(oracle_mod):
+    """The analytic gradient stays the derivative of the free energy with
+    spin-constrained Fermi occupations (triplet CH2, 300 K)."""
+    x = np.array([[0.0, 0.0, 0.0], [0.0, 0.95, 0.55], [0.0, -0.95, 0.55]]) * ANGSTROM_TO_BOHR
+    opt = oracle_mod.make_options(energy_tolerance=1e-11, charge_tolerance=1e-9, spin_multiplicity=3)
+    r = oracle_mod.run([6, 1, 1], x, options=opt)
+    h = 1e-4
+    for a, k in ((0, 2), (1, 1), (2, 2)):
+        xp, xm = x.copy(), x.copy()
+        xp[a, k] += h
+        xm[a, k] -= h
+        fd = (oracle_mod.run([6, 1, 1], xp, options=opt, gradient=False).energy
+              - oracle_mod.run([6, 1, 1], xm, options=opt, gradient=False).energy) / (2 * h)
+        assert abs(fd - r.gradient[a, k]) < 5e-5
