@@ -275,6 +275,8 @@ struct gfn1_batch {
   gfn1_options opt;
   bool has_init_q = false;
   bool profiling = false;
+  std::string host_err;   // message of the first molecule the host validation rejected
+  int host_err_mol = -1;  // that molecule, or -1
   gfn1_guess* guess = nullptr;       // learned guess used when no initial charges are set
   DevBuf<float> gx, gy;              // guess features [natoms x 100] and outputs [natoms x 2]
   DevBuf<double> gq;                 // guessed initial shell charges [nshells]
@@ -572,6 +574,22 @@ void fill_default(gfn1_options* o) {
   o->electronic_temperature = 300.0;
   o->enable_dispersion = 1;
   o->compute_gradient = 1;
+  o->spin_multiplicity = 0;
+}
+
+// Checks of a requested spin multiplicity (resolve_spin_channels,
+// src/electronic.rs:545-598); returns an empty string when it is usable.
+std::string spin_multiplicity_error(int mult, double nelec, int norb) {
+  if (mult == 0) return "";
+  if (mult < 1) return "spin multiplicity must be at least 1";
+  const double rounded = std::round(nelec);
+  if (std::fabs(nelec - rounded) > 1e-8) return "spin multiplicity requires an integer electron count";
+  const long long ne = (long long)rounded, unpaired = mult - 1;
+  if (unpaired > ne) return "spin multiplicity needs more unpaired electrons than the system has";
+  if ((ne - unpaired) % 2 != 0) return "spin multiplicity " + std::to_string(mult) + " is incompatible with " +
+                                       std::to_string(ne) + " electrons";
+  if ((ne + unpaired) / 2 > norb) return "spin multiplicity needs more orbitals than the basis has";
+  return "";
 }
 
 }  // namespace
@@ -632,6 +650,13 @@ int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t*
       st = GFN1_E_INVALID_INPUT;
       if (first_err.empty()) first_err = "molecule " + std::to_string(m) + ": invalid electron count";
     }
+    if (st == GFN1_OK) {
+      const std::string se = spin_multiplicity_error(o.spin_multiplicity, nelec, n);
+      if (!se.empty()) {
+        st = GFN1_E_INVALID_INPUT;
+        if (first_err.empty()) first_err = "molecule " + std::to_string(m) + ": " + se;
+      }
+    }
     st_m[m] = st;
     worst = std::max(worst, st);
     nsh_m[m] = s;
@@ -647,6 +672,10 @@ int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t*
   }
   b->nshells = nshells;
   b->naos = naos;
+  b->host_err = first_err;
+  b->host_err_mol = -1;
+  for (int m = 0; m < nmol && b->host_err_mol < 0; ++m)
+    if (st_m[m] != GFN1_OK) b->host_err_mol = m;
   b->mat_total = mat_total;
   b->gam_total = gam_total;
   b->pair_total = pair_total;
@@ -905,6 +934,7 @@ int launch_stage(gfn1_batch* b, int stage, cudaStream_t st) {
     so.charge_tol = b->opt.charge_tolerance;
     so.mixing = b->opt.mixing;
     so.etemp = b->opt.electronic_temperature;
+    so.spin_mult = b->opt.spin_multiplicity;
     // fork: the small-molecule class runs on the side stream next to the large one
     if ((e = cudaEventRecord(b->ev_fork, st)) != cudaSuccess || (e = cudaStreamWaitEvent(b->side, b->ev_fork, 0)) != cudaSuccess)
       return cuda_fail(eng, e, "stream fork");
@@ -996,7 +1026,9 @@ int finish(gfn1_batch* b, const gfn1_outputs* out, cudaStream_t st) {
     if (status[m] > worst) worst = status[m];
     if (status[m] != GFN1_OK && first < 0) first = m;
   }
-  if (worst != GFN1_OK) {
+  if (worst != GFN1_OK && first == b->host_err_mol && !b->host_err.empty()) {
+    return fail(eng, worst, b->host_err);  // the host validation's own message
+  } else if (worst != GFN1_OK) {
     std::string msg = "molecule " + std::to_string(first) + ": ";
     switch (status[first]) {
       case GFN1_E_SCC_NOT_CONVERGED: msg += "GFN1 SCC did not converge"; break;
@@ -1445,6 +1477,10 @@ extern "C" int gfn1_run_noalloc(gfn1_engine* eng, int nat, const uint8_t* z, con
   const double nelec = nref - charge;
   if (!std::isfinite(nelec) || nelec < -1e-8 || nelec > 2.0 * n + 1e-8)
     return fail(eng, GFN1_E_INVALID_INPUT, "invalid electron count");
+  {
+    const std::string se = spin_multiplicity_error(o.spin_multiplicity, nelec, n);
+    if (!se.empty()) return fail(eng, GFN1_E_INVALID_INPUT, se);
+  }
   const int dev = eng->device;
   if (dev < 0 || dev >= kNaMaxDevices) return fail(eng, GFN1_E_INVALID_INPUT, "device ordinal out of range");
   cudaError_t e = cudaSetDevice(dev);
@@ -1564,6 +1600,7 @@ extern "C" int gfn1_run_noalloc(gfn1_engine* eng, int nat, const uint8_t* z, con
   so.charge_tol = o.charge_tolerance;
   so.mixing = o.mixing;
   so.etemp = o.electronic_temperature;
+  so.spin_mult = o.spin_multiplicity;
   const size_t sm_setup = sizeof(double) * (16 * (size_t)nat + 32) + sizeof(int) * (3 * (size_t)nat + 2 + 2 * (size_t)nsh);
   const size_t sm_scc = std::max(scc_smem_bytes(nsh, n, nat, 0),
                                  std::min(scc_smem_bytes(nsh, n, nat, n), scc_max_dynamic_smem(n > 96 ? 512 : 256)));

@@ -67,6 +67,7 @@ struct SccOptions {
   int broyden;       // 1 = Broyden, 0 = linear damping
   int broyden_size;  // memory
   int enable_dispersion;
+  int spin_mult;     // 0: no spin multiplicity; n >= 1: spin-constrained occupations
   double energy_tol, charge_tol, mixing, etemp;
 };
 

@@ -557,7 +557,7 @@ __device__ void eigenvalues(const double* d, const double* esq, int N, int nneed
 // between lie at or above eps[nneed-1]; while a trial mu keeps them beyond the
 // +80 kT clamp each contributes exactly 2/(1+e^80).  When a decision would need
 // them, `ambiguous` is set and the caller computes every eigenvalue.
-__device__ void fermi_warp(const double* eps, int N, int nneed, double nelec, double kt, double* occ, double& mu_out,
+__device__ void fermi_warp(const double* eps, int N, int nneed, double nelec, double kt, double cap, double* occ, double& mu_out,
                            double& ts_out, bool& ambiguous) {
   const int lane = threadIdx.x & 31;
   ambiguous = false;
@@ -566,7 +566,7 @@ __device__ void fermi_warp(const double* eps, int N, int nneed, double nelec, do
     double rem = fmax(nelec, 0.0);
     int homo = 0;
     for (int i = 0; i < N; ++i) {
-      const double fill = fmin(rem, 2.0);
+      const double fill = fmin(rem, cap);
       if (lane == 0) occ[i] = fill;
       rem -= fill;
       if (fill > 1e-12) homo = i;
@@ -576,12 +576,12 @@ __device__ void fermi_warp(const double* eps, int N, int nneed, double nelec, do
   } else if (nelec <= 0.0) {
     for (int i = lane; i < N; i += 32) occ[i] = 0.0;
     mu = eps[0];
-  } else if (nelec >= 2.0 * N) {
-    for (int i = lane; i < N; i += 32) occ[i] = 2.0;
+  } else if (nelec >= cap * N) {
+    for (int i = lane; i < N; i += 32) occ[i] = cap;
     mu = eps[N - 1];
   } else {
-    const double c80 = 2.0 / (1.0 + exp(80.0));
-    const double cm80 = 2.0 / (1.0 + exp(-80.0));
+    const double c80 = cap / (1.0 + exp(80.0));
+    const double cm80 = cap / (1.0 + exp(-80.0));
     const int nunc = (nneed < N) ? (N - 1 - nneed) : 0;
     const double etop = eps[nneed - 1];
     const double ikt = 1.0 / kt;
@@ -589,7 +589,7 @@ __device__ void fermi_warp(const double* eps, int N, int nneed, double nelec, do
       const double x = (ei - m) * ikt;
       if (x >= 80.0) return c80;
       if (x <= -80.0) return cm80;
-      return 2.0 / (1.0 + exp(x));
+      return cap / (1.0 + exp(x));
     };
     double lo = eps[0] - 100.0 * kt - 10.0, hi = eps[N - 1] + 100.0 * kt + 10.0;
     for (int it = 0; it < 200; ++it) {
@@ -620,8 +620,8 @@ __device__ void fermi_warp(const double* eps, int N, int nneed, double nelec, do
         const bool known = i < nneed || i == N - 1;
         const double f = known ? fo(eps[i], mu) : c80;
         occ[i] = f;
-        const double nn = fmin(1.0 - 1e-16, fmax(1e-16, 0.5 * f));
-        t += 2.0 * kt * (nn * log(nn) + (1.0 - nn) * log(1.0 - nn));
+        const double nn = fmin(1.0 - 1e-16, fmax(1e-16, f / cap));
+        t += cap * kt * (nn * log(nn) + (1.0 - nn) * log(1.0 - nn));
       }
       ts = warp_sum(t);
     }
@@ -641,13 +641,14 @@ __device__ void fermi_warp(const double* eps, int N, int nneed, double nelec, do
 // matter makes the result ambiguous (the caller then computes all of them).
 // Shared scratch: sh.VtV rows 0 and 1.
 template <int NT>
-__device__ void fermi_cta(const double* eps, int N, int nneed, double nelec, double kt, double* occ, SccShared& sh,
+__device__ void fermi_cta(const double* eps, int N, int nneed, double nelec, double kt, double cap, double* occ,
+                          SccShared& sh,
                           double& mu_out, double& ts_out, bool& ambiguous) {
   constexpr int NW = NT / 32;
   static_assert(NW <= 16, "one trial point per warp");
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  const double c80 = 2.0 / (1.0 + exp(80.0));
-  const double cm80 = 2.0 / (1.0 + exp(-80.0));
+  const double c80 = cap / (1.0 + exp(80.0));
+  const double cm80 = cap / (1.0 + exp(-80.0));
   const int nunc = (nneed < N) ? (N - 1 - nneed) : 0;
   const double etop = eps[nneed - 1];
   const double ikt = 1.0 / kt;
@@ -655,7 +656,7 @@ __device__ void fermi_cta(const double* eps, int N, int nneed, double nelec, dou
     const double x = (ei - m) * ikt;
     if (x >= 80.0) return c80;
     if (x <= -80.0) return cm80;
-    return 2.0 / (1.0 + exp(x));
+    return cap / (1.0 + exp(x));
   };
   double lo = eps[0] - 100.0 * kt - 10.0, hi = eps[N - 1] + 100.0 * kt + 10.0;
   bool amb = false;
@@ -699,14 +700,57 @@ __device__ void fermi_cta(const double* eps, int N, int nneed, double nelec, dou
       const bool known = i < nneed || i == N - 1;
       const double f = known ? fo(eps[i], mu) : c80;
       occ[i] = f;
-      const double nn = fmin(1.0 - 1e-16, fmax(1e-16, 0.5 * f));
-      t += 2.0 * kt * (nn * log(nn) + (1.0 - nn) * log(1.0 - nn));
+      const double nn = fmin(1.0 - 1e-16, fmax(1e-16, f / cap));
+      t += cap * kt * (nn * log(nn) + (1.0 - nn) * log(1.0 - nn));
     }
     ts = block_sum(t, sh.red);
   }
   mu_out = mu;
   ts_out = ts;
   ambiguous = amb;
+}
+
+// A requested spin multiplicity fills the alpha and beta channels on their own,
+// each orbital holding at most one electron per channel (src/electronic.rs:
+// 3930-4045): occupation = alpha + beta, mu = their mean, TS = their sum.
+// Every thread takes part; the results land in sh.scal[1] (mu), sh.scal[2]
+// (TS) and sh.iscal[2] (ambiguous); `tmp` (N doubles) holds the beta channel.
+template <int NT>
+__device__ void spin_channel_occupations(const double* eps, int N, int nneed, double nalpha, double nbeta, double kt,
+                                         double* occ, double* tmp, SccShared& sh) {
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  double fm[2], ft[2];
+  bool amb[2];
+  for (int ch = 0; ch < 2; ++ch) {
+    const double ne = ch == 0 ? nalpha : nbeta;
+    double* o = ch == 0 ? occ : tmp;
+    if (kt > 0.0 && ne > 0.0 && ne < (double)N) {
+      fermi_cta<NT>(eps, N, nneed, ne, kt, 1.0, o, sh, fm[ch], ft[ch], amb[ch]);
+    } else {
+      if (wid == 0) {
+        double m, t;
+        bool a;
+        fermi_warp(eps, N, nneed, ne, kt, 1.0, o, m, t, a);
+        if (lane == 0) {
+          sh.scal[4] = m;
+          sh.scal[5] = t;
+          sh.iscal[4] = a ? 1 : 0;
+        }
+      }
+      __syncthreads();
+      fm[ch] = sh.scal[4];
+      ft[ch] = sh.scal[5];
+      amb[ch] = sh.iscal[4] != 0;
+      __syncthreads();
+    }
+  }
+  for (int i = tid; i < N; i += NT) occ[i] += tmp[i];
+  if (tid == 0) {
+    sh.scal[1] = 0.5 * (fm[0] + fm[1]);
+    sh.scal[2] = ft[0] + ft[1];
+    sh.iscal[2] = (amb[0] || amb[1]) ? 1 : 0;
+  }
+  __syncthreads();
 }
 
 // Z := Q Z for the first ncol columns, Q = H_0 ... H_{N-3}, applied in blocks of
@@ -1225,7 +1269,11 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
   double nref = 0.0;
   for (int s = 0; s < nsh; ++s) nref += M.elem[B.z[a0 + sh_atom[s]]].refocc[sh_k[s]];
   const double nelec = nref - B.charge[m];
-  const int nneed0 = min(N, max(1, (int)ceil(0.5 * nelec) + 8));
+  // a requested spin multiplicity: alpha and beta electron counts (validated on the host)
+  const bool spin = opt.spin_mult > 0;
+  const double nalpha = spin ? 0.5 * (rint(nelec) + (opt.spin_mult - 1)) : 0.0;
+  const double nbeta = spin ? 0.5 * (rint(nelec) - (opt.spin_mult - 1)) : 0.0;
+  const int nneed0 = min(N, max(1, (int)ceil(spin ? nalpha : 0.5 * nelec) + 8));
   int bro_iter = 0;
   double last_e = 0.0;
   bool have_e = false;
@@ -1338,10 +1386,12 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
       eigenvalues<NT>(d, esq, N, nneed, gl, gu, pivmin, 4.0 * DBL_EPSILON * onenrm, eps);
       clk.mark(kStEigval);
       // (5) occupations (src/electronic.rs:3815-3921)
-      if (kt > 0.0 && nelec > 0.0 && nelec < 2.0 * N) {
+      if (spin) {
+        spin_channel_occupations<NT>(eps, N, nneed, nalpha, nbeta, kt, occ, pop, sh);
+      } else if (kt > 0.0 && nelec > 0.0 && nelec < 2.0 * N) {
         double fm, ft;
         bool amb;
-        fermi_cta<NT>(eps, N, nneed, nelec, kt, occ, sh, fm, ft, amb);
+        fermi_cta<NT>(eps, N, nneed, nelec, kt, 2.0, occ, sh, fm, ft, amb);
         if (tid == 0) {
           sh.scal[1] = fm;
           sh.scal[2] = ft;
@@ -1350,7 +1400,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
       } else if (wid == 0) {  // aufbau and the empty / full limits
         double fm, ft;
         bool amb;
-        fermi_warp(eps, N, nneed, nelec, kt, occ, fm, ft, amb);
+        fermi_warp(eps, N, nneed, nelec, kt, 2.0, occ, fm, ft, amb);
         if (lane == 0) {
           sh.scal[1] = fm;
           sh.scal[2] = ft;
@@ -1571,8 +1621,8 @@ __global__ void __launch_bounds__(NT, 512 / NT) scc_kernel(Batch B, Model M, Scc
 // row-major copies are used as they are.
 
 struct DenseState {
-  int status, nocc, converged, iter, bro_iter, have_e;
-  double last_e, e_el, e2, e3, ts, mu, rms, nelec, kt;
+  int status, nocc, converged, iter, bro_iter, have_e, spin;
+  double last_e, e_el, e2, e3, ts, mu, rms, nelec, kt, nalpha, nbeta;
 };
 constexpr int kDenseNT = 512;
 
@@ -1629,6 +1679,9 @@ __global__ void __launch_bounds__(kDenseNT, 1) dense_init_kernel(Batch B, Model 
     st->last_e = st->e_el = st->e2 = st->e3 = st->ts = st->mu = st->rms = 0.0;
     st->nelec = nref - B.charge[m];
     st->kt = fmax(opt.etemp, 0.0) * kBoltzmann;
+    st->spin = opt.spin_mult > 0;
+    st->nalpha = st->spin ? 0.5 * (rint(st->nelec) + (opt.spin_mult - 1)) : 0.0;
+    st->nbeta = st->spin ? 0.5 * (rint(st->nelec) - (opt.spin_mult - 1)) : 0.0;
     if (!ok) {
       B.status[m] = kErrInvalidInput;
       B.iterations[m] = 0;
@@ -1668,10 +1721,12 @@ __global__ void __launch_bounds__(kDenseNT, 1) dense_fermi_kernel(int N, DenseWo
   DenseState* st = (DenseState*)dw.state;
   const double nelec = st->nelec, kt = st->kt;
   const int tid = threadIdx.x;
-  if (kt > 0.0 && nelec > 0.0 && nelec < 2.0 * N) {
+  if (st->spin) {
+    spin_channel_occupations<kDenseNT>(dw.eps, N, N, st->nalpha, st->nbeta, kt, dw.occ, dw.pop, sh);
+  } else if (kt > 0.0 && nelec > 0.0 && nelec < 2.0 * N) {
     double fm, ft;
     bool amb;
-    fermi_cta<kDenseNT>(dw.eps, N, N, nelec, kt, dw.occ, sh, fm, ft, amb);
+    fermi_cta<kDenseNT>(dw.eps, N, N, nelec, kt, 2.0, dw.occ, sh, fm, ft, amb);
     if (tid == 0) {
       sh.scal[1] = fm;
       sh.scal[2] = ft;
@@ -1679,7 +1734,7 @@ __global__ void __launch_bounds__(kDenseNT, 1) dense_fermi_kernel(int N, DenseWo
   } else if (tid < 32) {
     double fm, ft;
     bool amb;
-    fermi_warp(dw.eps, N, N, nelec, kt, dw.occ, fm, ft, amb);
+    fermi_warp(dw.eps, N, N, nelec, kt, 2.0, dw.occ, fm, ft, amb);
     if (tid == 0) {
       sh.scal[1] = fm;
       sh.scal[2] = ft;

@@ -39,6 +39,7 @@ class Options(ctypes.Structure):
         ("electronic_temperature", ctypes.c_double),
         ("enable_dispersion", ctypes.c_int32),
         ("compute_gradient", ctypes.c_int32),
+        ("spin_multiplicity", ctypes.c_int32),
     ]
 
 

@@ -5,8 +5,9 @@ mirrors gfn1-rs's pyo3 class (src/python.rs:116-375): same constructor keywords
 and defaults, same ``calculate`` signature, a ``CalculationResult`` with the same
 fields (src/python.rs:2845-2950), and every error surfaces as ``ValueError``
 (src/python.rs:3344-3346).  Options outside the plain GFN1 energy+gradient path
-(multipole, exchange, spin, +U, D4, fields, ...) are rejected with ValueError
-when set to a non-default value.
+(multipole, exchange, spin polarization, +U, D4, fields, ...) are rejected
+with ValueError when set to a non-default value; ``multiplicity`` selects the
+reference's spin-constrained occupations in restricted orbitals.
 """
 from __future__ import annotations
 
@@ -27,7 +28,7 @@ _UNIT_SCALE = {"angstrom": ANGSTROM_TO_BOHR, "Angstrom": ANGSTROM_TO_BOHR, "A": 
 # Keywords of the reference constructor that select paths outside the plain
 # non-periodic GFN1 SCC, with the value that keeps them off.
 _OFF_PATH_DEFAULTS = {
-    "multiplicity": None, "spin_polarization": False, "experimental_d4": False, "d4_cutoff": None,
+    "spin_polarization": False, "experimental_d4": False, "d4_cutoff": None,
     "d4_cn_cutoff": None, "d4_atm": True, "d4_atm_cutoff": None, "d4_s9": None, "enable_cn_hamiltonian": True,
     "electric_field": None, "level_shift": 0.0, "scc_accelerator": None, "multipole": False,
     "multipole_octupole": False, "field_multipole": False, "multipole_third_order": False,
@@ -38,6 +39,16 @@ _OFF_PATH_DEFAULTS = {
     "hubbard_v": (), "hubbard_v_cutoff": 10.0, "hubbard_u_linear_response": False, "plus_u_all_d": False,
     "d3_reference_path": None,
 }
+
+
+def _multiplicity(m) -> int:
+    """ElectronicOptions::spin_multiplicity: None -> 0 (none), else the integer (>= 1)."""
+    if m is None:
+        return 0
+    m = int(m)
+    if m < 1:
+        raise ValueError("spin multiplicity must be at least 1")
+    return m
 
 
 def unit_scale(unit: str) -> float:
@@ -101,7 +112,7 @@ class Gfn1NativeCalculator:
                  energy_tolerance=1.0e-6, charge_tolerance=2.0e-5, mixing=0.4, scc_broyden=True,
                  scc_broyden_size=250, electronic_temperature=300.0, nprim=0, eigen_tolerance=1.0e-12,
                  enable_dispersion=True, device=0, **kwargs):
-        off = dict(multiplicity=multiplicity, spin_polarization=spin_polarization)
+        off = dict(spin_polarization=spin_polarization)
         off.update(kwargs)
         for k, v in off.items():
             if k not in _OFF_PATH_DEFAULTS:
@@ -117,7 +128,8 @@ class Gfn1NativeCalculator:
         self.charge = float(charge)
         self._opts = dict(max_scc=max_scc, energy_tolerance=energy_tolerance, charge_tolerance=charge_tolerance,
                           mixing=mixing, scc_broyden=int(bool(scc_broyden)), scc_broyden_size=scc_broyden_size,
-                          electronic_temperature=electronic_temperature, enable_dispersion=int(bool(enable_dispersion)))
+                          electronic_temperature=electronic_temperature, enable_dispersion=int(bool(enable_dispersion)),
+                          spin_multiplicity=_multiplicity(multiplicity))
         self._param_path = param_path
         self._engine = _lib.Engine(param_path, device)
 

@@ -49,6 +49,9 @@ typedef struct gfn1_options {
   double electronic_temperature; /* 300 K */
   int32_t enable_dispersion;     /* 1 */
   int32_t compute_gradient;      /* 1 */
+  int32_t spin_multiplicity;     /* 0 = None; n >= 1: ElectronicOptions::spin_multiplicity
+                                    (src/electronic.rs:159), spin-constrained occupations
+                                    in restricted orbitals (src/electronic.rs:3930-4045) */
 } gfn1_options;
 
 /* Per-batch outputs; any pointer may be NULL.  For gfn1_batch_download the
