@@ -349,20 +349,138 @@ __device__ __forceinline__ void warp_sum4(double& a, double& b, double& c, doubl
 // norm of the next column; a second barrier.  While the trailing size is at
 // most 32 * kCols, each lane keeps v_j and w_j of its columns in registers, so
 // the update reads and writes each element once.
+// One column of the Householder reduction after its reflector (v0, beta,
+// alpha) is known: p = beta A22 v, the rank-2 update and the norm of the next
+// column, which it returns.  Cached: the trailing size fits 32 * kCols and each
+// lane keeps its columns of v and w in registers.
+template <int NT, bool Cached>
+__device__ __forceinline__ double householder_column(double* A, int lda, int N, int k, double v0, double beta,
+                                                     double alpha, double* d, double* e, double* tau, double* pvec,
+                                                     SccShared& sh) {
+  constexpr int NW = NT / 32;
+  constexpr int kCols = 6;
+  constexpr bool cached = Cached;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int m = N - k - 1;
+  double* rowk = A + (long long)k * lda + (k + 1);
+  double* a22 = A + (long long)(k + 1) * lda + (k + 1);
+  double vreg[kCols], wreg[kCols];
+#pragma unroll
+  for (int c = 0; c < kCols; ++c) {
+    const int j = lane + 32 * c;
+    vreg[c] = (cached && j < m) ? (j == 0 ? v0 : rowk[j]) : 0.0;
+  }
+  // p = beta A22 v
+  double pv_part = 0.0;
+  for (int i0 = wid; i0 < m; i0 += 4 * NW) {
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    if (cached) {
+#pragma unroll
+      for (int c = 0; c < kCols; ++c) {
+        const int j = lane + 32 * c;
+        if (j < m) {
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const int i = i0 + r * NW;
+            if (i < m) s[r] += a22[(long long)i * lda + j] * vreg[c];
+          }
+        }
+      }
+    } else {
+      for (int j = lane; j < m; j += 32) {
+        const double v = (j == 0) ? v0 : rowk[j];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int i = i0 + r * NW;
+          if (i < m) s[r] += a22[(long long)i * lda + j] * v;
+        }
+      }
+    }
+    warp_sum4(s[0], s[1], s[2], s[3]);
+    if (lane == 0) {
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int i = i0 + r * NW;
+        if (i < m) {
+          const double pi = beta * s[r];
+          pvec[i] = pi;
+          pv_part += pi * (i == 0 ? v0 : rowk[i]);
+        }
+      }
+    }
+  }
+  if (lane == 0) sh.red[wid] = pv_part;
+  __syncthreads();
+  double pv = 0.0;
+#pragma unroll
+  for (int w = 0; w < NW; ++w) pv += sh.red[w];
+  const double K = 0.5 * beta * pv;
+  if (tid == 0) {
+    d[k] = A[(long long)k * lda + k];
+    e[k] = alpha;
+    tau[k] = beta;
+  }
+#pragma unroll
+  for (int c = 0; c < kCols; ++c) {
+    const int j = lane + 32 * c;
+    wreg[c] = (cached && j < m) ? pvec[j] - K * vreg[c] : 0.0;
+  }
+  // A22 -= v w^T + w v^T; warp 0 also takes the norm of the next column (row 1 of A22 from entry 1)
+  double nrm = 0.0;
+  for (int i = wid; i < m; i += NW) {
+    double* brow = a22 + (long long)i * lda;
+    const double vi = (i == 0) ? v0 : rowk[i];
+    const double wi = pvec[i] - K * vi;
+    if (cached) {
+#pragma unroll
+      for (int c = 0; c < kCols; ++c) {
+        const int j = lane + 32 * c;
+        if (j < m) {
+          const double nb = brow[j] - (vi * wreg[c] + wi * vreg[c]);
+          brow[j] = nb;
+          if (i == 0 && j >= 1) nrm += nb * nb;
+        }
+      }
+    } else {
+      for (int j = lane; j < m; j += 32) {
+        const double vj = (j == 0) ? v0 : rowk[j];
+        const double wj = pvec[j] - K * vj;
+        const double nb = brow[j] - (vi * wj + wi * vj);
+        brow[j] = nb;
+        if (i == 0 && j >= 1) nrm += nb * nb;
+      }
+    }
+  }
+  if (wid == 0) {
+    nrm = warp_sum(nrm);
+    if (lane == 0) sh.scal[3] = nrm;
+  }
+  __syncthreads();
+  if (tid == 0) rowk[0] = v0;  // the reflector of column k is row k from entry k+1
+  return sh.scal[3];
+}
+
+// The large-trailing-size column out of line, so that the hot loop of the
+// usual sizes stays compact.
+template <int NT>
+__device__ __noinline__ double householder_column_wide(double* A, int lda, int N, int k, double v0, double beta,
+                                                       double alpha, double* d, double* e, double* tau, double* pvec,
+                                                       SccShared& sh) {
+  return householder_column<NT, false>(A, lda, N, k, v0, beta, alpha, d, e, tau, pvec, sh);
+}
+
 template <int NT>
 __device__ void tridiagonalize(double* A, int lda, int N, double* d, double* e, double* tau, double* pvec,
                                SccShared& sh) {
-  constexpr int NW = NT / 32;
   constexpr int kCols = 6;
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int tid = threadIdx.x;
   double part = 0.0;
   if (N >= 3)
     for (int j = 1 + tid; j < N; j += NT) part += A[j] * A[j];
   double xn2 = block_sum(part, sh.red);
   for (int k = 0; k < N - 2; ++k) {
     const int m = N - k - 1;
-    double* rowk = A + (long long)k * lda + (k + 1);
-    double* a22 = A + (long long)(k + 1) * lda + (k + 1);
+    const double* rowk = A + (long long)k * lda + (k + 1);
     const double x0 = rowk[0];
     const double tail = xn2 - x0 * x0;
     if (tail == 0.0) {  // column already reduced
@@ -382,101 +500,8 @@ __device__ void tridiagonalize(double* A, int lda, int N, double* d, double* e, 
     const double alpha = x0 >= 0.0 ? -xn : xn;
     const double v0 = x0 - alpha;
     const double beta = 2.0 / (v0 * v0 + tail);
-    const bool cached = m <= 32 * kCols;
-    double vreg[kCols], wreg[kCols];
-#pragma unroll
-    for (int c = 0; c < kCols; ++c) {
-      const int j = lane + 32 * c;
-      vreg[c] = (cached && j < m) ? (j == 0 ? v0 : rowk[j]) : 0.0;
-    }
-    // p = beta A22 v
-    double pv_part = 0.0;
-    for (int i0 = wid; i0 < m; i0 += 4 * NW) {
-      double s[4] = {0.0, 0.0, 0.0, 0.0};
-      if (cached) {
-#pragma unroll
-        for (int c = 0; c < kCols; ++c) {
-          const int j = lane + 32 * c;
-          if (j < m) {
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-              const int i = i0 + r * NW;
-              if (i < m) s[r] += a22[(long long)i * lda + j] * vreg[c];
-            }
-          }
-        }
-      } else {
-        for (int j = lane; j < m; j += 32) {
-          const double v = (j == 0) ? v0 : rowk[j];
-#pragma unroll
-          for (int r = 0; r < 4; ++r) {
-            const int i = i0 + r * NW;
-            if (i < m) s[r] += a22[(long long)i * lda + j] * v;
-          }
-        }
-      }
-      warp_sum4(s[0], s[1], s[2], s[3]);
-      if (lane == 0) {
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          const int i = i0 + r * NW;
-          if (i < m) {
-            const double pi = beta * s[r];
-            pvec[i] = pi;
-            pv_part += pi * (i == 0 ? v0 : rowk[i]);
-          }
-        }
-      }
-    }
-    if (lane == 0) sh.red[wid] = pv_part;
-    __syncthreads();
-    double pv = 0.0;
-#pragma unroll
-    for (int w = 0; w < NW; ++w) pv += sh.red[w];
-    const double K = 0.5 * beta * pv;
-    if (tid == 0) {
-      d[k] = A[(long long)k * lda + k];
-      e[k] = alpha;
-      tau[k] = beta;
-    }
-#pragma unroll
-    for (int c = 0; c < kCols; ++c) {
-      const int j = lane + 32 * c;
-      wreg[c] = (cached && j < m) ? pvec[j] - K * vreg[c] : 0.0;
-    }
-    // A22 -= v w^T + w v^T; warp 0 also takes the norm of the next column (row 1 of A22 from entry 1)
-    double nrm = 0.0;
-    for (int i = wid; i < m; i += NW) {
-      double* brow = a22 + (long long)i * lda;
-      const double vi = (i == 0) ? v0 : rowk[i];
-      const double wi = pvec[i] - K * vi;
-      if (cached) {
-#pragma unroll
-        for (int c = 0; c < kCols; ++c) {
-          const int j = lane + 32 * c;
-          if (j < m) {
-            const double nb = brow[j] - (vi * wreg[c] + wi * vreg[c]);
-            brow[j] = nb;
-            if (i == 0 && j >= 1) nrm += nb * nb;
-          }
-        }
-      } else {
-        for (int j = lane; j < m; j += 32) {
-          const double vj = (j == 0) ? v0 : rowk[j];
-          const double wj = pvec[j] - K * vj;
-          const double nb = brow[j] - (vi * wj + wi * vj);
-          brow[j] = nb;
-          if (i == 0 && j >= 1) nrm += nb * nb;
-        }
-      }
-    }
-    if (wid == 0) {
-      nrm = warp_sum(nrm);
-      if (lane == 0) sh.scal[3] = nrm;
-    }
-    __syncthreads();
-    if (tid == 0) rowk[0] = v0;  // the reflector of column k is row k from entry k+1
-    xn2 = sh.scal[3];
+    xn2 = (m <= 32 * kCols) ? householder_column<NT, true>(A, lda, N, k, v0, beta, alpha, d, e, tau, pvec, sh)
+                            : householder_column_wide<NT>(A, lda, N, k, v0, beta, alpha, d, e, tau, pvec, sh);
   }
   __syncthreads();
   if (tid == 0) {
