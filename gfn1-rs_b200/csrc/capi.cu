@@ -275,6 +275,9 @@ struct gfn1_batch {
   gfn1_options opt;
   bool has_init_q = false;
   bool profiling = false;
+  DevBuf<int> shift_list;  // with a requested level shift: the molecules for the ladder kernel
+  DevBuf<int> shift_count; // their number (copied into queue[3])
+  int n_shift = 0;
   std::string host_err;   // message of the first molecule the host validation rejected
   int host_err_mol = -1;  // that molecule, or -1
   gfn1_guess* guess = nullptr;       // learned guess used when no initial charges are set
@@ -575,6 +578,7 @@ void fill_default(gfn1_options* o) {
   o->enable_dispersion = 1;
   o->compute_gradient = 1;
   o->spin_multiplicity = 0;
+  o->level_shift = 0.0;
 }
 
 // Checks of a requested spin multiplicity (resolve_spin_channels,
@@ -774,6 +778,36 @@ int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t*
     dmaxnsh = std::max(dmaxnsh, nsh_m[mm]);
     dmaxnat = std::max(dmaxnat, atom_offsets[mm + 1] - atom_offsets[mm]);
   }
+  b->n_shift = 0;
+  if (o.level_shift != 0.0) {
+    if (!std::isfinite(o.level_shift)) return fail(eng, GFN1_E_INVALID_INPUT, "level shift must be finite");
+    std::vector<int> lst;
+    for (int q = 0; q < nmol; ++q) {
+      const int mm = h_order[q];
+      if (h_st[mm] != GFN1_OK) continue;
+      if (q < n_dense) {  // the library-backed path has no level shift
+        h_st[mm] = st_m[mm] = GFN1_E_INVALID_INPUT;
+        worst = std::max(worst, (int)GFN1_E_INVALID_INPUT);
+        if (first_err.empty())
+          first_err = "molecule " + std::to_string(mm) + ": a level shift is applied up to 1024 AOs only";
+        continue;
+      }
+      lst.push_back(mm);
+    }
+    b->n_shift = (int)lst.size();
+    b->dense_ids.clear();  // every large molecule was rejected above
+    b->dense_n.clear();
+    b->dense_mo.clear();
+    b->host_err = first_err;
+    b->host_err_mol = -1;
+    for (int m = 0; m < nmol && b->host_err_mol < 0; ++m)
+      if (h_st[m] != GFN1_OK) b->host_err_mol = m;
+    if (!b->shift_list.ensure(std::max<size_t>(lst.size(), 1)) || !b->shift_count.ensure(1) ||
+        (!lst.empty() && cudaMemcpy(b->shift_list.p, lst.data(), sizeof(int) * lst.size(), cudaMemcpyHostToDevice) !=
+                             cudaSuccess) ||
+        cudaMemcpy(b->shift_count.p, &b->n_shift, sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(eng, GFN1_E_DEVICE, "device copy of the level-shift list failed");
+  }
   int n_large = n_dense;
   while (n_large < nmol && n_m[h_order[n_large]] > kSplitN) ++n_large;
   long long ws_total = 0;
@@ -816,7 +850,9 @@ int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t*
     R.nt = 128;
     const size_t fixed = scc_smem_bytes(R.maxnsh, R.maxn, R.maxnat, 0);
     while (R.nt < 512 && fixed > scc_max_dynamic_smem(R.nt)) R.nt *= 2;
-    R.n_cta = count == 0 ? 0 : std::min(count, 64);
+    // a requested level shift runs every molecule on this kernel: full width
+    const int width = o.level_shift != 0.0 ? (512 / R.nt) * eng->num_sms : 64;
+    R.n_cta = count == 0 ? 0 : std::min(count, width);
     R.ws_stride = count == 0 ? 0 : scc_workspace_doubles(std::max(R.maxn, 1), std::max(R.maxnsh, 1), b->cap,
                                                            std::max(R.maxnat, 1));
     R.ws_offset = ws_total;
@@ -935,10 +971,17 @@ int launch_stage(gfn1_batch* b, int stage, cudaStream_t st) {
     so.mixing = b->opt.mixing;
     so.etemp = b->opt.electronic_temperature;
     so.spin_mult = b->opt.spin_multiplicity;
+    so.level_shift = b->opt.level_shift;
     // fork: the small-molecule class runs on the side stream next to the large one
     if ((e = cudaEventRecord(b->ev_fork, st)) != cudaSuccess || (e = cudaStreamWaitEvent(b->side, b->ev_fork, 0)) != cudaSuccess)
       return cuda_fail(eng, e, "stream fork");
-    for (int c = 0; c < 2; ++c) {
+    if (so.level_shift != 0.0 && b->n_shift > 0) {  // every molecule to the ladder kernel, from rung 0
+      if ((e = cudaMemcpyAsync(b->failed.p, b->shift_list.p, sizeof(int) * b->n_shift, cudaMemcpyDeviceToDevice, st)) !=
+              cudaSuccess ||
+          (e = cudaMemcpyAsync(b->queue.p + 3, b->shift_count.p, sizeof(int), cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
+        return cuda_fail(eng, e, "level-shift list");
+    }
+    for (int c = 0; c < 2 && so.level_shift == 0.0; ++c) {
       const gfn1_batch::SccClass& K = b->cls[c];
       if (K.n_cta == 0) continue;
       SccLaunch SL;
@@ -1481,6 +1524,8 @@ extern "C" int gfn1_run_noalloc(gfn1_engine* eng, int nat, const uint8_t* z, con
     const std::string se = spin_multiplicity_error(o.spin_multiplicity, nelec, n);
     if (!se.empty()) return fail(eng, GFN1_E_INVALID_INPUT, se);
   }
+  if (o.level_shift != 0.0)
+    return fail(eng, GFN1_E_INVALID_INPUT, "gfn1_run_noalloc runs without a level shift (use gfn1_run)");
   const int dev = eng->device;
   if (dev < 0 || dev >= kNaMaxDevices) return fail(eng, GFN1_E_INVALID_INPUT, "device ordinal out of range");
   cudaError_t e = cudaSetDevice(dev);
@@ -1601,6 +1646,7 @@ extern "C" int gfn1_run_noalloc(gfn1_engine* eng, int nat, const uint8_t* z, con
   so.mixing = o.mixing;
   so.etemp = o.electronic_temperature;
   so.spin_mult = o.spin_multiplicity;
+  so.level_shift = 0.0;
   const size_t sm_setup = sizeof(double) * (16 * (size_t)nat + 32) + sizeof(int) * (3 * (size_t)nat + 2 + 2 * (size_t)nsh);
   const size_t sm_scc = std::max(scc_smem_bytes(nsh, n, nat, 0),
                                  std::min(scc_smem_bytes(nsh, n, nat, n), scc_max_dynamic_smem(n > 96 ? 512 : 256)));

@@ -69,6 +69,7 @@ struct SccOptions {
   int enable_dispersion;
   int spin_mult;     // 0: no spin multiplicity; n >= 1: spin-constrained occupations
   double energy_tol, charge_tol, mixing, etemp;
+  double level_shift;  // requested virtual level shift (Eh), 0 = none
 };
 
 // Parameters of one launch of the persistent SCC kernel (one size class).

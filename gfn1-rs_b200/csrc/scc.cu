@@ -1315,20 +1315,23 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
   // The reference's fallback ladder (src/electronic.rs:1390-1447): rung 0 is
   // the requested options (the main kernel); rungs 1-3 (the Robust kernel,
   // for molecules rung 0 left unconverged) restart from the initial charges
-  // with linear mixing 0.2 and a 0.2 Eh level shift, then 0.1 / 0.1, then
-  // Broyden at T_el >= 3000 K.
-  const int rung_first = Robust ? 1 : 0, rung_last = Robust ? 3 : 0;
+  // with linear mixing 0.2 and a level shift of max(requested, 0.2 Eh), then
+  // 0.1 / max(requested, 0.1), then Broyden at T_el >= 3000 K without shift.
+  // A requested level shift sends every molecule to the Robust kernel, which
+  // then starts at rung 0 (the main kernel carries no level-shift code).
+  const int rung_first = Robust ? (opt.level_shift != 0.0 ? 0 : 1) : 0, rung_last = Robust ? 3 : 0;
   for (int rung = rung_first; rung <= rung_last && !converged; ++rung) {
   SccOptions ro = opt;
-  double lshift = 0.0;  // the plain path has no level shift on rung 0
+  double lshift = Robust ? opt.level_shift : 0.0;
   if (rung == 1 || rung == 2) {
     ro.broyden = 0;
     ro.mixing = rung == 1 ? 0.20 : 0.10;
-    lshift = rung == 1 ? 0.20 : 0.10;
+    lshift = fmax(opt.level_shift, rung == 1 ? 0.20 : 0.10);
     ro.max_scc = max(opt.max_scc, 800);
   } else if (rung == 3) {
     ro.etemp = fmax(opt.etemp, 3000.0);
     ro.max_scc = max(opt.max_scc, 250);
+    lshift = 0.0;
   }
   const double kt = fmax(ro.etemp, 0.0) * kBoltzmann;
   for (int s = tid; s < nsh; s += NT) w.qin[s] = B.init_q ? B.init_q[sh0 + s] : 0.0;

@@ -40,6 +40,7 @@ class Options(ctypes.Structure):
         ("enable_dispersion", ctypes.c_int32),
         ("compute_gradient", ctypes.c_int32),
         ("spin_multiplicity", ctypes.c_int32),
+        ("level_shift", ctypes.c_double),
     ]
 
 

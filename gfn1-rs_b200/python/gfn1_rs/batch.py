@@ -62,11 +62,12 @@ def _matrices(engine, off, z, m: int, call) -> dict:
 class BatchCalculator:
     def __init__(self, param_path=None, device=0, max_scc=250, energy_tolerance=1.0e-6, charge_tolerance=2.0e-5,
                  mixing=0.4, scc_broyden=True, scc_broyden_size=250, electronic_temperature=300.0,
-                 enable_dispersion=True, learned_guess=None, spin_multiplicity=None):
+                 enable_dispersion=True, learned_guess=None, spin_multiplicity=None, level_shift=0.0):
         """learned_guess: None/False for the reference's zero initial guess, True for
         the packaged trained network, or a path to a parameter file.
         spin_multiplicity: None (the reference's default) or n >= 1 for every
-        molecule of a call (spin-constrained occupations)."""
+        molecule of a call (spin-constrained occupations).  level_shift: the
+        reference's virtual level shift (Eh), molecules up to 1024 AOs."""
         self.engine = _lib.Engine(param_path, device)
         self.guess = None
         if learned_guess:
@@ -77,7 +78,7 @@ class BatchCalculator:
                          mixing=mixing, scc_broyden=int(bool(scc_broyden)), scc_broyden_size=scc_broyden_size,
                          electronic_temperature=electronic_temperature,
                          enable_dispersion=int(bool(enable_dispersion)),
-                         spin_multiplicity=int(spin_multiplicity or 0))
+                         spin_multiplicity=int(spin_multiplicity or 0), level_shift=float(level_shift))
         self._last = None  # (atom_offsets, numbers) of the last calculate_flat call
 
     def shell_offsets(self, atom_offsets, numbers) -> np.ndarray:

@@ -30,7 +30,7 @@ _UNIT_SCALE = {"angstrom": ANGSTROM_TO_BOHR, "Angstrom": ANGSTROM_TO_BOHR, "A": 
 _OFF_PATH_DEFAULTS = {
     "spin_polarization": False, "experimental_d4": False, "d4_cutoff": None,
     "d4_cn_cutoff": None, "d4_atm": True, "d4_atm_cutoff": None, "d4_s9": None, "enable_cn_hamiltonian": True,
-    "electric_field": None, "level_shift": 0.0, "scc_accelerator": None, "multipole": False,
+    "electric_field": None, "scc_accelerator": None, "multipole": False,
     "multipole_octupole": False, "field_multipole": False, "multipole_third_order": False,
     "multipole_secondary_basis": None, "multipole_order": 0, "multipole_charge_order": (), "lr_exchange": False,
     "onsite_exchange": False, "dynamic_omega": False, "scf_trah": False, "charge_order": 3,
@@ -111,7 +111,7 @@ class Gfn1NativeCalculator:
     def __init__(self, param_path=None, charge=0.0, multiplicity=None, spin_polarization=False, max_scc=250,
                  energy_tolerance=1.0e-6, charge_tolerance=2.0e-5, mixing=0.4, scc_broyden=True,
                  scc_broyden_size=250, electronic_temperature=300.0, nprim=0, eigen_tolerance=1.0e-12,
-                 enable_dispersion=True, device=0, **kwargs):
+                 enable_dispersion=True, device=0, level_shift=0.0, **kwargs):
         off = dict(spin_polarization=spin_polarization)
         off.update(kwargs)
         for k, v in off.items():
@@ -129,7 +129,7 @@ class Gfn1NativeCalculator:
         self._opts = dict(max_scc=max_scc, energy_tolerance=energy_tolerance, charge_tolerance=charge_tolerance,
                           mixing=mixing, scc_broyden=int(bool(scc_broyden)), scc_broyden_size=scc_broyden_size,
                           electronic_temperature=electronic_temperature, enable_dispersion=int(bool(enable_dispersion)),
-                          spin_multiplicity=_multiplicity(multiplicity))
+                          spin_multiplicity=_multiplicity(multiplicity), level_shift=float(level_shift))
         self._param_path = param_path
         self._engine = _lib.Engine(param_path, device)
 

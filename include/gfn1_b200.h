@@ -52,6 +52,8 @@ typedef struct gfn1_options {
   int32_t spin_multiplicity;     /* 0 = None; n >= 1: ElectronicOptions::spin_multiplicity
                                     (src/electronic.rs:159), spin-constrained occupations
                                     in restricted orbitals (src/electronic.rs:3930-4045) */
+  double level_shift;            /* 0 Eh: ElectronicOptions::level_shift (src/electronic.rs:1413-1416,
+                                    2125-2137), up to 1024 AOs */
 } gfn1_options;
 
 /* Per-batch outputs; any pointer may be NULL.  For gfn1_batch_download the

@@ -1,0 +1,69 @@
+"""A requested virtual level shift (ElectronicOptions::level_shift,
+src/electronic.rs:1413-1416, :2125-2137) on the GPU against the oracle with the
+same shift: the device runs every molecule on its fallback-ladder kernel from
+rung 0.  Tolerances as the other parity tests (tight SCC)."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import smoke_molecule
+
+pytestmark = pytest.mark.gpu
+
+TIGHT = dict(energy_tolerance=1e-10, charge_tolerance=1e-8)
+NAMES = ("water", "phosphine", "caffeine", "ferrocene")
+
+
+def _flat(mols):
+    off = np.concatenate([[0], np.cumsum([len(z) for z, _ in mols])]).astype(np.int32)
+    return off, np.concatenate([z for z, _ in mols]), np.concatenate([x for _, x in mols])
+
+
+@pytest.mark.parametrize("shift", [0.3, 0.05])
+def test_level_shift_matches_oracle(gpu_calc, oracle_mod, fixtures, shift):
+    from gfn1_rs import BatchCalculator
+
+    mols = [smoke_molecule(fixtures, n) for n in NAMES]
+    off, z, x = _flat(mols)
+    r = BatchCalculator(level_shift=shift, **TIGHT).calculate_flat(off, z, x)
+    plain = BatchCalculator(**TIGHT).calculate_flat(off, z, x)
+    for m, (zm, xm) in enumerate(mols):
+        o = oracle_mod.run(zm, xm, options=oracle_mod.make_options(level_shift=shift, **TIGHT))
+        assert r.status[m] == 0, NAMES[m]
+        a0, a1 = off[m], off[m + 1]
+        assert abs(r.energy[m] - o.energy) <= 1e-6, NAMES[m]
+        assert np.max(np.abs(r.gradient[a0:a1] - o.gradient)) <= 1e-5, NAMES[m]
+        # the shift moves the path, not the fixed point
+        assert abs(r.energy[m] - plain.energy[m]) <= 1e-6, NAMES[m]
+
+
+def test_level_shift_rejected_on_the_large_molecule_path(gpu_calc, fixtures):
+    from gfn1_rs import BatchCalculator, Gfn1Error
+
+    mols = [smoke_molecule(fixtures, n) for n in ("water", "caffeine")]
+    off, z, x = _flat(mols)
+    calc = BatchCalculator(level_shift=0.2, **TIGHT)
+    old = os.environ.get("GFN1_DENSE_N")
+    os.environ["GFN1_DENSE_N"] = "16"  # caffeine above the threshold, water below
+    try:
+        r = calc.calculate_flat(off, z, x)
+        with pytest.raises(Gfn1Error, match="level shift"):
+            calc.calculate_flat(off, z, x, raise_on_error=True)
+    finally:
+        if old is None:
+            os.environ.pop("GFN1_DENSE_N", None)
+        else:
+            os.environ["GFN1_DENSE_N"] = old
+    assert r.status[0] == 0 and r.status[1] == 3
+
+
+def test_native_calculator_level_shift(gpu_calc, oracle_mod, fixtures):
+    from gfn1_rs import Gfn1NativeCalculator
+    from gfn1_rs.native import BOHR_TO_ANGSTROM
+
+    z, x = smoke_molecule(fixtures, "water")
+    r = Gfn1NativeCalculator(level_shift=0.25).calculate(z.tolist(), (x * BOHR_TO_ANGSTROM).tolist(),
+                                                         compute_gradient=True)
+    o = oracle_mod.run(z, x, options=oracle_mod.make_options(level_shift=0.25))
+    assert r.converged and abs(r.energy_hartree - o.energy) <= 1e-6
