@@ -22,6 +22,10 @@ ANGSTROM_TO_BOHR = 1.8897261246257702              # src/constants.rs:27
 BOHR_TO_ANGSTROM = 1.0 / ANGSTROM_TO_BOHR
 FORCE_HARTREE_PER_BOHR_TO_EV_PER_ANGSTROM = HARTREE_TO_EV / BOHR_TO_ANGSTROM
 
+_SYMBOLS = ("X H He Li Be B C N O F Ne Na Mg Al Si P S Cl Ar K Ca Sc Ti V Cr Mn Fe Co Ni Cu Zn Ga Ge As Se Br Kr "
+            "Rb Sr Y Zr Nb Mo Tc Ru Rh Pd Ag Cd In Sn Sb Te I Xe Cs Ba La Ce Pr Nd Pm Sm Eu Gd Tb Dy Ho Er Tm "
+            "Yb Lu Hf Ta W Re Os Ir Pt Au Hg Tl Pb Bi Po At Rn").split()
+
 _UNIT_SCALE = {"angstrom": ANGSTROM_TO_BOHR, "Angstrom": ANGSTROM_TO_BOHR, "A": ANGSTROM_TO_BOHR,
                "bohr": 1.0, "Bohr": 1.0, "au": 1.0}
 
@@ -169,3 +173,85 @@ class Gfn1NativeCalculator:
         _lib.check(rc, self._engine.handle)
         return CalculationResult(terms[0], terms, grad, qat, dip, iters[0], status[0] == 0, shell_charges=qsh,
                                  fermi_level=float(fermi[0]))
+
+    # ------------------------------------------------------------------ batch-backed methods
+    def _batch(self):
+        if getattr(self, "_batch_calc", None) is None:
+            from .batch import BatchCalculator
+            self._batch_calc = BatchCalculator(param_path=self._param_path, device=self._engine.device, **self._opts)
+        return self._batch_calc
+
+    def optimize(self, numbers, positions, unit="angstrom", cell=None, pbc=(True, True, True), max_iterations=250,
+                 gradient_tolerance=1.0e-4, step_tolerance=1.0e-7, history=12, max_atom_step=0.30,
+                 trajectory_path=None) -> "OptimizationResult":
+        """L-BFGS geometry optimisation (src/python.rs:490-546 over
+        src/optimizer.rs:78-320); non-periodic only."""
+        from .optimize import OptimizeOptions, optimize_batch
+        if cell is not None:
+            raise ValueError("the B200 engine optimises non-periodic systems only")
+        z, xyz = build_system(numbers, positions, unit)
+        if len(z) == 0:
+            raise ValueError("cannot run GFN1 SCC for an empty basis")
+        opts = OptimizeOptions(max_iterations=int(max_iterations), gradient_tolerance=float(gradient_tolerance),
+                               step_tolerance=float(step_tolerance), history=int(history),
+                               max_atom_step=float(max_atom_step))
+        out = optimize_batch(self._batch(), [0, len(z)], z, xyz, charges=[self.charge], options=opts)
+        if out["errors"][0] is not None and out["gradient"][0] is None:
+            raise ValueError(out["errors"][0])
+        res = OptimizationResult(z, out, 0)
+        if trajectory_path:
+            res.write_trajectory(trajectory_path)
+        return res
+
+    def hessian(self, numbers, positions, unit="angstrom"):
+        """Nuclear Hessian (Eh/bohr^2) as a 3N x 3N nested list, atom-major
+        (src/python.rs:1747-1771); central differences of the analytic
+        gradient (gfn1_rs.hessian)."""
+        return self._hessian_array(numbers, positions, unit).tolist()
+
+    def vibrational_frequencies(self, numbers, positions, unit="angstrom") -> dict:
+        """``wavenumbers`` (cm^-1, imaginary as negative) and ``modes``
+        (src/python.rs:1821-1850)."""
+        from .hessian import vibrational_analysis
+        z, _ = build_system(numbers, positions, unit)
+        v = vibrational_analysis(self._hessian_array(numbers, positions, unit), z)
+        return {"wavenumbers": v["wavenumbers"].tolist(), "modes": v["modes"].tolist()}
+
+    def _hessian_array(self, numbers, positions, unit):
+        from .hessian import hessian_batch
+        z, xyz = build_system(numbers, positions, unit)
+        if len(z) == 0:
+            raise ValueError("cannot run GFN1 SCC for an empty basis")
+        out = hessian_batch(self._batch(), [0, len(z)], z, xyz, charges=[self.charge])
+        if out["hessians"][0] is None:
+            _lib.check(int(out["status"][0]) or 8)
+        return out["hessians"][0]
+
+
+class OptimizationResult:
+    """Result of ``Gfn1NativeCalculator.optimize`` (src/python.rs:2954-3010)."""
+
+    def __init__(self, numbers, out: dict, m: int):
+        frames = out["frames"][m]
+        g = np.asarray(out["gradient"][m]).reshape(-1, 3)
+        self.numbers = [int(v) for v in numbers]
+        self.energy_hartree = float(out["energy"][m])
+        self.energy_ev = self.energy_hartree * HARTREE_TO_EV
+        self.positions_angstrom = (np.asarray(frames[-1]).reshape(-1, 3) * BOHR_TO_ANGSTROM).tolist()
+        self.gradient_hartree_per_bohr = g.tolist()
+        self.forces_ev_per_angstrom = (-g * FORCE_HARTREE_PER_BOHR_TO_EV_PER_ANGSTROM).tolist()
+        self.iterations = int(out["iterations"][m])
+        self.converged = bool(out["converged"][m])
+        self.max_gradient = float(out["max_gradient"][m])
+        self.trajectory_positions_angstrom = [(np.asarray(f).reshape(-1, 3) * BOHR_TO_ANGSTROM).tolist()
+                                              for f in frames]
+        self.trajectory_energies_hartree = [float(t[1]) for t in out["trajectories"][m]]
+
+    def write_trajectory(self, path: str) -> None:
+        """XYZ frames of the accepted steps (energy in the comment line)."""
+        with open(path, "w") as fh:
+            for xyz, e in zip(self.trajectory_positions_angstrom, self.trajectory_energies_hartree):
+                fh.write(f"{len(self.numbers)}\nenergy_hartree={e:.12f}\n")
+                for zz, p in zip(self.numbers, xyz):
+                    fh.write(f"{_SYMBOLS[zz]} {p[0]:.10f} {p[1]:.10f} {p[2]:.10f}\n")
+

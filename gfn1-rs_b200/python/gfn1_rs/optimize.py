@@ -50,6 +50,7 @@ class _Mol:
     tries: int = 0
     dd: float = 0.0
     trajectory: list = field(default_factory=list)
+    frames: list = field(default_factory=list)  # accepted geometries, frame 0 the input
 
 
 def lbfgs_direction(g, s_hist, y_hist, rho_hist):
@@ -93,6 +94,7 @@ def optimize(evaluate, x0_list, options: OptimizeOptions | None = None):
         m.energy, m.grad, m.q = e, np.asarray(g, dtype=np.float64).ravel(), q
         m.converged = float(np.abs(m.grad).max()) <= opt.gradient_tolerance
         m.trajectory.append((0, m.energy, float(np.abs(m.grad).max()), 0.0))
+        m.frames.append(m.x.copy())
     hist_len = max(opt.history, 1)
     while True:
         for m in mols:  # start a new step where no line search is pending
@@ -127,6 +129,7 @@ def optimize(evaluate, x0_list, options: OptimizeOptions | None = None):
                 m.x, m.energy, m.grad, m.q = xt, e, g, q
                 maxg = float(np.abs(g).max())
                 m.trajectory.append((m.iterations, e, maxg, step_norm))
+                m.frames.append(xt.copy())
                 m.converged = maxg <= opt.gradient_tolerance or step_norm <= opt.step_tolerance
                 m.direction = None
             else:
@@ -176,4 +179,5 @@ def optimize_batch(calc, atom_offsets, numbers, xyz_bohr, charges=None, options:
             "iterations": np.array([m.iterations for m in mols]),
             "converged": np.array([m.converged for m in mols]),
             "errors": [m.error for m in mols], "engine_calls": calls[0],
-            "trajectories": [m.trajectory for m in mols], "shell_offsets": shoff}
+            "trajectories": [m.trajectory for m in mols], "frames": [m.frames for m in mols],
+            "gradient": [m.grad for m in mols], "shell_offsets": shoff}
