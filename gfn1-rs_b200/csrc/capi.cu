@@ -937,7 +937,7 @@ int launch_stage(gfn1_batch* b, int stage, cudaStream_t st) {
   gfn1_engine* eng = b->eng;
   const Batch B = b->dev();
   const Model M = eng->model();
-  const int nt = 256;
+  const int nt = 128;  // setup CTA: four per SM (measured 8.9 against 9.0 ms with 256 threads)
   cudaError_t e = cudaSuccess;
   if (stage == 0) {
     // reset status from the host-validated copy and the work counter
@@ -1651,7 +1651,7 @@ extern "C" int gfn1_run_noalloc(gfn1_engine* eng, int nat, const uint8_t* z, con
   const size_t sm_scc = std::max(scc_smem_bytes(nsh, n, nat, 0),
                                  std::min(scc_smem_bytes(nsh, n, nat, n), scc_max_dynamic_smem(n > 96 ? 512 : 256)));
   const size_t sm_grad = sizeof(double) * 7 * (size_t)nat + sizeof(int) * (3 * (size_t)nat + 2);
-  setup_kernel<<<1, 256, sm_setup, st>>>(B, M, o.enable_dispersion, nsh);
+  setup_kernel<<<1, 128, sm_setup, st>>>(B, M, o.enable_dispersion, nsh);
   SccLaunch SL;
   SL.q_begin = 0;
   SL.q_end = 1;

@@ -122,9 +122,9 @@ __device__ double halogen_term(const Model& M, const int* zs, const double* xyz,
   return e;
 }
 
-// Two CTAs per SM (128 registers): the s/p pairs fit, pairs with a d shell
-// (rare) keep part of their blocks in local memory.
-__global__ void __launch_bounds__(256, 2) setup_kernel(Batch B, Model M, int enable_dispersion, int max_nsh) {
+// 128-thread CTAs, four per SM (128 registers): the s/p pairs fit, pairs with
+// a d shell (rare) keep part of their blocks in local memory.
+__global__ void __launch_bounds__(128, 4) setup_kernel(Batch B, Model M, int enable_dispersion, int max_nsh) {
   extern __shared__ double smem[];
   const int m = blockIdx.x;
   if (B.status[m] != kOk) return;  // rejected by the host-side validation
