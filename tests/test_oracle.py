@@ -177,3 +177,21 @@ def test_spin_multiplicity_gradient_is_derivative(oracle_mod):
         fd = (oracle_mod.run([6, 1, 1], xp, options=opt, gradient=False).energy
               - oracle_mod.run([6, 1, 1], xm, options=opt, gradient=False).energy) / (2 * h)
         assert abs(fd - r.gradient[a, k]) < 5e-5
+
+
+def test_d_shell_rotation_invariance(oracle_mod, fixtures):
+    """The five real d functions transform among themselves under rotation only
+    with the right combination coefficients (src/basis.rs:406-436): the
+    ferrocene energy is invariant under random rotations."""
+    z, x = smoke_molecule(fixtures, "ferrocene")
+    opt = oracle_mod.make_options(energy_tolerance=1e-10, charge_tolerance=1e-8)
+    e0 = oracle_mod.run(z, x, options=opt, gradient=False).energy
+    rng = np.random.default_rng(4)
+    for _ in range(2):
+        q = rng.normal(size=4)
+        a, b, c, d = q / np.linalg.norm(q)
+        R = np.array([[a * a + b * b - c * c - d * d, 2 * (b * c - a * d), 2 * (b * d + a * c)],
+                      [2 * (b * c + a * d), a * a - b * b + c * c - d * d, 2 * (c * d - a * b)],
+                      [2 * (b * d - a * c), 2 * (c * d + a * b), a * a - b * b - c * c + d * d]])
+        e = oracle_mod.run(z, x @ R.T, options=opt, gradient=False).energy
+        assert abs(e - e0) < 1e-8
