@@ -92,6 +92,8 @@ class GFN1RSCalculator(_AseCalculator):
     default_parameters = {
         "param_path": None,
         "charge": 0.0,
+        "multiplicity": None,
+        "level_shift": 0.0,
         "max_scc": 250,
         "energy_tolerance": 1.0e-6,
         "charge_tolerance": 2.0e-5,
@@ -127,7 +129,9 @@ class GFN1RSCalculator(_AseCalculator):
         if self._batch is None:
             from .batch import BatchCalculator
             self._batch = BatchCalculator(param_path=self.parameters["param_path"], device=self.parameters["device"],
-                                          learned_guess=self.parameters["learned_guess"], **self._options())
+                                          learned_guess=self.parameters["learned_guess"],
+                                          spin_multiplicity=self.parameters["multiplicity"],
+                                          level_shift=self.parameters["level_shift"], **self._options())
         return self._batch
 
     @staticmethod
@@ -187,7 +191,8 @@ class GFN1RSCalculator(_AseCalculator):
             opts = self._options()
             self._native = Gfn1NativeCalculator(param_path=self.parameters["param_path"],
                                                 charge=self.parameters["charge"], device=self.parameters["device"],
-                                                **opts)
+                                                multiplicity=self.parameters["multiplicity"],
+                                                level_shift=self.parameters["level_shift"], **opts)
         return self._native
 
     def get_dipole_au(self, atoms=None):

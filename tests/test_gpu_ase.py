@@ -69,3 +69,15 @@ def test_periodic_rejected(gpu_calc):
     from gfn1_rs.ase import GFN1RSCalculator
     with pytest.raises(ValueError):
         GFN1RSCalculator().calculate(FakeAtoms([1, 1], [[0, 0, 0], [0.74, 0, 0]], pbc=True), ["energy"])
+
+
+def test_multiplicity_and_level_shift_parameters(gpu_calc):
+    from gfn1_rs import BatchCalculator
+    from gfn1_rs.ase import _HARTREE, GFN1RSCalculator
+    from gfn1_rs.native import ANGSTROM_TO_BOHR
+
+    o2 = FakeAtoms([8, 8], [[0.0, 0.0, 0.0], [0.0, 0.0, 1.21]])
+    calc = GFN1RSCalculator(multiplicity=3, level_shift=0.1)
+    calc.calculate(o2, ["energy"])
+    ref = BatchCalculator(spin_multiplicity=3).calculate_flat([0, 2], o2.numbers, o2.positions * ANGSTROM_TO_BOHR)
+    assert abs(calc.results["energy"] - ref.energy[0] * _HARTREE) <= 1e-5
