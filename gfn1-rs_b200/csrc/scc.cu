@@ -341,6 +341,15 @@ __device__ __forceinline__ void warp_sum4(double& a, double& b, double& c, doubl
   }
 }
 
+// D += A B for one 8x8x4 FP64 tile on the tensor cores (PTX mma.m8n8k4 .f64,
+// row-major A, column-major B): lane l holds A[l/4][l%4], B[l%4][l/4] and
+// D[l/4][2(l%4)], D[l/4][2(l%4)+1].
+__device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
 // Householder reduction of the symmetric A (full storage, leading dimension
 // lda) to tridiagonal form: d, e, reflector scalars tau, and the reflector of
 // column k in row k (entries k+1..N-1).  Per column: p = beta A22 v by warps
@@ -1264,36 +1273,56 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     }
   }
   __syncthreads();
-  // H0' = L^-1 H0 L^-T as U = L^-1 H0, then H0' = U (L^-1)^T with (L^-1)^T
-  // stored explicitly, so both products read rows (lanes over columns) and
-  // broadcast the other factor.  U and the transpose use the eigenvector and
-  // global work matrices, free until the first iteration.
-  double* U = w.A;
-  double* LiT = w.Z;
-  for (int i = wid; i < N; i += NW)
-    for (int j = lane; j < N; j += 32) LiT[(long long)j * N + i] = Li[(long long)i * N + j];
-  for (int i = wid; i < N; i += NW) {
-    const double* lir = Li + (long long)i * N;
-    for (int j = lane; j < N; j += 32) {
-      double s = 0.0;
-#pragma unroll 4
-      for (int k = 0; k <= i; ++k) s += lir[k] * H0[(long long)k * N + j];
-      U[(long long)i * N + j] = s;
+  // H0' = L^-1 H0 L^-T on the FP64 tensor cores: U = L^-1 H0 in 8x8 tiles
+  // (row i of L^-1 ends at the diagonal), then H0' = U (L^-1)^T for the tiles
+  // on and below the diagonal, each written to both triangles so that H0' is
+  // exactly symmetric.  U uses the global work matrix, free until the first
+  // iteration.  Each warp owns whole tiles; lanes beyond N load zeros.
+  {
+    double* U = w.A;
+    const int T = (N + 7) >> 3;
+    const int g = lane >> 2, t4 = lane & 3;
+    for (int tile = wid; tile < T * T; tile += NW) {
+      const int I = tile / T, J = tile - I * T;
+      const int i = I * 8 + g, jb = J * 8 + g;
+      const int kend = min(N, I * 8 + 8);
+      double d0 = 0.0, d1 = 0.0;
+      for (int k0 = 0; k0 < kend; k0 += 4) {
+        const int k = k0 + t4;
+        const double a = (i < N && k < N) ? Li[(long long)i * N + k] : 0.0;
+        const double b = (k < N && jb < N) ? H0[(long long)k * N + jb] : 0.0;
+        dmma_m8n8k4(d0, d1, a, b);
+      }
+      const int jc = J * 8 + 2 * t4;
+      if (i < N && jc < N) U[(long long)i * N + jc] = d0;
+      if (i < N && jc + 1 < N) U[(long long)i * N + jc + 1] = d1;
     }
-  }
-  __syncthreads();
-  for (int i = wid; i < N; i += NW) {
-    const double* ur = U + (long long)i * N;
-    for (int j = lane; j <= i; j += 32) {
-      double s = 0.0;
-#pragma unroll 4
-      for (int k = 0; k <= j; ++k) s += ur[k] * LiT[(long long)k * N + j];
-      Hp[(long long)i * N + j] = s;
+    __syncthreads();
+    for (int tile = wid; tile < T * (T + 1) / 2; tile += NW) {
+      int I = 0;
+      while ((I + 1) * (I + 2) / 2 <= tile) ++I;
+      const int J = tile - I * (I + 1) / 2;
+      const int i = I * 8 + g, jb = J * 8 + g;
+      const int kend = min(N, J * 8 + 8);
+      double d0 = 0.0, d1 = 0.0;
+      for (int k0 = 0; k0 < kend; k0 += 4) {
+        const int k = k0 + t4;
+        const double a = (i < N && k < N) ? U[(long long)i * N + k] : 0.0;
+        const double b = (jb < N && k < N) ? Li[(long long)jb * N + k] : 0.0;
+        dmma_m8n8k4(d0, d1, a, b);
+      }
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const int j = J * 8 + 2 * t4 + c;
+        if (i < N && j < N && (I != J || j <= i)) {
+          const double v = c ? d1 : d0;
+          Hp[(long long)i * N + j] = v;
+          Hp[(long long)j * N + i] = v;
+        }
+      }
     }
+    __syncthreads();
   }
-  __syncthreads();
-  for (int i = wid; i < N; i += NW)
-    for (int j = i + 1 + lane; j < N; j += 32) Hp[(long long)i * N + j] = Hp[(long long)j * N + i];
 
   // ---- SCC state
   double nref = 0.0;
