@@ -1190,7 +1190,6 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
   double* Hp = w.Hp;
   double* Z = w.Z;
   double* C = w.C;
-  double* D = w.D;
   double* iw = w.iw;
   const double* G = B.gam + B.gam_off[m];
   const bool a_shared = (long long)N * work_lda(N) <= as_cap;  // shared memory when the launch gave room
@@ -1523,57 +1522,46 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     // (7) back-transformation Z := Q Z
     back_transform<NT>(A, lda, tau, N, Z, N, nocc, w.W1, w.W2, sh);
     clk.mark(kStBackTr);
-    // (8) C = L^-T Z, D = L Z and the AO populations (S P)_mu,mu; warps own
-    //     4-row groups, lanes eigenvectors.  L is lower triangular, so row mu
-    //     of D needs k <= mu and row mu of C (column mu of L^-1) needs k >= mu.
-    for (int rg = wid; rg * 4 < N; rg += NW) {
-      const int m0 = rg * 4;
-      const int mmax = min(m0 + 3, N - 1);
-      int mu_r[4];
-#pragma unroll
-      for (int r = 0; r < 4; ++r) mu_r[r] = min(m0 + r, mmax);
-      double pp[4] = {0.0, 0.0, 0.0, 0.0};
-      for (int i0 = 0; i0 < nocc; i0 += 32) {
-        const int i = i0 + lane;
-        if (i < nocc) {
-          double c[4] = {0.0, 0.0, 0.0, 0.0}, dd[4] = {0.0, 0.0, 0.0, 0.0};
-          const double* zc = Z + i;
-#pragma unroll 4
-          for (int k = 0; k < m0; ++k) {  // D only
-            const double z = zc[(long long)k * N];
-#pragma unroll
-            for (int r = 0; r < 4; ++r) dd[r] += L[(long long)mu_r[r] * N + k] * z;
+    // (8) C = L^-T Z, D = L Z (= S C) and the AO populations
+    //     (S P)_mu,mu = sum_i f_i C_mu,i D_mu,i on the FP64 tensor cores: each
+    //     warp owns 8-row blocks of mu and runs over 8-column tiles of the
+    //     occupied eigenvectors.  Row mu of L ends and column mu of L^-1 starts
+    //     at the diagonal.  D only feeds the populations and is not stored.
+    {
+      const int T = (N + 7) >> 3, Ti = (nocc + 7) >> 3;
+      const int g = lane >> 2, t4 = lane & 3;
+      for (int MU = wid; MU < T; MU += NW) {
+        const int mu = MU * 8 + g;
+        double pp = 0.0;
+        for (int IV = 0; IV < Ti; ++IV) {
+          const int ib = IV * 8 + g;
+          double c0 = 0.0, c1 = 0.0, d0 = 0.0, d1 = 0.0;
+          const int dend = min(N, MU * 8 + 8);
+          for (int k0 = 0; k0 < dend; k0 += 4) {
+            const int k = k0 + t4;
+            const double a = (mu < N && k < N) ? L[(long long)mu * N + k] : 0.0;
+            const double b = (k < N && ib < nocc) ? Z[(long long)k * N + ib] : 0.0;
+            dmma_m8n8k4(d0, d1, a, b);
           }
-          for (int k = m0; k <= mmax; ++k) {  // the diagonal block: both, triangular
-            const double z = zc[(long long)k * N];
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-              if (k <= mu_r[r]) dd[r] += L[(long long)mu_r[r] * N + k] * z;
-              if (k >= mu_r[r]) c[r] += Li[(long long)k * N + mu_r[r]] * z;
-            }
+          for (int k0 = MU * 8; k0 < N; k0 += 4) {
+            const int k = k0 + t4;
+            const double a = (mu < N && k < N) ? Li[(long long)k * N + mu] : 0.0;
+            const double b = (k < N && ib < nocc) ? Z[(long long)k * N + ib] : 0.0;
+            dmma_m8n8k4(c0, c1, a, b);
           }
-#pragma unroll 4
-          for (int k = mmax + 1; k < N; ++k) {  // C only
-            const double z = zc[(long long)k * N];
-            const double* lik = Li + (long long)k * N;
-#pragma unroll
-            for (int r = 0; r < 4; ++r) c[r] += lik[mu_r[r]] * z;
+          const int ic = IV * 8 + 2 * t4;
+          if (mu < N && ic < nocc) {
+            C[(long long)mu * N + ic] = c0;
+            pp += occ[ic] * c0 * d0;
           }
-#pragma unroll
-          for (int r = 0; r < 4; ++r) {
-            const int mu_ = m0 + r;
-            if (mu_ <= mmax) {
-              C[(long long)mu_ * N + i] = c[r];
-              D[(long long)mu_ * N + i] = dd[r];
-              pp[r] += occ[i] * c[r] * dd[r];
-            }
+          if (mu < N && ic + 1 < nocc) {
+            C[(long long)mu * N + ic + 1] = c1;
+            pp += occ[ic + 1] * c1 * d1;
           }
         }
-      }
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const double s = warp_sum(pp[r]);
-        if (lane == 0 && m0 + r <= mmax) pop[m0 + r] = s;
+        pp += __shfl_xor_sync(0xffffffffu, pp, 1);
+        pp += __shfl_xor_sync(0xffffffffu, pp, 2);
+        if (t4 == 0 && mu < N) pop[mu] = pp;
       }
     }
     __syncthreads();
