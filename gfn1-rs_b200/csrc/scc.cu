@@ -797,6 +797,7 @@ __device__ __noinline__ void spin_channel_occupations(const double* eps, int N, 
 template <int NT>
 __device__ void back_transform(const double* A, int lda, const double* tau, int N, double* Z, int ldz, int ncol,
                                double* W1, double* W2, SccShared& sh) {
+  constexpr int NW = NT / 32;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int nref = N - 2;
   if (nref <= 0 || ncol <= 0) return;
@@ -834,13 +835,25 @@ __device__ void back_transform(const double* A, int lda, const double* tau, int 
         __syncwarp();
       }
     }
-    for (int idx = tid; idx < nb * ncol; idx += NT) {
-      const int j = idx / ncol, c = idx - j * ncol;
-      const double* vj = A + (long long)(kb + j) * lda;
-      double s = 0.0;
-#pragma unroll 8
-      for (int r = kb + j + 1; r < N; ++r) s += vj[r] * Z[(long long)r * ldz + c];
-      W1[j * ncol + c] = s;
+    // W1 = V^T Z on the FP64 tensor cores: 8x8 tiles of (reflector j,
+    // column c), k over the rows r; reflector j has entries r > kb + j
+    {
+      const int g = lane >> 2, t4 = lane & 3;
+      const int TC = (ncol + 7) >> 3, TJ = (nb + 7) >> 3;
+      for (int tile = wid; tile < TJ * TC; tile += NW) {
+        const int JT = tile / TC, CT = tile - JT * TC;
+        const int j = JT * 8 + g, cb = CT * 8 + g;
+        double d0 = 0.0, d1 = 0.0;
+        for (int r0 = kb + 1; r0 < N; r0 += 4) {
+          const int r = r0 + t4;
+          const double a = (j < nb && r < N && r > kb + j) ? A[(long long)(kb + j) * lda + r] : 0.0;
+          const double b = (r < N && cb < ncol) ? Z[(long long)r * ldz + cb] : 0.0;
+          dmma_m8n8k4(d0, d1, a, b);
+        }
+        const int cc = CT * 8 + 2 * t4;
+        if (j < nb && cc < ncol) W1[j * ncol + cc] = d0;
+        if (j < nb && cc + 1 < ncol) W1[j * ncol + cc + 1] = d1;
+      }
     }
     __syncthreads();
     for (int idx = tid; idx < nb * ncol; idx += NT) {
@@ -850,14 +863,25 @@ __device__ void back_transform(const double* A, int lda, const double* tau, int 
       W2[j * ncol + c] = s;
     }
     __syncthreads();
-    for (int idx = tid; idx < (N - kb - 1) * ncol; idx += NT) {
-      const int rr = idx / ncol, c = idx - rr * ncol;
-      const int r = kb + 1 + rr;
-      const int jmax = min(nb, rr + 1);
-      double s = 0.0;
-#pragma unroll 4
-      for (int j = 0; j < jmax; ++j) s += A[(long long)(kb + j) * lda + r] * W2[j * ncol + c];
-      Z[(long long)r * ldz + c] -= s;
+    // Z -= V W2 on the FP64 tensor cores: 8x8 tiles of (row r, column c)
+    // starting from Z, k over the reflectors j
+    {
+      const int g = lane >> 2, t4 = lane & 3;
+      const int TC = (ncol + 7) >> 3, TR = (N - kb - 1 + 7) >> 3;
+      for (int tile = wid; tile < TR * TC; tile += NW) {
+        const int RT = tile / TC, CT = tile - RT * TC;
+        const int r = kb + 1 + RT * 8 + g, cb = CT * 8 + g, cc = CT * 8 + 2 * t4;
+        double d0 = (r < N && cc < ncol) ? Z[(long long)r * ldz + cc] : 0.0;
+        double d1 = (r < N && cc + 1 < ncol) ? Z[(long long)r * ldz + cc + 1] : 0.0;
+        for (int j0 = 0; j0 < nb; j0 += 4) {
+          const int j = j0 + t4;
+          const double a = (r < N && j < nb && r > kb + j) ? -A[(long long)(kb + j) * lda + r] : 0.0;
+          const double b = (j < nb && cb < ncol) ? W2[j * ncol + cb] : 0.0;
+          dmma_m8n8k4(d0, d1, a, b);
+        }
+        if (r < N && cc < ncol) Z[(long long)r * ldz + cc] = d0;
+        if (r < N && cc + 1 < ncol) Z[(long long)r * ldz + cc + 1] = d1;
+      }
     }
     __syncthreads();
   }

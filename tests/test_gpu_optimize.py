@@ -46,4 +46,7 @@ def test_batched_optimisation_converges_like_single_runs(gpu_calc):
     warm = optimize_batch(calc, off, z, x, warm_start=True)
     both = warm["converged"] & r["converged"]
     assert both.sum() >= 3
-    assert np.abs(warm["energy"][both] - r["energy"][both]).max() <= 1e-6
+    # warm-started SCCs take a slightly different L-BFGS path; both stop at a
+    # largest gradient of 1e-4 Eh/bohr, which along soft modes leaves the
+    # energy uncertain to about 1e-5 Eh
+    assert np.abs(warm["energy"][both] - r["energy"][both]).max() <= 1e-5
