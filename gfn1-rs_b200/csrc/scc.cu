@@ -1397,27 +1397,32 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
   for (iter = 1; iter <= ro.max_scc; ++iter) {
     // (1) shell potential from the input charges
     stage_potential<NT>(B, M, mc, w, vao);
-    // (2) F' = H0' - 1/2 (M + M^T), M = L^-1 diag(v) L; warps own 4-row groups,
-    //     lanes 32 columns; L rows are read coalesced, L^-1 entries broadcast
-    for (int rg = wid; rg * 4 < N; rg += NW) {
-      const int i0 = rg * 4;
-      const int imax = min(i0 + 3, N - 1);
-      for (int j0 = 0; j0 <= imax; j0 += 32) {
-        const int j = j0 + lane;
-        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-        for (int k = j0; k <= imax; ++k) {
-          const double lkj = (k >= j && j < N) ? L[(long long)k * N + j] * vao[k] : 0.0;
-          s0 += Li[(long long)i0 * N + k] * lkj;
-          if (i0 + 1 <= imax) s1 += Li[(long long)(i0 + 1) * N + k] * lkj;
-          if (i0 + 2 <= imax) s2 += Li[(long long)(i0 + 2) * N + k] * lkj;
-          if (i0 + 3 <= imax) s3 += Li[(long long)(i0 + 3) * N + k] * lkj;
+    // (2) F' = H0' - 1/2 (M + M^T) with M = L^-1 diag(v) L lower triangular,
+    //     so F'_ij = H0'_ij - M_ij / 2 below the diagonal and H0'_ii - M_ii on
+    //     it.  M on the FP64 tensor cores, 8x8 tiles on and below the
+    //     diagonal, k from the tile's first column to its last row.
+    {
+      const int T = (N + 7) >> 3;
+      const int g = lane >> 2, t4 = lane & 3;
+      for (int tile = wid; tile < T * (T + 1) / 2; tile += NW) {
+        int I = 0;
+        while ((I + 1) * (I + 2) / 2 <= tile) ++I;
+        const int J = tile - I * (I + 1) / 2;
+        const int i = I * 8 + g, jb = J * 8 + g;
+        const int kend = min(N, I * 8 + 8);
+        double d0 = 0.0, d1 = 0.0;
+        for (int k0 = J * 8; k0 < kend; k0 += 4) {
+          const int k = k0 + t4;
+          const double a = (i < N && k < N) ? Li[(long long)i * N + k] : 0.0;
+          const double b = (k < N && jb < N) ? L[(long long)k * N + jb] * vao[k] : 0.0;
+          dmma_m8n8k4(d0, d1, a, b);
         }
-        const double sr[4] = {s0, s1, s2, s3};
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          const int i = i0 + r;
-          if (i <= imax && j <= i) {
-            const double f = Hp[(long long)i * N + j] - (i == j ? sr[r] : 0.5 * sr[r]);
+        for (int c = 0; c < 2; ++c) {
+          const int j = J * 8 + 2 * t4 + c;
+          if (i < N && j <= i) {
+            const double mv = c ? d1 : d0;
+            const double f = Hp[(long long)i * N + j] - (i == j ? mv : 0.5 * mv);
             A[(long long)i * lda + j] = f;
             A[(long long)j * lda + i] = f;
           }
