@@ -1637,20 +1637,38 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     }
   }
   // density and energy-weighted density of the last diagonalisation
-  // (src/linalg.rs:243-273), kept per molecule for the gradient kernel
-  for (int i = wid; i < N; i += NW)
-    for (int j = lane; j <= i; j += 32) {
-      double p = 0.0, q = 0.0;
-      for (int k = 0; k < nocc; ++k) {
-        const double cc = C[(long long)i * N + k] * C[(long long)j * N + k];
-        p += occ[k] * cc;
-        q += occ[k] * eps[k] * cc;
+  // (src/linalg.rs:243-273), kept per molecule for the gradient kernel:
+  // P = C f C^T and W = C f eps C^T on the FP64 tensor cores, 8x8 tiles on
+  // and below the diagonal written to both triangles
+  {
+    const int T = (N + 7) >> 3;
+    const int g = lane >> 2, t4 = lane & 3;
+    for (int tile = wid; tile < T * (T + 1) / 2; tile += NW) {
+      int I = 0;
+      while ((I + 1) * (I + 2) / 2 <= tile) ++I;
+      const int J = tile - I * (I + 1) / 2;
+      const int i = I * 8 + g, jb = J * 8 + g;
+      double p0 = 0.0, p1 = 0.0, q0 = 0.0, q1 = 0.0;
+      for (int k0 = 0; k0 < nocc; k0 += 4) {
+        const int k = k0 + t4;
+        const double ci = (i < N && k < nocc) ? C[(long long)i * N + k] * occ[k] : 0.0;
+        const double cj = (jb < N && k < nocc) ? C[(long long)jb * N + k] : 0.0;
+        dmma_m8n8k4(p0, p1, ci, cj);
+        dmma_m8n8k4(q0, q1, k < nocc ? ci * eps[k] : 0.0, cj);
       }
-      B.P[mo + (long long)i * N + j] = p;
-      B.P[mo + (long long)j * N + i] = p;
-      B.W[mo + (long long)i * N + j] = q;
-      B.W[mo + (long long)j * N + i] = q;
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const int j = J * 8 + 2 * t4 + c;
+        if (i < N && j <= i) {
+          const double pv = c ? p1 : p0, qv = c ? q1 : q0;
+          B.P[mo + (long long)i * N + j] = pv;
+          B.P[mo + (long long)j * N + i] = pv;
+          B.W[mo + (long long)i * N + j] = qv;
+          B.W[mo + (long long)j * N + i] = qv;
+        }
+      }
     }
+  }
   __syncthreads();
   clk.mark(kStFinal);
 }
