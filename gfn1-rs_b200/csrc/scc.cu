@@ -526,6 +526,177 @@ __device__ void tridiagonalize(double* A, int lda, int N, double* d, double* e, 
   __syncthreads();
 }
 
+// Blocked Householder reduction (panels of kPanel columns, four-warp CTAs, at
+// most 32 * 6 + 1 rows): the same reflectors as tridiagonalize, but the rank-2
+// updates of a panel are applied lazily to each panel column and, at the end
+// of the panel, to the trailing matrix in one FP64 tensor-core pass,
+// A22 -= V W^T + W V^T.  Per column: the column with the panel's earlier
+// updates (x), its reflector (stored in row k as before), p = beta (A22 v -
+// V (W^T v) - W (V^T v)) with A22 as of the panel start, and w = p - K v kept
+// in Wp (kPanel x N, row l for the panel's column l).  V is read from the
+// reflector rows of A.  xs and pvec are N-vectors of scratch.
+constexpr int kPanel = 16;
+template <int NT>
+__device__ void tridiagonalize_blocked(double* A, int lda, int N, double* d, double* e, double* tau, double* pvec,
+                                       double* xs, double* Wp, SccShared& sh) {
+  constexpr int NW = NT / 32;
+  constexpr int kCols = 6;
+  static_assert(NW == 4, "four warps");
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int g = lane >> 2, t4 = lane & 3;
+  for (int k0 = 0; k0 < N - 2; k0 += kPanel) {
+    const int nbp = min(kPanel, N - 2 - k0);
+    for (int j = 0; j < nbp; ++j) {
+      const int k = k0 + j, m = N - k - 1;
+      // x: row k (= column k) from the diagonal, with the panel's earlier updates
+      double part = 0.0;
+      for (int t = tid; t <= m; t += NT) {
+        const int i = k + t;
+        double x = A[(long long)k * lda + i];
+        for (int l = 0; l < j; ++l) {
+          const double* vl = A + (long long)(k0 + l) * lda;
+          const double* wl = Wp + (long long)l * N;
+          x -= vl[k] * wl[i] + wl[k] * vl[i];
+        }
+        xs[t] = x;
+        if (t >= 1) part += x * x;
+      }
+      part = warp_sum(part);
+      if (lane == 0) sh.red[wid] = part;
+      __syncthreads();
+      const double xn2 = (sh.red[0] + sh.red[1]) + (sh.red[2] + sh.red[3]);
+      const double x0 = xs[1];
+      const double tail = xn2 - x0 * x0;
+      if (tid == 0) d[k] = xs[0];
+      if (tail == 0.0) {  // column already reduced: no reflector, W column zero
+        for (int t = tid; t < m; t += NT) {
+          A[(long long)k * lda + k + 1 + t] = xs[1 + t];
+          Wp[(long long)j * N + k + 1 + t] = 0.0;
+        }
+        if (tid == 0) {
+          e[k] = x0;
+          tau[k] = 0.0;
+        }
+        __syncthreads();
+        continue;
+      }
+      const double xn = sqrt(xn2);
+      const double alpha = x0 >= 0.0 ? -xn : xn;
+      const double v0 = x0 - alpha;
+      const double beta = 2.0 / (v0 * v0 + tail);
+      double vreg[kCols];
+#pragma unroll
+      for (int c = 0; c < kCols; ++c) {
+        const int jj = lane + 32 * c;
+        vreg[c] = jj < m ? (jj == 0 ? v0 : xs[1 + jj]) : 0.0;
+      }
+      if (wid == 0) {  // the reflector of column k is row k from entry k+1
+#pragma unroll
+        for (int c = 0; c < kCols; ++c) {
+          const int jj = lane + 32 * c;
+          if (jj < m) A[(long long)k * lda + k + 1 + jj] = vreg[c];
+        }
+      }
+      // raw A22 v (four rows per warp pass) and the panel products W^T v, V^T v
+      const double* a22 = A + (long long)(k + 1) * lda + (k + 1);
+      for (int i0 = wid; i0 < m; i0 += 4 * NW) {
+        double s[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int c = 0; c < kCols; ++c) {
+          const int jj = lane + 32 * c;
+          if (jj < m) {
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+              const int i = i0 + r * NW;
+              if (i < m) s[r] += a22[(long long)i * lda + jj] * vreg[c];
+            }
+          }
+        }
+        warp_sum4(s[0], s[1], s[2], s[3]);
+        if (lane == 0) {
+#pragma unroll
+          for (int r = 0; r < 4; ++r)
+            if (i0 + r * NW < m) pvec[i0 + r * NW] = s[r];
+        }
+      }
+      for (int l = wid; l < j; l += NW) {
+        const double* vl = A + (long long)(k0 + l) * lda + (k + 1);
+        const double* wl = Wp + (long long)l * N + (k + 1);
+        double om = 0.0, nu = 0.0;
+#pragma unroll
+        for (int c = 0; c < kCols; ++c) {
+          const int jj = lane + 32 * c;
+          if (jj < m) {
+            om += wl[jj] * vreg[c];
+            nu += vl[jj] * vreg[c];
+          }
+        }
+        om = warp_sum(om);
+        nu = warp_sum(nu);
+        if (lane == 0) {
+          sh.VtV[0][l] = om;
+          sh.VtV[1][l] = nu;
+        }
+      }
+      __syncthreads();
+      // p = beta (A22 v - V (W^T v) - W (V^T v)) and p.v
+      double pv_part = 0.0;
+      for (int t = tid; t < m; t += NT) {
+        const int i = k + 1 + t;
+        double p = pvec[t];
+        for (int l = 0; l < j; ++l)
+          p -= A[(long long)(k0 + l) * lda + i] * sh.VtV[0][l] + Wp[(long long)l * N + i] * sh.VtV[1][l];
+        p *= beta;
+        pvec[t] = p;
+        pv_part += p * (t == 0 ? v0 : xs[1 + t]);
+      }
+      pv_part = warp_sum(pv_part);
+      if (lane == 0) sh.red[4 + wid] = pv_part;
+      __syncthreads();
+      const double K = 0.5 * beta * ((sh.red[4] + sh.red[5]) + (sh.red[6] + sh.red[7]));
+      for (int t = tid; t < m; t += NT)
+        Wp[(long long)j * N + k + 1 + t] = pvec[t] - K * (t == 0 ? v0 : xs[1 + t]);
+      if (tid == 0) {
+        e[k] = alpha;
+        tau[k] = beta;
+      }
+      __syncthreads();
+    }
+    // trailing matrix: A22 -= V W^T + W V^T for rows and columns >= s0, as
+    // 8x8 tiles starting from A, k over the panel's columns
+    const int s0 = k0 + nbp, ms = N - s0;
+    const int T = (ms + 7) >> 3;
+    for (int tile = wid; tile < T * T; tile += NW) {
+      const int I = tile / T, J = tile - I * T;
+      const int i = s0 + I * 8 + g, jb = s0 + J * 8 + g, jc = s0 + J * 8 + 2 * t4;
+      double c0 = (i < N && jc < N) ? A[(long long)i * lda + jc] : 0.0;
+      double c1 = (i < N && jc + 1 < N) ? A[(long long)i * lda + jc + 1] : 0.0;
+      for (int l0 = 0; l0 < nbp; l0 += 4) {
+        const int l = l0 + t4;
+        const bool lok = l < nbp;
+        const double* vl = A + (long long)(k0 + (lok ? l : 0)) * lda;
+        const double* wl = Wp + (long long)(lok ? l : 0) * N;
+        dmma_m8n8k4(c0, c1, (lok && i < N) ? -vl[i] : 0.0, (lok && jb < N) ? wl[jb] : 0.0);
+        dmma_m8n8k4(c0, c1, (lok && i < N) ? -wl[i] : 0.0, (lok && jb < N) ? vl[jb] : 0.0);
+      }
+      if (i < N && jc < N) A[(long long)i * lda + jc] = c0;
+      if (i < N && jc + 1 < N) A[(long long)i * lda + jc + 1] = c1;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    if (N >= 2) {
+      d[N - 2] = A[(long long)(N - 2) * lda + (N - 2)];
+      e[N - 2] = A[(long long)(N - 1) * lda + (N - 2)];
+      tau[N - 2] = 0.0;
+    }
+    d[N - 1] = A[(long long)(N - 1) * lda + (N - 1)];
+    e[N - 1] = 0.0;
+    tau[N - 1] = 0.0;
+  }
+  __syncthreads();
+}
+
 // Eigenvalues k = 0..nneed-1 and N-1 of the tridiagonal, one thread each.
 // Bisection on the Sturm count until the count at the iterate x says that
 // eigenvalue k is the nearest one above (count k) or below (count k+1); from
@@ -1447,7 +1618,14 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     }
     clk.mark(kStFock);
     // (3) Householder tridiagonalisation
-    tridiagonalize<NT>(A, lda, N, d, e, tau, pvec, sh);
+    if constexpr (NT == 128) {
+      if (N <= 32 * 6 + 1)
+        tridiagonalize_blocked<NT>(A, lda, N, d, e, tau, pvec, eps, w.W1, sh);
+      else
+        tridiagonalize<NT>(A, lda, N, d, e, tau, pvec, sh);
+    } else {
+      tridiagonalize<NT>(A, lda, N, d, e, tau, pvec, sh);
+    }
     clk.mark(kStTridiag);
     // (4) eigenvalues needed by the occupations
     double gl = INFINITY, gu = -INFINITY, onenrm = 0.0, emax2 = 0.0;
