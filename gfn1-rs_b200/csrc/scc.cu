@@ -535,7 +535,7 @@ __device__ void tridiagonalize(double* A, int lda, int N, double* d, double* e, 
 // V (W^T v) - W (V^T v)) with A22 as of the panel start, and w = p - K v kept
 // in Wp (kPanel x N, row l for the panel's column l).  V is read from the
 // reflector rows of A.  xs and pvec are N-vectors of scratch.
-constexpr int kPanel = 16;
+constexpr int kPanel = 8;
 template <int NT>
 __device__ void tridiagonalize_blocked(double* A, int lda, int N, double* d, double* e, double* tau, double* pvec,
                                        double* xs, double* Wp, SccShared& sh) {
