@@ -6,7 +6,7 @@ network here predicts that vector from the geometry: per H/C/N/O atom, 64
 radial and 32 angular descriptors (cutoff 6 bohr) plus the element one-hot feed
 three SiLU layers of 128 and a linear layer to the atom's two shell charges,
 which are then shifted so each molecule sums to its charge.  The converged SCC
-always judges the result; a worse guess only costs iterations.
+always decides the result; a worse guess only costs iterations.
 
 Training runs on the GPU through the library's own kernels (descriptors, FP32
 GEMMs with fused SiLU epilogues, projection loss, Adam); torch only provides

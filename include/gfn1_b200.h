@@ -179,7 +179,7 @@ int gfn1_run_noalloc(gfn1_engine* eng, int nat, const uint8_t* z, const double* 
  * of 128 and a linear layer to the atom's two shell charges; each molecule's
  * charges are shifted to sum to its total charge.  Molecules with other
  * elements get the zero guess.  Inference runs with BF16 weights and
- * activations (FP32 accumulation); the converged SCC always judges the result.
+ * activations (FP32 accumulation); the converged SCC always decides the result.
  *
  * Parameters (float32, gfn1_guess_param_count() values): feature mean[96],
  * feature scale[96], W1[100x128], b1[128], W2[128x128], b2[128],
