@@ -254,7 +254,7 @@ struct gfn1_engine {
 // (one device->host copy); byte offsets, 256-byte aligned.
 struct BlobLayout {
   size_t atom_off, shell_off, ao_off, mat_off, gam_off, pair_off, order, status0, z, charge, xyz, init_q, in_bytes;
-  size_t terms, grad, shell_q, atom_q, dipole, fermi, iterations, status, out_bytes;
+  size_t terms, grad, shell_q, atom_q, dipole, fermi, iterations, status, rung, out_bytes;
 };
 
 struct gfn1_batch {
@@ -345,6 +345,7 @@ struct gfn1_batch {
     B.fermi = dout<double>(lay.fermi);
     B.iterations = dout<int>(lay.iterations);
     B.status = dout<int>(lay.status);
+    B.rung = dout<int>(lay.rung);
     B.orb_eps = orb_eps.p;
     B.orb_occ = orb_occ.p;
     B.queue = queue.p;
@@ -713,6 +714,7 @@ int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t*
   L.fermi = take(sizeof(double) * nmol);
   L.iterations = take(sizeof(int) * nmol);
   L.status = take(sizeof(int) * nmol);
+  L.rung = take(sizeof(int) * nmol);
   L.out_bytes = off;
   if (!b->h_in.ensure(L.in_bytes) || !b->h_out.ensure(L.out_bytes))
     return fail(eng, GFN1_E_DEVICE, "pinned host allocation failed");
@@ -943,7 +945,8 @@ int launch_stage(gfn1_batch* b, int stage, cudaStream_t st) {
     // reset status from the host-validated copy and the work counter
     if ((e = cudaMemcpyAsync(B.status, b->din<int>(b->lay.status0), sizeof(int) * b->nmol, cudaMemcpyDeviceToDevice,
                              st)) != cudaSuccess ||
-        (e = cudaMemsetAsync(b->queue.p, 0, sizeof(int) * 4, st)) != cudaSuccess)
+        (e = cudaMemsetAsync(b->queue.p, 0, sizeof(int) * 4, st)) != cudaSuccess ||
+        (e = cudaMemsetAsync(B.rung, 0, sizeof(int) * b->nmol, st)) != cudaSuccess)
       return cuda_fail(eng, e, "batch reset");
     if (b->profiling && (e = cudaMemsetAsync(b->stage.p, 0, sizeof(unsigned long long) * kStages, st)) != cudaSuccess)
       return cuda_fail(eng, e, "batch reset");
@@ -1063,6 +1066,10 @@ int finish(gfn1_batch* b, const gfn1_outputs* out, cudaStream_t st) {
     if (out->fermi_level) std::memcpy(out->fermi_level, b->hout<double>(L.fermi), sizeof(double) * nmol);
     if (out->iterations) std::memcpy(out->iterations, b->hout<int>(L.iterations), sizeof(int) * nmol);
     if (out->status) std::memcpy(out->status, status, sizeof(int) * nmol);
+    if (out->rung) {
+      const int* rung = b->hout<int>(L.rung);
+      for (int m = 0; m < nmol; ++m) out->rung[m] = status[m] == GFN1_OK ? rung[m] : -1;
+    }
   }
   int worst = GFN1_OK, first = -1;
   for (int m = 0; m < b->nmol; ++m) {
@@ -1289,6 +1296,7 @@ int gfn1_batch_outputs_device(gfn1_batch* b, gfn1_outputs* out) {
   out->fermi_level = b->dout<double>(L.fermi);
   out->iterations = b->dout<int>(L.iterations);
   out->status = b->dout<int>(L.status);
+  out->rung = b->dout<int>(L.rung);
   return GFN1_OK;
 }
 
@@ -1683,6 +1691,7 @@ extern "C" int gfn1_run_noalloc(gfn1_engine* eng, int nat, const uint8_t* z, con
     if (out->fermi_level) std::memcpy(out->fermi_level, hp(o_fermi), sizeof(double));
     if (out->iterations) std::memcpy(out->iterations, hp(o_iter), sizeof(int));
     if (out->status) out->status[0] = status;
+    if (out->rung) out->rung[0] = status == GFN1_OK ? 0 : -1;  // this entry point runs rung 0 only
   }
   if (status != GFN1_OK)
     return fail(eng, status, status == GFN1_E_SCC_NOT_CONVERGED ? "GFN1 SCC did not converge"

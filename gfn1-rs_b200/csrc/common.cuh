@@ -134,6 +134,7 @@ struct Batch {
   double* fermi;            // [nmol]
   int* iterations;          // [nmol]
   int* status;              // [nmol]
+  int* rung;                // [nmol] fallback-ladder rung whose SCC converged (-1: none), or null
   double* orb_eps;          // [naos] orbital energies of the last diagonalisation (offset ao_off[m]), or null
   double* orb_occ;          // [naos] their occupations, or null
   int* queue;               // work counters: [0], [1] size classes, [2] fallback ladder, [3] failed count

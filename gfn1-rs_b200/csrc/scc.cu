@@ -1543,7 +1543,9 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
   // A requested level shift sends every molecule to the Robust kernel, which
   // then starts at rung 0 (the main kernel carries no level-shift code).
   const int rung_first = Robust ? (opt.level_shift != 0.0 ? 0 : 1) : 0, rung_last = Robust ? 3 : 0;
+  [[maybe_unused]] int rung_used = rung_first;  // the rung whose SCC converged (reported by the ladder kernel)
   for (int rung = rung_first; rung <= rung_last && !converged; ++rung) {
+  rung_used = rung;
   SccOptions ro = opt;
   double lshift = Robust ? opt.level_shift : 0.0;
   if (rung == 1 || rung == 2) {
@@ -1804,6 +1806,9 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
   if (iter > ro.max_scc) iter = ro.max_scc;
   }  // rungs
   if (!Robust && !converged && B.failed && tid == 0) B.failed[atomicAdd(B.queue + 3, 1)] = m;
+  if constexpr (Robust) {  // rung-0 molecules keep the 0 the host wrote before the launches
+    if (B.rung && tid == 0) B.rung[m] = converged ? rung_used : -1;
+  }
 
   // ---- results
   stage_results<NT>(B, mc, w, iter, converged, e_el, e2, e3, ts, mu);

@@ -52,7 +52,7 @@ class Outputs(ctypes.Structure):
     _fields_ = [
         ("energy", _dp), ("terms", _dp), ("gradient", _dp), ("shell_charges", _dp),
         ("atomic_charges", _dp), ("dipole", _dp), ("fermi_level", _dp), ("iterations", _ip),
-        ("status", _ip),
+        ("status", _ip), ("rung", _ip),
     ]
 
 

@@ -29,6 +29,10 @@ class BatchResult:
     status: np.ndarray          # [nmol]
     atom_offsets: np.ndarray
     shell_offsets: np.ndarray
+    # [nmol] rung of the reference's fallback ladder (src/electronic.rs:1390-1447)
+    # whose SCC converged: 0 = the requested scheme, 1-2 = linear mixing with a
+    # level shift, 3 = T_el raised to max(T_el, 3000 K); -1 where none converged
+    rung: np.ndarray | None = None
 
 
 def _flatten(molecules, unit):
@@ -116,9 +120,10 @@ class BatchCalculator:
         fermi = np.zeros(nmol)
         iters = np.zeros(nmol, dtype=np.int32)
         status = np.zeros(nmol, dtype=np.int32)
+        rung = np.zeros(nmol, dtype=np.int32)
         out = _lib.Outputs(_lib.ptr(energy), _lib.ptr(terms), _lib.ptr(grad), _lib.ptr(qsh), _lib.ptr(qat),
                            _lib.ptr(dip), _lib.ptr(fermi), _lib.ptr(iters, ctypes.c_int32),
-                           _lib.ptr(status, ctypes.c_int32))
+                           _lib.ptr(status, ctypes.c_int32), _lib.ptr(rung, ctypes.c_int32))
         opt = _options(self.opts, compute_gradient)
         rc = L.gfn1_batch_energy_gradient(self.engine.handle, nmol, _lib.ptr(off, ctypes.c_int32),
                                           _lib.ptr(z, ctypes.c_uint8), _lib.ptr(xyz), _lib.ptr(ch), _lib.ptr(q0),
@@ -126,7 +131,7 @@ class BatchCalculator:
         self._last = (off, z)
         if rc != 0 and (raise_on_error or rc not in (3, 4, 8, 12)):
             _lib.check(rc, self.engine.handle)
-        return BatchResult(energy, terms, grad, qsh, qat, dip, fermi, iters, status, off, shoff)
+        return BatchResult(energy, terms, grad, qsh, qat, dip, fermi, iters, status, off, shoff, rung)
 
     def molecule_matrices(self, m: int) -> dict:
         """S, H0, P, W ([N, N]) and orbital energies / occupations ([N]) of
@@ -247,7 +252,7 @@ class ResidentBatch:
         def addr(p):
             return ctypes.cast(p, ctypes.c_void_p).value
         return {k: addr(getattr(out, k)) for k in ("terms", "gradient", "shell_charges", "atomic_charges", "dipole",
-                                                   "fermi_level", "iterations", "status")}
+                                                   "fermi_level", "iterations", "status", "rung")}
 
     def download(self) -> BatchResult:
         L = _lib.load()
@@ -260,14 +265,15 @@ class ResidentBatch:
         fermi = np.zeros(self.nmol)
         iters = np.zeros(self.nmol, dtype=np.int32)
         status = np.zeros(self.nmol, dtype=np.int32)
+        rung = np.zeros(self.nmol, dtype=np.int32)
         out = _lib.Outputs(_lib.ptr(energy), _lib.ptr(terms), _lib.ptr(grad), _lib.ptr(qsh), _lib.ptr(qat),
                            _lib.ptr(dip), _lib.ptr(fermi), _lib.ptr(iters, ctypes.c_int32),
-                           _lib.ptr(status, ctypes.c_int32))
+                           _lib.ptr(status, ctypes.c_int32), _lib.ptr(rung, ctypes.c_int32))
         rc = L.gfn1_batch_download(self.handle, ctypes.byref(out))
         if rc not in (0, 3, 4, 8, 12):
             _lib.check(rc, self.calc.engine.handle)
         shoff = self.calc.shell_offsets(self.atom_offsets, self.numbers)
-        return BatchResult(energy, terms, grad, qsh, qat, dip, fermi, iters, status, self.atom_offsets, shoff)
+        return BatchResult(energy, terms, grad, qsh, qat, dip, fermi, iters, status, self.atom_offsets, shoff, rung)
 
 
 __all__ = ["BatchCalculator", "BatchResult", "ResidentBatch", "unit_scale"]

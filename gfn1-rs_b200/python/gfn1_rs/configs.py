@@ -13,8 +13,9 @@
   1000 + i), semi-numerical Hessians through gfn1_rs.hessian.hessian_batch
   (6N displaced gradients per molecule, batched).
 
-Each line is JSON: evals/s, SCC iterations and, for the guess modes, the
-largest energy difference to the zero-guess run.
+Each line is JSON: evals/s, SCC iterations, frames per fallback-ladder rung
+(trajectories) and, for the guess modes, the largest energy difference to the
+zero-guess run.
 """
 from __future__ import annotations
 
@@ -95,7 +96,7 @@ def trajectories(frames: int, batch: int):
         print(json.dumps({"workload": f"water96 trajectory, {frames} frames in batches of {batch}", "mode": mode,
                           "evals_per_s": frames / r["seconds"], "iterations_mean": float(r["iterations"].mean()),
                           "iterations_p95": float(np.percentile(r["iterations"], 95)),
-                          "failed": int((r["status"] != 0).sum()),
+                          "failed": int((r["status"] != 0).sum()), "rungs": trajectory.rung_usage(r["rung"]),
                           "max_abs_dE_vs_plain": float(np.abs(r["energy"] - ref["energy"]).max())}), flush=True)
 
 

@@ -29,7 +29,8 @@ MODES = ("plain", "learned", "previous", "learned+previous")
 def run_trajectory(numbers, frames_bohr, batch: int = 64, mode: str = "learned+previous", calc=None,
                    guess=None, compute_gradient: bool = True) -> dict:
     """frames_bohr: [F, nat, 3].  Returns per-frame energies, iterations,
-    statuses, gradients (if requested) and the wall time of the engine calls."""
+    statuses, fallback-ladder rungs, gradients (if requested) and the wall time
+    of the engine calls."""
     from .batch import BatchCalculator
     if mode not in MODES:
         raise ValueError(f"mode must be one of {MODES}")
@@ -44,6 +45,7 @@ def run_trajectory(numbers, frames_bohr, batch: int = 64, mode: str = "learned+p
     energy = np.zeros(nf)
     iters = np.zeros(nf, dtype=np.int32)
     status = np.zeros(nf, dtype=np.int32)
+    rung = np.zeros(nf, dtype=np.int32)
     grads = np.zeros((nf, nat, 3)) if compute_gradient else None
     last_q = None      # converged shell charges of the last frame of the previous batch
     last_corr = None   # converged minus learned guess of that frame
@@ -71,14 +73,23 @@ def run_trajectory(numbers, frames_bohr, batch: int = 64, mode: str = "learned+p
         energy[b0:b1] = res.energy
         iters[b0:b1] = res.iterations
         status[b0:b1] = res.status
+        rung[b0:b1] = res.rung
         if compute_gradient:
             grads[b0:b1] = res.gradient.reshape(k, nat, 3)
         qs = res.shell_charges.reshape(k, nsh_atom)
         last_q = qs[-1].copy()
         if learned_q is not None:
             last_corr = qs[-1] - learned_q[-1]
-    return {"energy": energy, "iterations": iters, "status": status, "gradient": grads, "seconds": seconds,
-            "mode": mode, "batch": batch}
+    return {"energy": energy, "iterations": iters, "status": status, "rung": rung, "gradient": grads,
+            "seconds": seconds, "mode": mode, "batch": batch}
+
+
+def rung_usage(rung) -> dict:
+    """Frames per fallback-ladder rung ("0".."3"; "none" = not converged)."""
+    rung = np.asarray(rung)
+    out = {str(k): int(np.sum(rung == k)) for k in range(4)}
+    out["none"] = int(np.sum(rung < 0))
+    return out
 
 
 def main():
@@ -102,7 +113,7 @@ def main():
             ref = r
         out[mode] = {"evals_per_s": a.frames / r["seconds"], "iterations_mean": float(r["iterations"].mean()),
                      "iterations_p95": float(np.percentile(r["iterations"], 95)),
-                     "failed": int((r["status"] != 0).sum()),
+                     "failed": int((r["status"] != 0).sum()), "rungs": rung_usage(r["rung"]),
                      "max_abs_dE_vs_plain": float(np.abs(r["energy"] - ref["energy"]).max())}
         print(mode, json.dumps(out[mode]), flush=True)
 

@@ -69,6 +69,9 @@ typedef struct gfn1_outputs {
   double* fermi_level;    /* [nmol] */
   int32_t* iterations;    /* [nmol] */
   int32_t* status;        /* [nmol] per-molecule status code */
+  int32_t* rung;          /* [nmol] rung of the fallback ladder (src/electronic.rs:1390-1447) whose SCC
+                             converged: 0 = the requested scheme, 1 and 2 = linear mixing with a level
+                             shift, 3 = T_el raised to max(T_el, 3000 K); -1 where status is not 0 */
 } gfn1_outputs;
 
 /* Fills the ElectronicOptions defaults. */
@@ -148,7 +151,8 @@ int gfn1_batch_download(gfn1_batch* b, const gfn1_outputs* out);
  * last launch (waits for the device first). */
 int gfn1_batch_molecule_matrices(gfn1_batch* b, int m, double* S, double* H0, double* P, double* W, double* eps,
                                  double* occ);
-/* Device pointers of the batch-owned result arrays (valid until destroy). */
+/* Device pointers of the batch-owned result arrays (valid until destroy);
+ * there `rung` is meaningful where `status` is 0. */
 int gfn1_batch_outputs_device(gfn1_batch* b, gfn1_outputs* out);
 /* Sizes of the batch: natoms, nshells, total AOs; launches = kernels per run. */
 int gfn1_batch_info(const gfn1_batch* b, int64_t* natoms, int64_t* nshells, int64_t* naos, int32_t* launches);
@@ -162,6 +166,8 @@ int gfn1_batch_info(const gfn1_batch* b, int64_t* natoms, int64_t* nshells, int6
  * exit; host staging uses the stack.  Limits: at most 64 atoms, 128 AOs,
  * 128 shells and 250 Broyden history vectors (min(scc_broyden_size, max_scc));
  * larger inputs return GFN1_E_INVALID_INPUT with a message naming the limit.
+ * Only rung 0 of the fallback ladder runs here: a molecule that needs the
+ * later rungs returns GFN1_E_SCC_NOT_CONVERGED.
  * The first call on a device looks up the array's device address (once per
  * device, that device current); make that first call before any stream
  * capture.  Every call reuses the same array, so calls that overlap on the GPU

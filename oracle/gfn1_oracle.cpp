@@ -1241,6 +1241,8 @@ struct Result {
   Vec3 dipole;
   int iterations = 0;
   bool converged = false;
+  int rung = -1;       // fallback-ladder attempt that converged (src/electronic.rs:1420)
+  double etemp = 0.0;  // electronic temperature of that attempt (src/electronic.rs:2024-2026)
   double fermi = 0, nelec = 0, rms = 0;
   Mat S, H0, P, W;
   int nao = 0, nsh = 0;
@@ -1408,8 +1410,10 @@ Result run(const System& sys, const Options& opt, const double* init_q, bool wan
     for (size_t k = 0; k < P.a.size(); ++k) s += H0.a[k] * P.a[k];
     return s;
   };
+  int rung_used = -1;
   for (int attempt = 0; attempt < 4 && !converged; ++attempt) {
     const Rung& rg = ladder[attempt];
+    rung_used = attempt;
     std::vector<double> vmix(nsh, 0.0);
     if (init_q) for (int i = 0; i < nsh; ++i) vmix[i] = init_q[i];
     Broyden br(nsh, std::max(opt.scc_broyden_size, 2), rg.mix);
@@ -1470,6 +1474,8 @@ Result run(const System& sys, const Options& opt, const double* init_q, bool wan
   double t[15] = {total_free, total_internal, erep, eel, sc.e2, sc.e3, 0.0, edisp, ehal, 0.0, 0.0, 0.0, 0.0, 0.0, last.ts};
   std::memcpy(res.terms, t, sizeof t);
   res.converged = true;
+  res.rung = rung_used;
+  res.etemp = ladder[rung_used].etemp;
   res.shell_q = last.q;
   res.atom_q = sc.qat;
   res.eps = last.eps;
@@ -1669,7 +1675,7 @@ int oracle_halogen(int nat, const int* z, const double* xyz_bohr, double* energy
 int oracle_run(int nat, const int* z, const double* xyz_bohr, const oracle_options* o, const double* init_shell_q,
                int want_grad, double* terms, double* grad, double* shell_q, double* atom_q, double* eps,
                double* occ, double* dipole, double* cn, int* iterations, int* converged, double* fermi, double* S,
-               double* H0, double* P, double* W) {
+               double* H0, double* P, double* W, int* rung, double* etemp_used) {
   try {
     System s;
     s.z.assign(z, z + nat);
@@ -1693,6 +1699,8 @@ int oracle_run(int nat, const int* z, const double* xyz_bohr, const oracle_optio
     if (H0) std::copy(r.H0.a.begin(), r.H0.a.end(), H0);
     if (P) std::copy(r.P.a.begin(), r.P.a.end(), P);
     if (W) std::copy(r.W.a.begin(), r.W.a.end(), W);
+    if (rung) *rung = r.rung;
+    if (etemp_used) *etemp_used = r.etemp;
     return OK;
   } catch (const OracleError& e) {
     t_err = e.what();
@@ -1708,7 +1716,7 @@ int oracle_run(int nat, const int* z, const double* xyz_bohr, const oracle_optio
 // null) places each molecule's shell charges in shell_q.
 int oracle_run_batch(int nmol, const int* atom_offsets, const int* z, const double* xyz_bohr, const double* charge,
                      const oracle_options* o, int want_grad, int nthreads, double* energy, double* grad,
-                     const int* shell_offsets, double* shell_q, int* iterations, int* status) {
+                     const int* shell_offsets, double* shell_q, int* iterations, int* status, int* rungs) {
   std::atomic<int> next(0), worst(OK);
   auto worker = [&]() {
     for (;;) {
@@ -1733,12 +1741,14 @@ int oracle_run_batch(int nmol, const int* atom_offsets, const int* z, const doub
           }
         if (shell_q && shell_offsets) std::copy(r.shell_q.begin(), r.shell_q.end(), shell_q + shell_offsets[m]);
         if (iterations) iterations[m] = r.iterations;
+        if (rungs) rungs[m] = r.rung;
       } catch (const OracleError& e) {
         code = e.code;
       } catch (const std::exception&) {
         code = E_INVALID_INPUT;
       }
       if (status) status[m] = code;
+      if (rungs && code != OK) rungs[m] = -1;
       int w = worst.load();
       while (code > w && !worst.compare_exchange_weak(w, code)) {
       }

@@ -10,6 +10,7 @@ from __future__ import annotations
 import ctypes
 import os
 import subprocess
+import threading
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -73,6 +74,8 @@ class OracleResult:
     iterations: int
     converged: bool
     fermi_level: float
+    rung: int = 0                        # fallback-ladder attempt that converged (0 = the requested scheme)
+    electronic_temperature: float = 0.0  # T_el of that attempt (raised on rung 3)
     S: np.ndarray | None = None
     H0: np.ndarray | None = None
     P: np.ndarray | None = None
@@ -81,6 +84,7 @@ class OracleResult:
 
 
 _lib = None
+_lib_lock = threading.Lock()
 
 
 def build(force: bool = False) -> str:
@@ -93,6 +97,12 @@ def build(force: bool = False) -> str:
 
 def lib():
     global _lib
+    with _lib_lock:  # first use from several threads: load and initialise once
+        return _load()
+
+
+def _load():
+    global _lib
     if _lib is None:
         build()
         L = ctypes.CDLL(LIB_PATH)
@@ -102,10 +112,10 @@ def lib():
         L.oracle_last_error.restype = ctypes.c_char_p
         L.oracle_sizes.argtypes = [ctypes.c_int, ip, ip, ip]
         L.oracle_run.argtypes = [ctypes.c_int, ip, dp, ctypes.POINTER(OracleOptions), dp, ctypes.c_int,
-                                 dp, dp, dp, dp, dp, dp, dp, dp, ip, ip, dp, dp, dp, dp, dp]
+                                 dp, dp, dp, dp, dp, dp, dp, dp, ip, ip, dp, dp, dp, dp, dp, ip, dp]
         L.oracle_halogen.argtypes = [ctypes.c_int, ip, dp, dp, dp]
         L.oracle_run_batch.argtypes = [ctypes.c_int, ip, ip, dp, dp, ctypes.POINTER(OracleOptions), ctypes.c_int,
-                                       ctypes.c_int, dp, dp, ip, dp, ip, ip]
+                                       ctypes.c_int, dp, dp, ip, dp, ip, ip, ip]
         rc = L.oracle_init(TABLES_PATH.encode())
         if rc != 0:
             raise OracleError(rc, L.oracle_last_error().decode())
@@ -151,17 +161,20 @@ def run(numbers, positions_bohr, options: OracleOptions | None = None, gradient:
     it = ctypes.c_int()
     conv = ctypes.c_int()
     fermi = ctypes.c_double()
+    rung = ctypes.c_int()
+    etemp = ctypes.c_double()
     mats = [np.zeros((nao, nao)) for _ in range(4)] if matrices else [None] * 4
     q0 = None if init_shell_charges is None else np.ascontiguousarray(init_shell_charges, dtype=np.float64)
     rc = L.oracle_run(nat, _ip(z), _dp(xyz), ctypes.byref(opt), _dp(q0), int(gradient), _dp(terms), _dp(grad),
                       _dp(qsh), _dp(qat), _dp(eps), _dp(occ), _dp(dip), _dp(cn), ctypes.byref(it),
-                      ctypes.byref(conv), ctypes.byref(fermi), *[_dp(m) for m in mats])
+                      ctypes.byref(conv), ctypes.byref(fermi), *[_dp(m) for m in mats], ctypes.byref(rung),
+                      ctypes.byref(etemp))
     if rc != 0:
         raise OracleError(rc, L.oracle_last_error().decode())
     return OracleResult(terms=dict(zip(TERM_NAMES, terms.tolist())), energy=float(terms[0]), gradient=grad,
                         shell_charges=qsh, atomic_charges=qat, orbital_energies=eps, occupations=occ,
                         dipole=dip, coordination_numbers=cn, iterations=it.value, converged=bool(conv.value),
-                        fermi_level=fermi.value, S=mats[0], H0=mats[1], P=mats[2], W=mats[3])
+                        fermi_level=fermi.value, rung=rung.value, electronic_temperature=etemp.value, S=mats[0], H0=mats[1], P=mats[2], W=mats[3])
 
 
 def halogen(numbers, positions_bohr, gradient: bool = True):
@@ -178,9 +191,11 @@ def halogen(numbers, positions_bohr, gradient: bool = True):
 
 
 def run_batch(atom_offsets, numbers, positions_bohr, charges=None, options: OracleOptions | None = None,
-              gradient: bool = True, nthreads: int = 0):
+              gradient: bool = True, nthreads: int = 0, with_rungs: bool = False):
     """Host-thread batch over molecules (one molecule per thread).  Returns
-    (energy[nmol], grad[natoms,3], shell_q (concatenated), iterations, status)."""
+    (energy[nmol], grad[natoms,3], shell_q (concatenated), shell offsets,
+    iterations, status), plus the fallback-ladder rung of each molecule (-1
+    where it did not converge) with ``with_rungs``."""
     L = lib()
     off = np.ascontiguousarray(atom_offsets, dtype=np.int32)
     z = np.ascontiguousarray(numbers, dtype=np.int32)
@@ -195,7 +210,10 @@ def run_batch(atom_offsets, numbers, positions_bohr, charges=None, options: Orac
     qsh = np.zeros(int(shell_off[-1]))
     iters = np.zeros(nmol, dtype=np.int32)
     status = np.zeros(nmol, dtype=np.int32)
+    rungs = np.zeros(nmol, dtype=np.int32)
     opt = options if options is not None else make_options()
     L.oracle_run_batch(nmol, _ip(off), _ip(z), _dp(xyz), _dp(ch), ctypes.byref(opt), int(gradient), int(nthreads),
-                       _dp(energy), _dp(grad), _ip(shell_off), _dp(qsh), _ip(iters), _ip(status))
+                       _dp(energy), _dp(grad), _ip(shell_off), _dp(qsh), _ip(iters), _ip(status), _ip(rungs))
+    if with_rungs:
+        return energy, grad, qsh, shell_off, iters, status, rungs
     return energy, grad, qsh, shell_off, iters, status

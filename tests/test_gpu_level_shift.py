@@ -36,6 +36,8 @@ def test_level_shift_matches_oracle(gpu_calc, oracle_mod, fixtures, shift):
         assert np.max(np.abs(r.gradient[a0:a1] - o.gradient)) <= 1e-5, NAMES[m]
         # the shift moves the path, not the fixed point
         assert abs(r.energy[m] - plain.energy[m]) <= 1e-6, NAMES[m]
+        # ferrocene at 0.3 Eh: rung 0 needs 519 iterations (oracle), so rung 1 converges it
+        assert r.rung[m] == o.rung and plain.rung[m] == 0, NAMES[m]
 
 
 def test_level_shift_rejected_on_the_large_molecule_path(gpu_calc, fixtures):

@@ -126,7 +126,7 @@ def test_not_converged_status_matches_oracle(calc, oracle_mod, fixtures):
     with pytest.raises(oracle_mod.OracleError) as ei:
         oracle_mod.run(z, x, options=oracle_mod.make_options(**opts), gradient=False)
     assert ei.value.code == 8
-    assert r.status[0] == 8
+    assert r.status[0] == 8 and r.rung[0] == -1
     assert r.iterations[0] == 250  # the last rung's limit, max(max_scc, 250)
 
 
@@ -144,6 +144,7 @@ def test_fallback_ladder_matches_oracle(calc, oracle_mod, fixtures, name):
     assert np.abs(r.gradient - o.gradient).max() <= G_TOL
     assert np.abs(r.shell_charges - o.shell_charges).max() <= Q_TOL
     assert r.iterations[0] == o.iterations
+    assert r.rung[0] == o.rung == 1  # linear mixing 0.2 with a 0.2 Eh level shift
 
 
 def test_fallback_ladder_in_a_batch(calc, oracle_mod, fixtures):
@@ -162,6 +163,8 @@ def test_fallback_ladder_in_a_batch(calc, oracle_mod, fixtures):
         o = oracle_mod.run(z, x, options=oracle_mod.make_options(max_scc=7), gradient=False)
         assert abs(r.energy[k] - o.energy) <= E_TOL
         assert r.iterations[k] == o.iterations
+        assert r.rung[k] == o.rung  # 1 for caffeine, 0 for the others
+    assert r.rung.tolist() == [0, 0, 0, 1]
 
 
 def test_charged_molecule(calc, oracle_mod, fixtures):

@@ -19,6 +19,8 @@ def test_trajectory_modes_agree_and_save_iterations(gpu_calc):
     for m, r in res.items():
         assert np.all(r["status"] == 0), m
         assert np.abs(r["energy"] - plain["energy"]).max() <= 1e-6, m
+        usage = trajectory.rung_usage(r["rung"])
+        assert sum(usage.values()) == len(frames) and usage["none"] == 0, m
     it = {m: r["iterations"].mean() for m, r in res.items()}
     print("mean iterations", it)
     assert it["learned"] < it["plain"]

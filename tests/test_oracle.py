@@ -113,10 +113,26 @@ def test_robust_ladder_recovers(oracle_mod, fixtures):
     """max_scc = 1 fails rung 0; the linear-mixing + level-shift rungs of the
     fallback ladder (src/electronic.rs:1390-1447) converge to the same energy."""
     z, x = smoke_molecule(fixtures, "water")
-    ref = oracle_mod.run(z, x, gradient=False).energy
+    r0 = oracle_mod.run(z, x, gradient=False)
+    assert r0.rung == 0 and r0.electronic_temperature == 300.0
     r = oracle_mod.run(z, x, options=oracle_mod.make_options(max_scc=1), gradient=False)
     assert r.converged and r.iterations > 1
-    assert abs(r.energy - ref) < 1e-6
+    assert r.rung == 1 and r.electronic_temperature == 300.0  # linear mixing 0.2 + level shift 0.2 Eh
+    assert abs(r.energy - r0.energy) < 1e-6
+
+
+def test_ladder_rungs_in_a_batch(oracle_mod, fixtures):
+    """Per-molecule rungs from the threaded batch: rung 1 where max_scc = 1
+    stops rung 0, -1 (with status SccNotConverged) where no rung converges."""
+    z, x = smoke_molecule(fixtures, "water")
+    off = np.array([0, len(z), 2 * len(z)], dtype=np.int32)
+    zz, xx = np.concatenate([z, z]), np.concatenate([x, x])
+    out = oracle_mod.run_batch(off, zz, xx, options=oracle_mod.make_options(max_scc=1), gradient=False,
+                               with_rungs=True)
+    assert out[-1].tolist() == [1, 1] and out[5].tolist() == [0, 0]
+    stuck = oracle_mod.make_options(max_scc=2, energy_tolerance=0.0, charge_tolerance=0.0)
+    out = oracle_mod.run_batch(off, zz, xx, options=stuck, gradient=False, with_rungs=True)
+    assert out[-1].tolist() == [-1, -1] and out[5].tolist() == [8, 8]
 
 
 def test_charged_h2_cation_aufbau(oracle_mod):
