@@ -1,0 +1,54 @@
+"""Oracle results on sample frames of the 96-water trajectory, written to
+trajectory_rungs.json.
+
+Frames 64, 128, 192 and 255 of the 96-water free-flight trajectory (seed 2,
+velocities seed 3, 0.5 fs steps, 0.002 A noise; 288 atoms, 768 AOs) at the
+default SCC options, the ones the trajectory workload runs with.  Per frame:
+the fallback-ladder rung that converged (src/electronic.rs:1390-1447), the
+iterations of that rung, the energy and the electronic temperature used.  The
+frames drift apart (no forces), so later frames need more SCC iterations; the
+record shows which rung the reference's ladder settles on for them.
+Run: python tests/golden/make_trajectory_rungs.py (CPU only; one thread per
+frame, about ten minutes).
+"""
+import json
+import os
+import sys
+import time
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "gfn1-rs_b200", "python"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import oracle  # noqa: E402
+from gfn1_rs import workloads  # noqa: E402
+
+A2B = 1.8897261246257702
+FRAMES = (64, 128, 192, 255)
+
+
+def record(z, x_ang):
+    t0 = time.time()
+    o = oracle.run(z, x_ang * A2B, gradient=False)
+    return {"positions_angstrom": np.asarray(x_ang).round(12).tolist(), "energy": o.energy,
+            "iterations": int(o.iterations), "rung": int(o.rung),
+            "electronic_temperature": o.electronic_temperature, "seconds": round(time.time() - t0, 1)}
+
+
+def main():
+    z, x = workloads.water_trajectory(96, frames=max(FRAMES) + 1)
+    oracle.lib()
+    with ThreadPoolExecutor(len(FRAMES)) as ex:
+        recs = list(ex.map(lambda f: record(z, x[f]), FRAMES))
+    out = {"numbers": [int(v) for v in z], "frames": dict(zip((str(f) for f in FRAMES), recs))}
+    print({f: (r["rung"], r["iterations"], r["seconds"]) for f, r in out["frames"].items()}, flush=True)
+    with open(os.path.join(HERE, "trajectory_rungs.json"), "w") as f:
+        json.dump(out, f)
+
+
+if __name__ == "__main__":
+    main()
