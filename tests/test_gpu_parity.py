@@ -49,6 +49,14 @@ def test_h2_golden_on_gpu(calc, fixtures):
     assert np.max(np.abs(r.gradient - np.array(g["gradient"]))) < 1e-7
 
 
+def test_d3_h2_known_answer_on_gpu(calc):
+    """D3(BJ) term of H2 at 0.74 A: the reference's known answer
+    -3.5462980e-5 Eh (src/dispersion.rs:3389-3396, tolerance 5e-10 Eh)."""
+    x = np.array([[0.0, 0.0, 0.0], [0.74, 0.0, 0.0]]) * ANGSTROM_TO_BOHR
+    r = calc.calculate_flat([0, 2], [1, 1], x, raise_on_error=True)
+    assert abs(r.terms[0, 7] - -0.000035462980) < 5e-10
+
+
 @pytest.mark.parametrize("name", ["hydrogen", "hydrogen fluoride", "water", "borane", "caffeine"])
 def test_reference_molecules(calc, oracle_mod, fixtures, name):
     z, x = smoke_molecule(fixtures, name)

@@ -24,6 +24,17 @@ def test_h2_golden(oracle_mod, fixtures):
     assert np.max(np.abs(r.gradient - np.array(g["gradient"]))) < 1e-7
 
 
+# D3(BJ) energy of H2 at 0.74 A with the GFN1 parameters, the reference's
+# known answer (src/dispersion.rs:3389-3396, tolerance 5e-10 Eh there)
+D3_H2_074 = -0.000035462980
+
+
+def test_d3_h2_known_answer(oracle_mod):
+    x = np.array([[0.0, 0.0, 0.0], [0.74, 0.0, 0.0]]) * ANGSTROM_TO_BOHR
+    r = oracle_mod.run([1, 1], x, gradient=False)
+    assert abs(r.terms["dispersion"] - D3_H2_074) < 5e-10
+
+
 def test_h2_gradient_is_exact_derivative(oracle_mod, fixtures):
     g = fixtures["h2_engrad"]
     opt = oracle_mod.make_options(energy_tolerance=1e-12, charge_tolerance=1e-10)
