@@ -201,6 +201,16 @@ class Engine:
             self._elem_sizes = (nao, nsh)
         return self._elem_sizes
 
+    def shell_count_table(self) -> np.ndarray:
+        """Shells per atom for each uint8 atomic number (0 where the device path
+        lacks the element, as the C side counts them)."""
+        if getattr(self, "_nsh_u8", None) is None:
+            nsh = self.element_sizes()[1]
+            table = np.zeros(256, dtype=np.int64)
+            table[1:87] = np.maximum(nsh[1:87], 0)
+            self._nsh_u8 = table
+        return self._nsh_u8
+
     def basis_size(self, numbers) -> tuple[int, int]:
         z = np.ascontiguousarray(numbers, dtype=np.uint8)
         nao, nsh = ctypes.c_int32(), ctypes.c_int32()

@@ -92,12 +92,14 @@ class BatchCalculator:
 
     @staticmethod
     def shell_offsets_for(engine, atom_offsets, numbers) -> np.ndarray:
-        off = np.asarray(atom_offsets, dtype=np.int64)
-        z = np.asarray(numbers, dtype=np.int64)
-        nsh_z = engine.element_sizes()[1]
-        per_atom = np.where((z >= 1) & (z <= 86), nsh_z[np.clip(z, 0, 86)], 0)
-        cum = np.concatenate([[0], np.cumsum(np.maximum(per_atom, 0))])
-        return cum[off]
+        # one table lookup per atom over the uint8 atomic numbers the C side receives
+        table = engine.shell_count_table()
+        z = np.asarray(numbers)
+        if z.dtype != np.uint8:
+            z = z.astype(np.uint8)
+        cum = np.zeros(len(z) + 1, dtype=np.int64)
+        np.cumsum(table[z], out=cum[1:])
+        return cum[np.asarray(atom_offsets)]
 
     def calculate_flat(self, atom_offsets, numbers, xyz_bohr, charges=None, initial_shell_charges=None,
                        compute_gradient=True, raise_on_error=False) -> BatchResult:
