@@ -79,10 +79,12 @@ def load():
         L = ctypes.CDLL(LIB_PATH)
         vp = ctypes.c_void_p
         L.gfn1_default_options.argtypes = [ctypes.POINTER(Options)]
+        L.gfn1_default_options.restype = None
         L.gfn1_last_error.argtypes = [vp]
         L.gfn1_last_error.restype = ctypes.c_char_p
         L.gfn1_engine_create.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(vp)]
         L.gfn1_engine_destroy.argtypes = [vp]
+        L.gfn1_engine_destroy.restype = None
         L.gfn1_basis_size.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_uint8), _ip, _ip]
         L.gfn1_run.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_uint8), _dp, ctypes.c_double, _dp,
                                ctypes.POINTER(Options), ctypes.POINTER(Outputs)]
@@ -91,6 +93,7 @@ def load():
         L.gfn1_batch_create.argtypes = [vp, ctypes.c_int, _ip, ctypes.POINTER(ctypes.c_uint8), _dp,
                                         ctypes.POINTER(Options), ctypes.POINTER(vp)]
         L.gfn1_batch_destroy.argtypes = [vp]
+        L.gfn1_batch_destroy.restype = None
         L.gfn1_batch_set_positions.argtypes = [vp, vp, ctypes.c_int]
         L.gfn1_batch_set_initial_charges.argtypes = [vp, vp, ctypes.c_int]
         L.gfn1_batch_launch.argtypes = [vp, vp]
