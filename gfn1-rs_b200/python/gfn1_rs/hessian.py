@@ -111,7 +111,9 @@ def hessian_batch(calc, atom_offsets, numbers, xyz_bohr, charges=None, step: flo
         mols = []
         for m in range(nmol):
             s0, s1 = r0.shell_offsets[m], r0.shell_offsets[m + 1]
-            q = r0.shell_charges[s0:s1].copy() if warm_start and r0.status[m] == 0 else None
+            q = None
+            if warm_start:  # a molecule that failed at R starts from zero charges, the others stay warm
+                q = r0.shell_charges[s0:s1].copy() if r0.status[m] == 0 else np.zeros(s1 - s0)
             mols.append((m, z[off[m]:off[m + 1]], x[off[m]:off[m + 1]], q))
 
         def evaluate(items):
