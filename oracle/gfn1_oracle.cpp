@@ -1670,6 +1670,29 @@ int oracle_halogen(int nat, const int* z, const double* xyz_bohr, double* energy
   }
 }
 
+// One classical term alone, energy and (grad not null) gradient [nat*3]:
+// which = 0 repulsion (src/repulsion.rs:24-59, 139-159), 1 D3(BJ) dispersion
+// (src/dispersion.rs:1232-1360), 2 halogen bonds (src/halogen.rs:64-160).
+// The per-term split of the reference's gradient probe
+// (tests/gradient_fd_probe.rs:41-120).
+int oracle_classical_term(int which, int nat, const int* z, const double* xyz_bohr, double* energy, double* grad) {
+  try {
+    if (which < 0 || which > 2) throw OracleError(E_INVALID_INPUT, "unknown classical term");
+    System s;
+    s.z.assign(z, z + nat);
+    for (int a = 0; a < nat; ++a) s.pos.push_back(Vec3(xyz_bohr[3 * a], xyz_bohr[3 * a + 1], xyz_bohr[3 * a + 2]));
+    std::vector<Vec3> g(nat);
+    std::vector<Vec3>* gp = grad ? &g : nullptr;
+    *energy = which == 0 ? repulsion(s, gp) : which == 1 ? dispersion(s, gp) : halogen(s, gp);
+    if (grad)
+      for (int a = 0; a < nat; ++a) { grad[3 * a] = g[a].x; grad[3 * a + 1] = g[a].y; grad[3 * a + 2] = g[a].z; }
+    return OK;
+  } catch (const OracleError& e) {
+    t_err = e.what();
+    return e.code;
+  }
+}
+
 // One molecule.  Output pointers may be null.  terms[15] in the order of
 // EnergyTerms::named_values (src/electronic.rs:681-699).
 int oracle_run(int nat, const int* z, const double* xyz_bohr, const oracle_options* o, const double* init_shell_q,

@@ -114,6 +114,7 @@ def _load():
         L.oracle_run.argtypes = [ctypes.c_int, ip, dp, ctypes.POINTER(OracleOptions), dp, ctypes.c_int,
                                  dp, dp, dp, dp, dp, dp, dp, dp, ip, ip, dp, dp, dp, dp, dp, ip, dp]
         L.oracle_halogen.argtypes = [ctypes.c_int, ip, dp, dp, dp]
+        L.oracle_classical_term.argtypes = [ctypes.c_int, ctypes.c_int, ip, dp, dp, dp]
         L.oracle_run_batch.argtypes = [ctypes.c_int, ip, ip, dp, dp, ctypes.POINTER(OracleOptions), ctypes.c_int,
                                        ctypes.c_int, dp, dp, ip, dp, ip, ip, ip]
         rc = L.oracle_init(TABLES_PATH.encode())
@@ -185,6 +186,23 @@ def halogen(numbers, positions_bohr, gradient: bool = True):
     e = np.zeros(1)
     g = np.zeros((len(z), 3)) if gradient else None
     rc = L.oracle_halogen(len(z), _ip(z), _dp(x), _dp(e), _dp(g))
+    if rc != 0:
+        raise OracleError(rc, L.oracle_last_error().decode())
+    return float(e[0]), g
+
+
+CLASSICAL_TERMS = ("repulsion", "dispersion", "halogen")
+
+
+def classical_term(name: str, numbers, positions_bohr, gradient: bool = True):
+    """Energy (Eh) and gradient (Eh/bohr) of one classical term alone:
+    "repulsion", "dispersion" (D3(BJ)) or "halogen"."""
+    L = lib()
+    z = np.ascontiguousarray(numbers, dtype=np.int32)
+    x = np.ascontiguousarray(positions_bohr, dtype=np.float64).reshape(-1, 3)
+    e = np.zeros(1)
+    g = np.zeros((len(z), 3)) if gradient else None
+    rc = L.oracle_classical_term(CLASSICAL_TERMS.index(name), len(z), _ip(z), _dp(x), _dp(e), _dp(g))
     if rc != 0:
         raise OracleError(rc, L.oracle_last_error().decode())
     return float(e[0]), g
