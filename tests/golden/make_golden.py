@@ -7,7 +7,9 @@ Sources (gfn1-rs v0.5.1):
 * the molecules embedded in tests/nonpbc_smoke.rs:14-50 (H/C/N/O/F/B/P subset),
   read as text;
 * the halogen-bond test systems embedded in src/halogen.rs (its unit tests,
-  from :788), keyed by their xyz title line.
+  from :788), keyed by their xyz title line;
+* the molecules of tests/scf_accelerators.rs:10-20 (water, 2-bromoethanol),
+  keyed by their constant's name in lower case.
 
 Run where the reference tree is available:
     python tests/golden/make_golden.py /path/to/gfn1-rs
@@ -75,6 +77,12 @@ def main(root: str) -> None:
             continue
         hal.setdefault(title, read_xyz_text(text))
     out["halogen_tests"] = hal
+    acc = {}
+    src = (root / "tests/scf_accelerators.rs").read_text()
+    for m in re.finditer(r'const (\w+): &str = "((?:[^"\\]|\\.)*)";', src, re.S):
+        lit = re.sub(r"\\\n\s*", "", m.group(2))  # Rust line continuations
+        acc[m.group(1).lower()] = read_xyz_text(lit.encode().decode("unicode_escape"))
+    out["scf_accelerators"] = acc
     dest = Path(__file__).with_name("reference_fixtures.json")
     dest.write_text(json.dumps(out, indent=1) + "\n")
 

@@ -7,7 +7,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import smoke_molecule
+from conftest import ANGSTROM_TO_BOHR, smoke_molecule
 
 pytestmark = pytest.mark.gpu
 
@@ -69,3 +69,27 @@ def test_native_calculator_level_shift(gpu_calc, oracle_mod, fixtures):
                                                          compute_gradient=True)
     o = oracle_mod.run(z, x, options=oracle_mod.make_options(level_shift=0.25))
     assert r.converged and abs(r.energy_hartree - o.energy) <= 1e-6
+
+
+def test_accelerator_consistency_on_gpu(gpu_calc, oracle_mod, fixtures):
+    """tests/scf_accelerators.rs:41-75 on its own molecules (water,
+    2-bromoethanol) and options (1e-9 Eh, 1e-8 e, max_scc 1000): Broyden,
+    linear mixing and a 0.15 Eh level shift on the device each land on the
+    oracle's Broyden energy (1e-6 Eh), and linear on Broyden's (1e-7 Eh), all
+    on rung 0."""
+    from gfn1_rs import BatchCalculator
+
+    accel = dict(energy_tolerance=1e-9, charge_tolerance=1e-8, max_scc=1000)
+    mols = []
+    for name in ("water", "bromoethanol"):
+        rec = fixtures["scf_accelerators"][name]
+        mols.append((np.array(rec["numbers"]), np.array(rec["positions_angstrom"]) * ANGSTROM_TO_BOHR))
+    off, z, x = _flat(mols)
+    runs = {k: BatchCalculator(**kw, **accel).calculate_flat(off, z, x, compute_gradient=False)
+            for k, kw in (("broyden", {}), ("linear", dict(scc_broyden=False)), ("shift", dict(level_shift=0.15)))}
+    for m, (zm, xm) in enumerate(mols):
+        o = oracle_mod.run(zm, xm, options=oracle_mod.make_options(**accel), gradient=False)
+        for k, r in runs.items():
+            assert r.status[m] == 0 and r.rung[m] == 0, (m, k)
+            assert abs(r.energy[m] - o.energy) <= 1e-6, (m, k)
+        assert abs(runs["linear"].energy[m] - runs["broyden"].energy[m]) < 1e-7, m

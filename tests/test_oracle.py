@@ -85,6 +85,23 @@ def test_mixer_independence(oracle_mod, fixtures):
     assert abs(eb - el) < 1e-7
 
 
+ACCEL = dict(energy_tolerance=1e-9, charge_tolerance=1e-8, max_scc=1000)
+
+
+@pytest.mark.parametrize("name", ["water", "bromoethanol"])
+def test_accelerator_consistency(oracle_mod, fixtures, name):
+    """tests/scf_accelerators.rs:41-75 on its own molecules and options:
+    linear mixing lands on Broyden's energy (1e-7 Eh) and a 0.15 Eh level
+    shift does not move it (1e-6 Eh)."""
+    rec = fixtures["scf_accelerators"][name]
+    z, x = rec["numbers"], np.array(rec["positions_angstrom"]) * ANGSTROM_TO_BOHR
+    e = {k: oracle_mod.run(z, x, options=oracle_mod.make_options(**kw, **ACCEL), gradient=False)
+         for k, kw in (("broyden", {}), ("linear", dict(scc_broyden=False)), ("shift", dict(level_shift=0.15)))}
+    assert all(r.rung == 0 for r in e.values())
+    assert abs(e["linear"].energy - e["broyden"].energy) < 1e-7
+    assert abs(e["shift"].energy - e["broyden"].energy) < 1e-6
+
+
 def test_translation_rotation_invariance(oracle_mod, fixtures):
     z, x = smoke_molecule(fixtures, "water")
     r0 = oracle_mod.run(z, x)
