@@ -174,6 +174,12 @@ class Gfn1NativeCalculator:
         return CalculationResult(terms[0], terms, grad, qat, dip, iters[0], status[0] == 0, shell_charges=qsh,
                                  fermi_level=float(fermi[0]))
 
+    def calculate_periodic(self, *args, **kwargs):
+        """The reference's periodic single point (src/python.rs:386) is outside
+        the B200 engine, which runs molecules only; like every engine error it
+        raises ValueError."""
+        raise ValueError("periodic systems are outside the B200 engine (non-periodic molecules only)")
+
     # ------------------------------------------------------------------ batch-backed methods
     def _batch(self):
         if getattr(self, "_batch_calc", None) is None:

@@ -58,3 +58,9 @@ def test_calculation_result_conversions():
     assert r.energy_terms_ev()["repulsion"] == pytest.approx(2.0 * HARTREE_TO_EV)
     r0 = CalculationResult(-1.5, terms, None, [0.0], [0, 0, 0], 1, False)
     assert r0.gradient_hartree_per_bohr is None and r0.forces_ev_per_angstrom is None
+
+
+def test_periodic_entry_point_raises_value_error():
+    from gfn1_rs import Gfn1NativeCalculator
+    with pytest.raises(ValueError, match="periodic"):
+        Gfn1NativeCalculator.calculate_periodic(None, [1, 1], [[0, 0, 0], [0.74, 0, 0]])
