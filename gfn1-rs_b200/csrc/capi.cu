@@ -11,6 +11,7 @@
 #include <cusolverDn.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -213,6 +214,24 @@ struct HostBuf {
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// Makes `dev` the current device for the scope of an entry point and puts the
+// caller's current device back on exit, so that no call of the C ABI leaves
+// the calling thread on another device.
+struct DeviceGuard {
+  int prev = -1;
+  cudaError_t status = cudaSuccess;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) status = cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+  DeviceGuard(const DeviceGuard&) = delete;
+  DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
+
 }  // namespace
 
 
@@ -295,7 +314,7 @@ struct gfn1_batch {
   BlobLayout lay;
   HostBuf h_in, h_out;               // pinned staging
   DevBuf<unsigned char> d_in, d_out; // device blobs
-  DevBuf<double> S, H0, P, W, ws, gam, pairbuf, cn, shell_pot, se, grad_classic, orb_eps, orb_occ;
+  DevBuf<double> S, H0, P, W, ws, gam, pairbuf, cn, shell_pot, shell_pot_in, se, grad_classic, orb_eps, orb_occ;
   DevBuf<int> queue;
   DevBuf<unsigned long long> stage;
   template <class T>
@@ -336,6 +355,7 @@ struct gfn1_batch {
     B.cn = cn.p;
     B.shell_q = dout<double>(lay.shell_q);
     B.shell_pot = shell_pot.p;
+    B.shell_pot_in = shell_pot_in.p;
     B.atom_q = dout<double>(lay.atom_q);
     B.se = se.p;
     B.terms = dout<double>(lay.terms);
@@ -358,7 +378,7 @@ struct gfn1_batch {
     h_out.release();
     d_in.release();
     d_out.release();
-    for (DevBuf<double>* d : {&S, &H0, &P, &W, &ws, &gam, &pairbuf, &cn, &shell_pot, &se, &grad_classic, &orb_eps, &orb_occ})
+    for (DevBuf<double>* d : {&S, &H0, &P, &W, &ws, &gam, &pairbuf, &cn, &shell_pot, &shell_pot_in, &se, &grad_classic, &orb_eps, &orb_occ})
       d->release();
     queue.release();
     stage.release();
@@ -872,7 +892,7 @@ int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t*
             b->stage.ensure(kStages) && b->S.ensure(mat_total) && b->H0.ensure(mat_total) && b->P.ensure(mat_total) &&
             b->W.ensure(mat_total) && b->ws.ensure((size_t)std::max<long long>(ws_total, 1)) && b->gam.ensure(gam_total) &&
             b->pairbuf.ensure(8 * std::max<long long>(pair_total, 1)) && b->cn.ensure(natoms) &&
-            b->shell_pot.ensure(nshells) && b->se.ensure(nshells) && b->grad_classic.ensure(3 * natoms) &&
+            b->shell_pot.ensure(nshells) && b->shell_pot_in.ensure(nshells) && b->se.ensure(nshells) && b->grad_classic.ensure(3 * natoms) &&
             b->orb_eps.ensure(std::max<long long>(naos, 1)) && b->orb_occ.ensure(std::max<long long>(naos, 1));
   if (!ok) return fail(eng, GFN1_E_DEVICE, "device allocation failed for the batch workspace");
   if (!b->dense_ids.empty()) {
@@ -1135,7 +1155,8 @@ int gfn1_engine_create(const char* param_spec, int device, gfn1_engine** out) {
     delete eng;
     return fail(nullptr, GFN1_E_MISSING_GLOBAL, err);
   }
-  cudaError_t e = cudaSetDevice(device);
+  DeviceGuard dg(device);
+  cudaError_t e = dg.status;
   if (e != cudaSuccess) {
     delete eng;
     return cuda_fail(nullptr, e, "cudaSetDevice");
@@ -1190,7 +1211,7 @@ int gfn1_batch_create(gfn1_engine* eng, int nmol, const int32_t* atom_offsets, c
                       const gfn1_options* opt, gfn1_batch** out) {
   if (!eng || !out || nmol < 1 || !atom_offsets || !z) return fail(eng, GFN1_E_INVALID_INPUT, "invalid batch arguments");
   *out = nullptr;
-  cudaSetDevice(eng->device);
+  DeviceGuard dg(eng->device);
   gfn1_batch* b = new gfn1_batch();
   b->eng = eng;
   const char* prof = std::getenv("GFN1_PROFILE");
@@ -1324,7 +1345,7 @@ int gfn1_batch_energy_gradient(gfn1_engine* eng, int nmol, const int32_t* atom_o
                                const double* xyz_bohr, const double* charge, const double* init_shell_q,
                                const gfn1_options* opt, const gfn1_outputs* out) {
   if (!eng || nmol < 1 || !atom_offsets || !z || !xyz_bohr) return fail(eng, GFN1_E_INVALID_INPUT, "invalid arguments");
-  cudaSetDevice(eng->device);
+  DeviceGuard dg(eng->device);
   if (!eng->oneshot) {
     eng->oneshot = new gfn1_batch();
     eng->oneshot->eng = eng;
@@ -1373,11 +1394,70 @@ static int copy_molecule_matrices(gfn1_batch* b, int m, double* S, double* H0, d
   return GFN1_OK;
 }
 
+// Fock matrix of the last diagonalisation, F = H0 - 1/2 S_mu,nu (v_mu + v_nu)
+// with v the AO potential of that diagonalisation's input charges
+// (fock_from_shell_potential, src/electronic.rs:3133-3158), the final shell
+// potential of the output charges (ElectronicResult::shell_scc_potential,
+// src/electronic.rs:1980, 2031) and the atoms' coordination numbers
+// (ElectronicResult::coordination_numbers, src/hamiltonian.rs:41, 87).
+static int copy_molecule_fock(gfn1_batch* b, int m, double* F, double* shell_potential, double* cn) {
+  gfn1_engine* eng = b->eng;
+  if (m < 0 || m >= b->nmol) return fail(eng, GFN1_E_INVALID_INPUT, "molecule index out of range");
+  const int* h_atom = b->hin<int>(b->lay.atom_off);
+  const int* h_shell = b->hin<int>(b->lay.shell_off);
+  const int* h_ao = b->hin<int>(b->lay.ao_off);
+  const long long* h_mat = b->hin<long long>(b->lay.mat_off);
+  const int* h_z = b->hin<int>(b->lay.z);
+  const int a0 = h_atom[m], nat = h_atom[m + 1] - a0, sh0 = h_shell[m], nsh = h_shell[m + 1] - sh0;
+  const size_t n = (size_t)(h_ao[m + 1] - h_ao[m]);
+  cudaError_t e = cudaSuccess;
+  if (shell_potential && nsh > 0)
+    e = cudaMemcpy(shell_potential, b->shell_pot.p + sh0, sizeof(double) * nsh, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && cn && nat > 0) e = cudaMemcpy(cn, b->cn.p + a0, sizeof(double) * nat, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && F && n > 0) {
+    std::vector<double> S(n * n), vin(nsh), vao(n);
+    e = cudaMemcpy(F, b->H0.p + h_mat[m], sizeof(double) * n * n, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(S.data(), b->S.p + h_mat[m], sizeof(double) * n * n, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(vin.data(), b->shell_pot_in.p + sh0, sizeof(double) * nsh, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) {
+      size_t o = 0;
+      int s = 0;
+      for (int a = 0; a < nat; ++a) {
+        const ElemTable& el = eng->elem[h_z[a0 + a]];
+        for (int k = 0; k < el.nsh; ++k)
+          for (int q = 0; q < 2 * el.l[k] + 1; ++q) vao[o + el.ao_first[k] + q] = vin[s + k];
+        s += el.nsh;
+        o += el.nao;
+      }
+      for (size_t i = 0; i < n; ++i)
+        for (size_t j = 0; j < n; ++j) F[i * n + j] -= 0.5 * S[i * n + j] * (vao[i] + vao[j]);
+    }
+  }
+  return e == cudaSuccess ? GFN1_OK : cuda_fail(eng, e, "Fock copy");
+}
+
+int gfn1_last_molecule_fock(gfn1_engine* eng, int m, double* F, double* shell_potential, double* cn) {
+  if (!eng) return fail(nullptr, GFN1_E_INVALID_INPUT, "null engine");
+  if (!eng->oneshot || eng->oneshot->nmol < 1) return fail(eng, GFN1_E_INVALID_INPUT, "no calculation on this engine");
+  DeviceGuard dg(eng->device);
+  cudaError_t e = cudaStreamSynchronize(eng->stream);
+  if (e != cudaSuccess) return cuda_fail(eng, e, "stream synchronise");
+  return copy_molecule_fock(eng->oneshot, m, F, shell_potential, cn);
+}
+
+int gfn1_batch_molecule_fock(gfn1_batch* b, int m, double* F, double* shell_potential, double* cn) {
+  if (!b) return fail(nullptr, GFN1_E_INVALID_INPUT, "null batch");
+  DeviceGuard dg(b->eng->device);
+  cudaError_t e = cudaDeviceSynchronize();  // launches may be on any of the caller's streams
+  if (e != cudaSuccess) return cuda_fail(b->eng, e, "device synchronise");
+  return copy_molecule_fock(b, m, F, shell_potential, cn);
+}
+
 int gfn1_last_molecule_matrices(gfn1_engine* eng, int m, double* S, double* H0, double* P, double* W, double* eps,
                                 double* occ) {
   if (!eng) return fail(nullptr, GFN1_E_INVALID_INPUT, "null engine");
   if (!eng->oneshot || eng->oneshot->nmol < 1) return fail(eng, GFN1_E_INVALID_INPUT, "no calculation on this engine");
-  cudaSetDevice(eng->device);
+  DeviceGuard dg(eng->device);
   cudaError_t e = cudaStreamSynchronize(eng->stream);
   if (e != cudaSuccess) return cuda_fail(eng, e, "stream synchronise");
   return copy_molecule_matrices(eng->oneshot, m, S, H0, P, W, eps, occ);
@@ -1386,7 +1466,7 @@ int gfn1_last_molecule_matrices(gfn1_engine* eng, int m, double* S, double* H0, 
 int gfn1_batch_molecule_matrices(gfn1_batch* b, int m, double* S, double* H0, double* P, double* W, double* eps,
                                  double* occ) {
   if (!b) return fail(nullptr, GFN1_E_INVALID_INPUT, "null batch");
-  cudaSetDevice(b->eng->device);
+  DeviceGuard dg(b->eng->device);
   cudaError_t e = cudaDeviceSynchronize();  // launches may be on any of the caller's streams
   if (e != cudaSuccess) return cuda_fail(b->eng, e, "device synchronise");
   return copy_molecule_matrices(b, m, S, H0, P, W, eps, occ);
@@ -1489,7 +1569,10 @@ constexpr int kNaMaxShells = 128;
 constexpr int kNaMaxHist = 250;
 constexpr size_t kNoallocBytes = 4456448;  // 4.25 MiB
 constexpr int kNaMaxDevices = 64;
-unsigned char* g_noalloc_dev_ptr[kNaMaxDevices];  // device address of the array, per device
+// Device address of the array, per device.  Host threads making their first
+// call on a device at the same time store the same value; the atomics keep
+// that well defined.
+std::atomic<unsigned char*> g_noalloc_dev_ptr[kNaMaxDevices];
 }  // namespace
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
@@ -1536,15 +1619,17 @@ extern "C" int gfn1_run_noalloc(gfn1_engine* eng, int nat, const uint8_t* z, con
     return fail(eng, GFN1_E_INVALID_INPUT, "gfn1_run_noalloc runs without a level shift (use gfn1_run)");
   const int dev = eng->device;
   if (dev < 0 || dev >= kNaMaxDevices) return fail(eng, GFN1_E_INVALID_INPUT, "device ordinal out of range");
-  cudaError_t e = cudaSetDevice(dev);
+  DeviceGuard dg(dev);  // the caller's current device comes back on return
+  cudaError_t e = dg.status;
   if (e != cudaSuccess) return cuda_fail(eng, e, "cudaSetDevice");
-  if (!g_noalloc_dev_ptr[dev]) {  // once per device, with that device current
+  unsigned char* base = g_noalloc_dev_ptr[dev].load(std::memory_order_acquire);
+  if (!base) {  // once per device, with that device current
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return cuda_fail(eng, e, "cudaGetSymbolAddress(g_noalloc_scratch)");
-    g_noalloc_dev_ptr[dev] = (unsigned char*)p;
+    base = (unsigned char*)p;
+    g_noalloc_dev_ptr[dev].store(base, std::memory_order_release);
   }
-  unsigned char* base = g_noalloc_dev_ptr[dev];
   cudaStream_t st = stream ? (cudaStream_t)stream : eng->stream;
 
   // ---- layout inside the scratch array (byte offsets, 256-aligned)
@@ -1578,6 +1663,11 @@ extern "C" int gfn1_run_noalloc(gfn1_engine* eng, int nat, const uint8_t* z, con
                w_pair = take(sizeof(double) * 8 * std::max<long long>(npair, 1)), w_cn = take(sizeof(double) * nat),
                w_pot = take(sizeof(double) * nsh), w_se = take(sizeof(double) * nsh),
                w_gcl = take(sizeof(double) * 3 * nat), w_queue = take(4 * sizeof(int));
+  // the engine's learned guess (as gfn1_run uses it) when the caller gives no
+  // initial charges: descriptors and network outputs of the molecule's atoms
+  const bool use_guess = eng->guess != nullptr && init_shell_q == nullptr;
+  const size_t w_gx = use_guess ? take(sizeof(float) * kGuessIn * nat) : 0,
+               w_gy = use_guess ? take(sizeof(float) * kGuessOut * nat) : 0;
   if (off > kNoallocBytes) return fail(eng, GFN1_E_INVALID_INPUT, "molecule exceeds the no-allocation scratch");
 
   // ---- stage inputs on the stack and copy them into the scratch array
@@ -1617,7 +1707,7 @@ extern "C" int gfn1_run_noalloc(gfn1_engine* eng, int nat, const uint8_t* z, con
   B.z = (const int*)(base + i_z);
   B.xyz = (const double*)(base + i_xyz);
   B.charge = (const double*)(base + i_charge);
-  B.init_q = init_shell_q ? (const double*)(base + i_q0) : nullptr;
+  B.init_q = (init_shell_q || use_guess) ? (const double*)(base + i_q0) : nullptr;
   B.S = (double*)(base + w_S);
   B.H0 = (double*)(base + w_H0);
   B.P = (double*)(base + w_P);
@@ -1659,6 +1749,17 @@ extern "C" int gfn1_run_noalloc(gfn1_engine* eng, int nat, const uint8_t* z, con
   const size_t sm_scc = std::max(scc_smem_bytes(nsh, n, nat, 0),
                                  std::min(scc_smem_bytes(nsh, n, nat, n), scc_max_dynamic_smem(n > 96 ? 512 : 256)));
   const size_t sm_grad = sizeof(double) * 7 * (size_t)nat + sizeof(int) * (3 * (size_t)nat + 2);
+  if (use_guess) {  // predicted shell charges into the initial-charge slot of the input region
+    const GuessModel& g = eng->guess->model;
+    float* gx = (float*)(base + w_gx);
+    float* gy = (float*)(base + w_gy);
+    if ((e = launch_guess_features(1, B.atom_off, B.z, B.xyz, g.params, g.params + kGuessDesc, gx, st)) !=
+            cudaSuccess ||
+        (e = launch_guess_infer(g, nat, gx, gy, st)) != cudaSuccess ||
+        (e = launch_guess_project(1, B.atom_off, B.shell_off, B.z, gy, B.charge, (double*)(base + i_q0), st)) !=
+            cudaSuccess)
+      return cuda_fail(eng, e, "learned guess");
+  }
   setup_kernel<<<1, 128, sm_setup, st>>>(B, M, o.enable_dispersion, nsh);
   SccLaunch SL;
   SL.q_begin = 0;

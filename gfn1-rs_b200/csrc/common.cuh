@@ -125,6 +125,7 @@ struct Batch {
   // per-atom / per-shell state
   double *cn, *cn_disp_dedcn; // [natoms]
   double *shell_q, *shell_pot, *atom_q; // [nshells], [nshells], [natoms]
+  double* shell_pot_in;     // [nshells] potential of the last diagonalised Fock matrix, or null
   double* se;               // [nshells] self energies
   // outputs
   double* terms;            // [nmol*kTerms]

@@ -1,10 +1,14 @@
 // Persistent SCC kernel: each CTA pulls molecules from a work queue (most
 // expensive first) and runs the complete self-consistent-charge loop of
 // gfn1-rs `run_scc_with_core` (src/electronic.rs:849-2054, plain charge-vector
-// branch, ladder rung 0) on the device.  Two size classes are launched
-// concurrently: 512 threads with one CTA per SM for the large molecules, 256
-// threads with two CTAs per SM for the rest.  The working matrix of the
-// eigensolver lives in shared memory whenever it fits.
+// branch, ladder rung 0) on the device.  The batch path launches two size
+// classes concurrently (above and below 96 AOs), both with 128-thread CTAs and
+// four CTAs per SM; shared memory holds the index tables and N-vectors, and the
+// eigensolver's working matrix lives in the CTA's global workspace slot, cached
+// by L1.  Up to 193 AOs the Householder reduction is blocked (8-column panels,
+// tensor-core trailing updates).  Wider CTAs (256/512 threads) and a working
+// matrix in shared memory are used only by the allocation-free single-molecule
+// entry point, which passes the room for it in the launch's shared memory.
 //
 // Algorithmic choices that differ from the reference but give the same results
 // up to FP64 rounding:
@@ -1363,6 +1367,7 @@ __device__ void stage_results(const Batch& B, const MolCtx& c, CtaWs& w, int ite
   for (int s = tid; s < nsh; s += NT) {
     B.shell_q[sh0 + s] = w.qout[s];
     B.shell_pot[sh0 + s] = w.vout[s];
+    if (B.shell_pot_in) B.shell_pot_in[sh0 + s] = w.vsh[s];
   }
   for (int a = tid; a < nat; a += NT) B.atom_q[a0 + a] = w.qat[a];
 }

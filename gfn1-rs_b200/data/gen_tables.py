@@ -229,4 +229,9 @@ def main(root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    import os
+
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GFN1_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: gen_tables.py REFERENCE_ROOT (or set GFN1_REFERENCE_ROOT): a gfn1-rs v0.5.1 checkout")
+    main(root)

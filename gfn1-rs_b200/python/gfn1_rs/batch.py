@@ -51,15 +51,21 @@ def _options(opts: dict, compute_gradient: bool) -> _lib.Options:
     return _lib.default_options(compute_gradient=int(bool(compute_gradient)), **opts)
 
 
-def _matrices(engine, off, z, m: int, call) -> dict:
+def _matrices(engine, off, z, m: int, call, fock_call) -> dict:
     if not 0 <= m < len(off) - 1:
         raise IndexError(f"molecule {m} out of range")
-    nao_z = engine.element_sizes()[0]
-    n = int(np.sum(nao_z[np.asarray(z[off[m]:off[m + 1]], dtype=np.int64)]))
+    nao_z, nsh_z = engine.element_sizes()
+    zm = np.asarray(z[off[m]:off[m + 1]], dtype=np.int64)
+    n, nsh = int(np.sum(nao_z[zm])), int(np.sum(nsh_z[zm]))
     keys = ("S", "H0", "P", "W", "orbital_energies", "occupations")
     out = {k: np.zeros((n, n)) for k in keys[:4]}
     out.update({k: np.zeros(n) for k in keys[4:]})
     _lib.check(call(*[_lib.ptr(out[k]) for k in keys]), engine.handle)
+    out["fock"] = np.zeros((n, n))
+    out["shell_scc_potential"] = np.zeros(nsh)
+    out["coordination_numbers"] = np.zeros(len(zm))
+    _lib.check(fock_call(_lib.ptr(out["fock"]), _lib.ptr(out["shell_scc_potential"]),
+                         _lib.ptr(out["coordination_numbers"])), engine.handle)
     return out
 
 
@@ -136,15 +142,17 @@ class BatchCalculator:
         return BatchResult(energy, terms, grad, qsh, qat, dip, fermi, iters, status, off, shoff, rung)
 
     def molecule_matrices(self, m: int) -> dict:
-        """S, H0, P, W ([N, N]) and orbital energies / occupations ([N]) of
+        """S, H0, P, W, fock ([N, N]), orbital energies / occupations ([N]),
+        shell_scc_potential ([nshells]) and coordination_numbers ([natoms]) of
         molecule m of the last calculate_flat call: the optional members of the
-        reference's ElectronicResult (gfn1-rs src/electronic.rs:600-612).
+        reference's ElectronicResult (gfn1-rs src/electronic.rs:600-620).
         Orbital energies the eigensolver did not need are NaN."""
         if self._last is None:
             raise RuntimeError("no calculation on this calculator yet")
         off, z = self._last
-        return _matrices(self.engine, off, z, m,
-                         lambda *p: _lib.load().gfn1_last_molecule_matrices(self.engine.handle, int(m), *p))
+        L, h = _lib.load(), self.engine.handle
+        return _matrices(self.engine, off, z, m, lambda *p: L.gfn1_last_molecule_matrices(h, int(m), *p),
+                         lambda *p: L.gfn1_last_molecule_fock(h, int(m), *p))
 
     def calculate(self, molecules, unit="angstrom", charges=None, compute_gradient=True, **kw) -> BatchResult:
         """molecules: iterable of (numbers, positions) in `unit`."""
@@ -179,8 +187,10 @@ class ResidentBatch:
 
     def molecule_matrices(self, m: int) -> dict:
         """As BatchCalculator.molecule_matrices, after this batch's last launch."""
+        L = _lib.load()
         return _matrices(self.calc.engine, self.atom_offsets, self.numbers, m,
-                         lambda *p: _lib.load().gfn1_batch_molecule_matrices(self.handle, int(m), *p))
+                         lambda *p: L.gfn1_batch_molecule_matrices(self.handle, int(m), *p),
+                         lambda *p: L.gfn1_batch_molecule_fock(self.handle, int(m), *p))
 
     def close(self):
         if getattr(self, "handle", None):

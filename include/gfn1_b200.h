@@ -120,6 +120,20 @@ int gfn1_batch_energy_gradient(gfn1_engine* eng, int nmol, const int32_t* atom_o
 int gfn1_last_molecule_matrices(gfn1_engine* eng, int m, double* S, double* H0, double* P, double* W, double* eps,
                                 double* occ);
 
+/* Fock matrix, shell potential and coordination numbers of molecule m of the
+ * last gfn1_run / gfn1_batch_energy_gradient call, the remaining optional
+ * members of ElectronicResult (src/electronic.rs:600-620):
+ *   F (N x N, row-major) = fock: H0 - 1/2 S_mu,nu (v_mu + v_nu) with v the AO
+ *     potential of the input charges of the last diagonalisation
+ *     (fock_from_shell_potential, src/electronic.rs:3133-3158).  On a rung of
+ *     the fallback ladder with a level shift the reference's member also holds
+ *     the shift projector b (S - 1/2 S P_prev S); F here does not;
+ *   shell_potential (nshells) = shell_scc_potential: the potential of the
+ *     final output shell charges (src/electronic.rs:1980, 2031);
+ *   cn (natoms) = coordination_numbers (src/hamiltonian.rs:41, 87).
+ * Any pointer may be NULL. */
+int gfn1_last_molecule_fock(gfn1_engine* eng, int m, double* F, double* shell_potential, double* cn);
+
 /* Resident-batch interface: the topology (atom counts, elements, charges) is
  * uploaded once; coordinates can then be replaced and the batch re-run with
  * inputs already on the device (molecular dynamics, benchmarking).
@@ -151,6 +165,9 @@ int gfn1_batch_download(gfn1_batch* b, const gfn1_outputs* out);
  * last launch (waits for the device first). */
 int gfn1_batch_molecule_matrices(gfn1_batch* b, int m, double* S, double* H0, double* P, double* W, double* eps,
                                  double* occ);
+/* As gfn1_last_molecule_fock for molecule m of a resident batch after its last
+ * launch (waits for the device first). */
+int gfn1_batch_molecule_fock(gfn1_batch* b, int m, double* F, double* shell_potential, double* cn);
 /* Device pointers of the batch-owned result arrays (valid until destroy);
  * there `rung` is meaningful where `status` is 0. */
 int gfn1_batch_outputs_device(gfn1_batch* b, gfn1_outputs* out);
@@ -167,7 +184,10 @@ int gfn1_batch_info(const gfn1_batch* b, int64_t* natoms, int64_t* nshells, int6
  * 128 shells and 250 Broyden history vectors (min(scc_broyden_size, max_scc));
  * larger inputs return GFN1_E_INVALID_INPUT with a message naming the limit.
  * Only rung 0 of the fallback ladder runs here: a molecule that needs the
- * later rungs returns GFN1_E_SCC_NOT_CONVERGED.
+ * later rungs returns GFN1_E_SCC_NOT_CONVERGED.  Like gfn1_run, the SCC starts
+ * from init_shell_q when given, else from the engine's learned guess when one
+ * is set (gfn1_engine_set_guess), else from zero charges.  The caller's
+ * current device is the same on return.
  * The first call on a device looks up the array's device address (once per
  * device, that device current); make that first call before any stream
  * capture.  Every call reuses the same array, so calls that overlap on the GPU

@@ -1244,7 +1244,8 @@ struct Result {
   int rung = -1;       // fallback-ladder attempt that converged (src/electronic.rs:1420)
   double etemp = 0.0;  // electronic temperature of that attempt (src/electronic.rs:2024-2026)
   double fermi = 0, nelec = 0, rms = 0;
-  Mat S, H0, P, W;
+  Mat S, H0, P, W, F;            // F: Fock matrix of the last step (SccStep::fock)
+  std::vector<double> shell_pot;  // potential of the final output charges (shell_scc_potential)
   int nao = 0, nsh = 0;
 };
 
@@ -1488,6 +1489,8 @@ Result run(const System& sys, const Options& opt, const double* init_q, bool wan
   res.H0 = H0;
   res.P = last.P;
   res.W = last.W;
+  res.F = last.F;          // src/electronic.rs:2019
+  res.shell_pot = sc.pot;  // src/electronic.rs:1980, 2031
   if (!want_grad) return res;
 
   // --- analytic gradient (src/gradient.rs:122-242, :244-531)
@@ -1698,7 +1701,7 @@ int oracle_classical_term(int which, int nat, const int* z, const double* xyz_bo
 int oracle_run(int nat, const int* z, const double* xyz_bohr, const oracle_options* o, const double* init_shell_q,
                int want_grad, double* terms, double* grad, double* shell_q, double* atom_q, double* eps,
                double* occ, double* dipole, double* cn, int* iterations, int* converged, double* fermi, double* S,
-               double* H0, double* P, double* W, int* rung, double* etemp_used) {
+               double* H0, double* P, double* W, int* rung, double* etemp_used, double* F, double* shell_pot) {
   try {
     System s;
     s.z.assign(z, z + nat);
@@ -1724,6 +1727,8 @@ int oracle_run(int nat, const int* z, const double* xyz_bohr, const oracle_optio
     if (W) std::copy(r.W.a.begin(), r.W.a.end(), W);
     if (rung) *rung = r.rung;
     if (etemp_used) *etemp_used = r.etemp;
+    if (F) std::copy(r.F.a.begin(), r.F.a.end(), F);
+    if (shell_pot) std::copy(r.shell_pot.begin(), r.shell_pot.end(), shell_pot);
     return OK;
   } catch (const OracleError& e) {
     t_err = e.what();

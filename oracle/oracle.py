@@ -80,6 +80,8 @@ class OracleResult:
     H0: np.ndarray | None = None
     P: np.ndarray | None = None
     W: np.ndarray | None = None
+    F: np.ndarray | None = None                  # Fock matrix of the last diagonalisation (matrices=True)
+    shell_potential: np.ndarray | None = None    # shell_scc_potential of the final charges (matrices=True)
     extra: dict = field(default_factory=dict)
 
 
@@ -112,7 +114,7 @@ def _load():
         L.oracle_last_error.restype = ctypes.c_char_p
         L.oracle_sizes.argtypes = [ctypes.c_int, ip, ip, ip]
         L.oracle_run.argtypes = [ctypes.c_int, ip, dp, ctypes.POINTER(OracleOptions), dp, ctypes.c_int,
-                                 dp, dp, dp, dp, dp, dp, dp, dp, ip, ip, dp, dp, dp, dp, dp, ip, dp]
+                                 dp, dp, dp, dp, dp, dp, dp, dp, ip, ip, dp, dp, dp, dp, dp, ip, dp, dp, dp]
         L.oracle_halogen.argtypes = [ctypes.c_int, ip, dp, dp, dp]
         L.oracle_classical_term.argtypes = [ctypes.c_int, ctypes.c_int, ip, dp, dp, dp]
         L.oracle_run_batch.argtypes = [ctypes.c_int, ip, ip, dp, dp, ctypes.POINTER(OracleOptions), ctypes.c_int,
@@ -164,18 +166,20 @@ def run(numbers, positions_bohr, options: OracleOptions | None = None, gradient:
     fermi = ctypes.c_double()
     rung = ctypes.c_int()
     etemp = ctypes.c_double()
-    mats = [np.zeros((nao, nao)) for _ in range(4)] if matrices else [None] * 4
+    mats = [np.zeros((nao, nao)) for _ in range(5)] if matrices else [None] * 5
+    spot = np.zeros(nsh) if matrices else None
     q0 = None if init_shell_charges is None else np.ascontiguousarray(init_shell_charges, dtype=np.float64)
     rc = L.oracle_run(nat, _ip(z), _dp(xyz), ctypes.byref(opt), _dp(q0), int(gradient), _dp(terms), _dp(grad),
                       _dp(qsh), _dp(qat), _dp(eps), _dp(occ), _dp(dip), _dp(cn), ctypes.byref(it),
-                      ctypes.byref(conv), ctypes.byref(fermi), *[_dp(m) for m in mats], ctypes.byref(rung),
-                      ctypes.byref(etemp))
+                      ctypes.byref(conv), ctypes.byref(fermi), *[_dp(m) for m in mats[:4]], ctypes.byref(rung),
+                      ctypes.byref(etemp), _dp(mats[4]), _dp(spot))
     if rc != 0:
         raise OracleError(rc, L.oracle_last_error().decode())
     return OracleResult(terms=dict(zip(TERM_NAMES, terms.tolist())), energy=float(terms[0]), gradient=grad,
                         shell_charges=qsh, atomic_charges=qat, orbital_energies=eps, occupations=occ,
                         dipole=dip, coordination_numbers=cn, iterations=it.value, converged=bool(conv.value),
-                        fermi_level=fermi.value, rung=rung.value, electronic_temperature=etemp.value, S=mats[0], H0=mats[1], P=mats[2], W=mats[3])
+                        fermi_level=fermi.value, rung=rung.value, electronic_temperature=etemp.value, S=mats[0], H0=mats[1], P=mats[2], W=mats[3],
+                        F=mats[4], shell_potential=spot)
 
 
 def halogen(numbers, positions_bohr, gradient: bool = True):

@@ -35,9 +35,11 @@ def test_tables_regenerate_identically():
 
     import pytest
 
-    ref = "/root/reference"
+    # a gfn1-rs v0.5.1 checkout: GFN1_REFERENCE_ROOT, else a sibling directory
+    # named "reference" next to this repository
+    ref = os.environ.get("GFN1_REFERENCE_ROOT") or os.path.join(os.path.dirname(ROOT), "reference")
     if not os.path.isdir(ref):
-        pytest.skip("reference tree not present")
+        pytest.skip("reference tree not present (set GFN1_REFERENCE_ROOT)")
     gen = os.path.join(ROOT, "gfn1-rs_b200", "data", "gen_tables.py")
     out = subprocess.run([sys.executable, gen, ref], check=True, capture_output=True, text=True).stdout
     committed = open(os.path.join(ROOT, "gfn1-rs_b200", "data", "gfn1_tables.txt")).read()

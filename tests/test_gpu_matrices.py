@@ -1,9 +1,11 @@
 """The optional ElectronicResult members (S, H0, P, W, orbital energies,
-occupations) through gfn1_last_molecule_matrices / gfn1_batch_molecule_matrices
-against the oracle's matrices, on both device paths.
+occupations, Fock matrix, shell potential, coordination numbers) through
+gfn1_last_molecule_matrices / gfn1_last_molecule_fock and their resident-batch
+twins against the oracle's, on both device paths.
 
-Tolerances: S and H0 to 1e-12 (geometry only); P, W, orbital energies and
-occupations to 1e-6 at tight SCC convergence (1e-10 Eh, 1e-8 e)."""
+Tolerances: S and H0 to 1e-12 (geometry only), coordination numbers to 1e-10;
+P, W, F, orbital energies, occupations and the shell potential to 1e-6 at
+tight SCC convergence (1e-10 Eh, 1e-8 e)."""
 import os
 
 import numpy as np
@@ -40,6 +42,10 @@ def _check(mats, o, full_spectrum):
     if full_spectrum:
         assert known.all()
     assert np.max(np.abs(eps[known] - o.orbital_energies[known])) <= 1e-6
+    # fock, shell_scc_potential, coordination_numbers (src/electronic.rs:600-620)
+    assert np.max(np.abs(mats["fock"] - o.F)) <= 1e-6
+    assert np.max(np.abs(mats["shell_scc_potential"] - o.shell_potential)) <= 1e-6
+    assert np.max(np.abs(mats["coordination_numbers"] - o.coordination_numbers)) <= 1e-10
 
 
 @pytest.mark.parametrize("dense_n", [None, 16])

@@ -30,7 +30,7 @@ def _outputs(nat, nsh):
     return out, arrs
 
 
-def _call(fn_name, engine, z, x, opt):
+def _call(fn_name, engine, z, x, opt, charge=0.0):
     from gfn1_rs import _lib
 
     L = _lib.load()
@@ -39,7 +39,7 @@ def _call(fn_name, engine, z, x, opt):
     nat = len(z8)
     nsh = engine.basis_size(z8)[1]
     out, arrs = _outputs(nat, nsh)
-    args = [engine.handle, nat, _lib.ptr(z8, ctypes.c_uint8), _lib.ptr(xb), 0.0, None, ctypes.byref(opt),
+    args = [engine.handle, nat, _lib.ptr(z8, ctypes.c_uint8), _lib.ptr(xb), float(charge), None, ctypes.byref(opt),
             ctypes.byref(out)]
     if fn_name == "gfn1_run_noalloc":
         args.append(None)
@@ -76,6 +76,100 @@ def test_noalloc_matches_allocating_entry_point_twice(engine, fixtures):
             assert np.max(np.abs(got["gradient"] - ref["gradient"])) <= G_TOL
             assert np.max(np.abs(got["shell"] - ref["shell"])) <= Q_TOL
             assert got["iters"][0] == ref["iters"][0] and got["status"][0] == 0
+
+
+def _assert_same(got, ref):
+    assert abs(got["energy"][0] - ref["energy"][0]) <= E_TOL
+    assert np.max(np.abs(got["terms"] - ref["terms"])) <= E_TOL
+    assert np.max(np.abs(got["gradient"] - ref["gradient"])) <= G_TOL
+    assert np.max(np.abs(got["shell"] - ref["shell"])) <= Q_TOL
+    assert got["iters"][0] == ref["iters"][0] and got["status"][0] == ref["status"][0]
+
+
+@pytest.mark.parametrize("case", ["ferrocene", "CBr...O", "NH3+ doublet"])
+def test_noalloc_d_shells_halogen_and_spin(engine, fixtures, case):
+    """d shells (ferrocene), the halogen-bond term (C-Br...O) and a charged
+    doublet with a requested spin multiplicity, each twice in a row, against
+    the allocating entry point."""
+    from gfn1_rs import _lib
+
+    charge, kw = 0.0, {}
+    if case == "ferrocene":
+        z, x = smoke_molecule(fixtures, case)
+    elif case == "CBr...O":
+        rec = fixtures["halogen_tests"][case]
+        z, x = np.array(rec["numbers"]), np.array(rec["positions_angstrom"]) * ANGSTROM_TO_BOHR
+    else:  # NH3+ radical cation, spin multiplicity 2
+        z = np.array([7, 1, 1, 1])
+        x = np.array([[0.0, 0.0, 0.0], [0.0, 0.94, 0.38], [0.81, -0.47, 0.38], [-0.81, -0.47, 0.38]]) * ANGSTROM_TO_BOHR
+        charge, kw = 1.0, dict(spin_multiplicity=2)
+    opt = _lib.default_options(**kw)
+    rc, ref = _call("gfn1_run", engine, z, x, opt, charge)
+    assert rc == 0, _lib.last_error()
+    for _ in range(2):
+        rc, got = _call("gfn1_run_noalloc", engine, z, x, opt, charge)
+        assert rc == 0, _lib.last_error()
+        _assert_same(got, ref)
+
+
+def test_noalloc_reports_unconverged_scc(engine, fixtures):
+    """max_scc = 1 cannot pass the convergence test (its first energy change is
+    infinite): status GFN1_E_SCC_NOT_CONVERGED, as from gfn1_run's rung 0."""
+    from gfn1_rs import _lib
+
+    z, x = smoke_molecule(fixtures, "caffeine")
+    opt = _lib.default_options(max_scc=1)
+    for _ in range(2):
+        rc, got = _call("gfn1_run_noalloc", engine, z, x, opt)
+        assert rc == 8, _lib.last_error()
+        assert got["status"][0] == 8 and got["iters"][0] == 1
+        assert "did not converge" in _lib.last_error()
+
+
+def test_noalloc_uses_the_engines_learned_guess(fixtures):
+    """With a learned guess set on the engine, both entry points start from the
+    predicted charges: same iteration count and results."""
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from gfn1_rs import _lib
+    from gfn1_rs.guess import LearnedGuess
+
+    eng = _lib.Engine()
+    guess = LearnedGuess.from_file(eng)
+    L = _lib.load()
+    _lib.check(L.gfn1_engine_set_guess(eng.handle, guess.handle), eng.handle)
+    try:
+        from gfn1_rs import workloads
+
+        z, x = workloads.water_cluster(8, 3)  # the kind of molecule the guess was trained on
+        x = x * ANGSTROM_TO_BOHR
+        opt = _lib.default_options()
+        rc, ref = _call("gfn1_run", eng, z, x, opt)
+        assert rc == 0, _lib.last_error()
+        rc0, plain = _call("gfn1_run_noalloc", _lib.Engine(), z, x, opt)
+        assert rc0 == 0
+        for _ in range(2):
+            rc, got = _call("gfn1_run_noalloc", eng, z, x, opt)
+            assert rc == 0, _lib.last_error()
+            _assert_same(got, ref)
+        assert ref["iters"][0] <= plain["iters"][0]  # the predicted start is no worse than zero charges
+    finally:
+        L.gfn1_engine_set_guess(eng.handle, None)
+        guess.close()
+
+
+def test_noalloc_keeps_the_callers_device(engine, fixtures):
+    import torch
+
+    from gfn1_rs import _lib
+
+    before = torch.cuda.current_device()
+    z, x = smoke_molecule(fixtures, "water")
+    rc, _ = _call("gfn1_run_noalloc", engine, z, x, _lib.default_options())
+    assert rc == 0, _lib.last_error()
+    assert torch.cuda.current_device() == before
 
 
 def test_noalloc_rejects_oversize_molecule(engine):
