@@ -6,9 +6,7 @@
 // primitive-count rule (src/basis.rs:251-279), same-centre orthogonalisation of
 // a second shell of the same angular momentum (src/basis.rs:318-344), the CN
 // shift (src/basis.rs:281-293) and the legacy eV->Eh factor (src/basis.rs:18).
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
-#include <cusolverDn.h>
 
 #include <algorithm>
 #include <atomic>
@@ -35,12 +33,19 @@ cudaError_t launch_scc(int nt, int grid, size_t smem, cudaStream_t st, const Bat
                        const SccOptions& opt, const SccLaunch& SL);
 cudaError_t launch_scc_robust(int nt, int grid, size_t smem, cudaStream_t st, const Batch& B, const Model& M,
                               const SccOptions& opt, const SccLaunch& SL);
-long long dense_ws_doubles(int maxnsh, int cap, int maxnat);
-size_t dense_smem_bytes(int maxnsh, int maxn, int maxnat);
-size_t dense_state_bytes();
-long long dense_solver_lwork(void* solver, int N);
-cudaError_t run_dense_molecule(const Batch& B, const Model& M, const SccOptions& opt, int m, int N, long long mo,
-                               DenseWork& dw, cudaStream_t st);
+// large molecules on many SMs (wide.cuh)
+struct WideRuntime;
+WideRuntime* wide_runtime_new();
+void wide_runtime_delete(WideRuntime* r);
+long long wide_slot_doubles(int N, int nsh, int nat, int cap);
+cudaError_t wide_bind_runtime(WideRuntime* r, const std::vector<int>& ids, const std::vector<int>& Ns,
+                              const std::vector<long long>& mos, const std::vector<int>& nshs,
+                              const std::vector<int>& nats, int cap, double* base,
+                              const std::vector<long long>& slot_off);
+cudaError_t wide_run(const Batch& B, const Model& M, const SccOptions& opt, WideRuntime* r, int nslots, int maxn,
+                     int maxnsh, int maxnat, int cap, int num_sms, cudaStream_t st);
+void wide_plan_info(const WideRuntime* r, int* nb, int* min_rows, int* group, float* ms, int* tuned);
+size_t dense_table_bytes_host(int maxnsh, int maxn, int maxnat);
 }  // namespace gfn1
 
 using namespace gfn1;
@@ -302,15 +307,11 @@ struct gfn1_batch {
   gfn1_guess* guess = nullptr;       // learned guess used when no initial charges are set
   DevBuf<float> gx, gy;              // guess features [natoms x 100] and outputs [natoms x 2]
   DevBuf<double> gq;                 // guessed initial shell charges [nshells]
-  // molecules above kDenseN AOs: library-backed SCC on their own stream, one at a time
-  std::vector<int> dense_ids;
-  std::vector<int> dense_n;
-  std::vector<long long> dense_mo;
-  DenseWork dw;
-  DevBuf<double> dense_buf;
-  DevBuf<int> dense_info;
-  cudaStream_t dense_stream = nullptr;
-  cudaEvent_t ev_djoin = nullptr;
+  // molecules above the wide threshold: SCC with each molecule on a group of SMs
+  std::vector<int> wide_ids;
+  int wide_maxn = 0, wide_maxnsh = 0, wide_maxnat = 0;
+  WideRuntime* wide = nullptr;
+  DevBuf<double> wide_buf;
   BlobLayout lay;
   HostBuf h_in, h_out;               // pinned staging
   DevBuf<unsigned char> d_in, d_out; // device blobs
@@ -386,16 +387,9 @@ struct gfn1_batch {
     gx.release();
     gy.release();
     gq.release();
-    dense_buf.release();
-    dense_info.release();
-    if (dw.blas) cublasDestroy((cublasHandle_t)dw.blas);
-    if (dw.solver) cusolverDnDestroy((cusolverDnHandle_t)dw.solver);
-    if (dw.h_state) cudaFreeHost(dw.h_state);
-    dw = DenseWork();
-    if (ev_djoin) cudaEventDestroy(ev_djoin);
-    if (dense_stream) cudaStreamDestroy(dense_stream);
-    ev_djoin = nullptr;
-    dense_stream = nullptr;
+    wide_buf.release();
+    if (wide) wide_runtime_delete(wide);
+    wide = nullptr;
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
     if (side) cudaStreamDestroy(side);
@@ -778,58 +772,54 @@ int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t*
   // A class whose vectors do not fit the per-CTA shared memory gets larger CTAs.
   const int kSplitN = 96;
   const int kClassNt[2] = {128, 128};
-  // above kDenseN AOs one SM per molecule is too slow: library-backed path.
-  // GFN1_DENSE_N overrides the threshold (used by the tests to run both paths
-  // on the same molecules).
-  int kDenseN = 1024;
+  // above kDenseN AOs one SM per molecule is too slow: those molecules run on
+  // groups of SMs (wide.cuh).  GFN1_DENSE_N overrides the threshold (the tests
+  // use it to run both paths on the same molecules).
+  int kDenseN = 256;
   if (const char* dn = std::getenv("GFN1_DENSE_N"))
     if (*dn) kDenseN = std::max(2, std::atoi(dn));
+  constexpr int kWideMaxN = 8192;  // the reduction keeps two N-vectors per CTA in shared memory
   int n_dense = 0;
   while (n_dense < nmol && n_m[h_order[n_dense]] > kDenseN) ++n_dense;
-  b->dense_ids.clear();
-  b->dense_n.clear();
-  b->dense_mo.clear();
-  int dmaxn = 0, dmaxnsh = 0, dmaxnat = 0;
+  b->wide_ids.clear();
+  b->wide_maxn = b->wide_maxnsh = b->wide_maxnat = 0;
   for (int q = 0; q < n_dense; ++q) {
     const int mm = h_order[q];
     if (st_m[mm] != GFN1_OK) continue;
-    b->dense_ids.push_back(mm);
-    b->dense_n.push_back(n_m[mm]);
-    b->dense_mo.push_back(h_mat[mm]);
-    dmaxn = std::max(dmaxn, n_m[mm]);
-    dmaxnsh = std::max(dmaxnsh, nsh_m[mm]);
-    dmaxnat = std::max(dmaxnat, atom_offsets[mm + 1] - atom_offsets[mm]);
+    if (n_m[mm] > kWideMaxN) {
+      h_st[mm] = st_m[mm] = GFN1_E_INVALID_INPUT;
+      worst = std::max(worst, (int)GFN1_E_INVALID_INPUT);
+      if (first_err.empty())
+        first_err = "molecule " + std::to_string(mm) + ": more than " + std::to_string(kWideMaxN) + " basis functions";
+      continue;
+    }
+    b->wide_ids.push_back(mm);
+    b->wide_maxn = std::max(b->wide_maxn, n_m[mm]);
+    b->wide_maxnsh = std::max(b->wide_maxnsh, nsh_m[mm]);
+    b->wide_maxnat = std::max(b->wide_maxnat, atom_offsets[mm + 1] - atom_offsets[mm]);
   }
   b->n_shift = 0;
   if (o.level_shift != 0.0) {
     if (!std::isfinite(o.level_shift)) return fail(eng, GFN1_E_INVALID_INPUT, "level shift must be finite");
+    // molecules on one SM go to the ladder kernel from rung 0; the wide path
+    // applies the shift itself
     std::vector<int> lst;
-    for (int q = 0; q < nmol; ++q) {
+    for (int q = n_dense; q < nmol; ++q) {
       const int mm = h_order[q];
       if (h_st[mm] != GFN1_OK) continue;
-      if (q < n_dense) {  // the library-backed path has no level shift
-        h_st[mm] = st_m[mm] = GFN1_E_INVALID_INPUT;
-        worst = std::max(worst, (int)GFN1_E_INVALID_INPUT);
-        if (first_err.empty())
-          first_err = "molecule " + std::to_string(mm) + ": a level shift is applied up to 1024 AOs only";
-        continue;
-      }
       lst.push_back(mm);
     }
     b->n_shift = (int)lst.size();
-    b->dense_ids.clear();  // every large molecule was rejected above
-    b->dense_n.clear();
-    b->dense_mo.clear();
-    b->host_err = first_err;
-    b->host_err_mol = -1;
-    for (int m = 0; m < nmol && b->host_err_mol < 0; ++m)
-      if (h_st[m] != GFN1_OK) b->host_err_mol = m;
     if (!b->shift_list.ensure(std::max<size_t>(lst.size(), 1)) || !b->shift_count.ensure(1) ||
         (!lst.empty() && cudaMemcpy(b->shift_list.p, lst.data(), sizeof(int) * lst.size(), cudaMemcpyHostToDevice) !=
                              cudaSuccess) ||
         cudaMemcpy(b->shift_count.p, &b->n_shift, sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
       return fail(eng, GFN1_E_DEVICE, "device copy of the level-shift list failed");
   }
+  b->host_err = first_err;
+  b->host_err_mol = -1;
+  for (int m = 0; m < nmol && b->host_err_mol < 0; ++m)
+    if (h_st[m] != GFN1_OK) b->host_err_mol = m;
   int n_large = n_dense;
   while (n_large < nmol && n_m[h_order[n_large]] > kSplitN) ++n_large;
   long long ws_total = 0;
@@ -895,51 +885,25 @@ int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t*
             b->shell_pot.ensure(nshells) && b->shell_pot_in.ensure(nshells) && b->se.ensure(nshells) && b->grad_classic.ensure(3 * natoms) &&
             b->orb_eps.ensure(std::max<long long>(naos, 1)) && b->orb_occ.ensure(std::max<long long>(naos, 1));
   if (!ok) return fail(eng, GFN1_E_DEVICE, "device allocation failed for the batch workspace");
-  if (!b->dense_ids.empty()) {
-    DenseWork& dw = b->dw;
-    if (!dw.blas) {
-      cublasHandle_t hb;
-      cusolverDnHandle_t hs;
-      if (cublasCreate(&hb) != CUBLAS_STATUS_SUCCESS) return fail(eng, GFN1_E_DEVICE, "cublasCreate failed");
-      dw.blas = hb;
-      if (cusolverDnCreate(&hs) != CUSOLVER_STATUS_SUCCESS) return fail(eng, GFN1_E_DEVICE, "cusolverDnCreate failed");
-      dw.solver = hs;
-      if (cudaHostAlloc(&dw.h_state, 4 * sizeof(int), cudaHostAllocDefault) != cudaSuccess)
-        return fail(eng, GFN1_E_DEVICE, "pinned host allocation failed");
-      if (cudaStreamCreateWithFlags(&b->dense_stream, cudaStreamNonBlocking) != cudaSuccess ||
-          cudaEventCreateWithFlags(&b->ev_djoin, cudaEventDisableTiming) != cudaSuccess)
-        return fail(eng, GFN1_E_DEVICE, "stream creation failed");
+  if (!b->wide_ids.empty()) {
+    std::vector<int> Ns, nshs, nats;
+    std::vector<long long> mos, slot_off;
+    long long tot = 0;
+    for (int mm : b->wide_ids) {  // the SCC vectors of every slot use the CtaWs layout of the largest molecule
+      Ns.push_back(n_m[mm]);
+      nshs.push_back(b->wide_maxnsh);
+      nats.push_back(b->wide_maxnat);
+      mos.push_back(h_mat[mm]);
+      slot_off.push_back(tot);
+      tot += wide_slot_doubles(n_m[mm], b->wide_maxnsh, b->wide_maxnat, b->cap);
     }
-    const long long lwork = dense_solver_lwork(dw.solver, dmaxn);
-    if (lwork < 0) return fail(eng, GFN1_E_DEVICE, "cuSOLVER workspace query failed");
-    const long long n2 = (long long)dmaxn * dmaxn;
-    const long long wsd = dense_ws_doubles(dmaxnsh, b->cap, dmaxnat);
-    const long long stated = ((long long)dense_state_bytes() + 7) / 8;
-    const long long total = 6 * n2 + 4LL * dmaxn + lwork + wsd + stated + 64;
-    if (!b->dense_buf.ensure((size_t)total) || !b->dense_info.ensure(4))
+    if (!b->wide) b->wide = wide_runtime_new();
+    if (!b->wide_buf.ensure((size_t)std::max<long long>(tot, 1)))
       return fail(eng, GFN1_E_DEVICE, "device allocation failed for the large-molecule path");
-    if (dense_smem_bytes(dmaxnsh, dmaxn, dmaxnat) > 200 * 1024)
+    if (dense_table_bytes_host(b->wide_maxnsh, b->wide_maxn, b->wide_maxnat) > 200 * 1024)
       return fail(eng, GFN1_E_INVALID_INPUT, "molecule too large for the large-molecule path's index tables");
-    double* p = b->dense_buf.p;
-    dw.maxn = dmaxn;
-    dw.maxnsh = dmaxnsh;
-    dw.maxnat = dmaxnat;
-    dw.cap = b->cap;
-    dw.L = p; p += n2;
-    dw.Hp = p; p += n2;
-    dw.Mm = p; p += n2;
-    dw.F = p; p += n2;
-    dw.C = p; p += n2;
-    dw.D = p; p += n2;
-    dw.eps = p; p += dmaxn;
-    dw.occ = p; p += dmaxn;
-    dw.pop = p; p += dmaxn;
-    dw.vao = p; p += dmaxn;
-    dw.solver_work = p; p += lwork;
-    dw.lwork = lwork;
-    dw.ws = p; p += wsd;
-    dw.state = p;
-    dw.info = b->dense_info.p;
+    cudaError_t e = wide_bind_runtime(b->wide, b->wide_ids, Ns, mos, nshs, nats, b->cap, b->wide_buf.p, slot_off);
+    if (e != cudaSuccess) return cuda_fail(eng, e, "large-molecule path set-up");
   }
   b->guess = eng->guess;
   if (b->guess && !(b->gx.ensure((size_t)kGuessIn * std::max<long long>(natoms, 1)) &&
@@ -1039,17 +1003,10 @@ int launch_stage(gfn1_batch* b, int stage, cudaStream_t st) {
       if ((e = launch_scc_robust(R.nt, R.n_cta, R.smem, st, B, M, so, SL)) != cudaSuccess)
         return cuda_fail(eng, e, "scc fallback launch");
     }
-    if (!b->dense_ids.empty()) {  // large molecules: host-driven, one at a time, next to the class launches
-      // wait for the setup kernel only (ev_fork was recorded before the class launches)
-      if ((e = cudaStreamWaitEvent(b->dense_stream, b->ev_fork, 0)) != cudaSuccess)
-        return cuda_fail(eng, e, "stream fork");
-      for (size_t q = 0; q < b->dense_ids.size(); ++q)
-        if ((e = run_dense_molecule(B, M, so, b->dense_ids[q], b->dense_n[q], b->dense_mo[q], b->dw, b->dense_stream)) !=
-            cudaSuccess)
-          return cuda_fail(eng, e, "large-molecule SCC");
-      if ((e = cudaEventRecord(b->ev_djoin, b->dense_stream)) != cudaSuccess ||
-          (e = cudaStreamWaitEvent(st, b->ev_djoin, 0)) != cudaSuccess)
-        return cuda_fail(eng, e, "stream join");
+    if (!b->wide_ids.empty()) {  // large molecules on groups of SMs, after the one-SM classes
+      if ((e = wide_run(B, M, so, b->wide, (int)b->wide_ids.size(), b->wide_maxn, b->wide_maxnsh, b->wide_maxnat,
+                        b->cap, eng->num_sms, st)) != cudaSuccess)
+        return cuda_fail(eng, e, "large-molecule SCC");
     }
   } else if (stage == 2) {
     if (!b->opt.compute_gradient) return GFN1_OK;

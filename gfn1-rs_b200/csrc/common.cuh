@@ -82,22 +82,6 @@ struct SccLaunch {
   int smem_bytes;       // dynamic shared memory of the launch
 };
 
-// Device buffers of the large-molecule path (one molecule at a time, sized for
-// the largest such molecule of the batch).  Matrices are column-major N x N.
-struct DenseWork {
-  int maxn = 0, maxnsh = 0, maxnat = 0, cap = 0;
-  double *L = nullptr, *Hp = nullptr, *Mm = nullptr, *F = nullptr, *C = nullptr, *D = nullptr;
-  double *eps = nullptr, *occ = nullptr, *pop = nullptr, *vao = nullptr;
-  double* ws = nullptr;           // SCC vectors and Broyden history (CtaWs layout)
-  double* solver_work = nullptr;  // cuSOLVER workspace
-  long long lwork = 0;            // doubles in solver_work
-  int* info = nullptr;            // cuSOLVER info
-  void* state = nullptr;          // per-molecule SCC state (device)
-  int* h_state = nullptr;         // pinned host copy of the state's first three ints (status, nocc, converged)
-  void* blas = nullptr;           // cublasHandle_t
-  void* solver = nullptr;         // cusolverDnHandle_t
-};
-
 // Everything a kernel needs about a batch of molecules.  All pointers are
 // device pointers; offsets index the flat per-batch arrays.
 struct Batch {

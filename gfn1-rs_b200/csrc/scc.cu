@@ -31,8 +31,6 @@
 // Fermi smearing (bisection to the bracket fixed point, :3853-3921), the
 // convergence test (:1881), Broyden mixing (:3203-3309, :3759-3806) and the final
 // energy assembly (:1957-2053) follow the reference step by step.
-#include <cublas_v2.h>
-#include <cusolverDn.h>
 #include <float.h>
 
 #include "common.cuh"
@@ -711,52 +709,58 @@ __device__ void tridiagonalize_blocked(double* A, int lda, int N, double* d, dou
 // tridiagonal eigenproblem - revisited", SIAM J. Sci. Comput. 15, 1994).
 // Every evaluation also tightens the bisection bracket, and a step that leaves
 // it falls back to bisection.
+// Eigenvalue k of the tridiagonal (one thread).
+__device__ __forceinline__ double eigenvalue_k(const double* d, const double* esq, int N, int k, double gl, double gu,
+                                              double pivmin, double atol) {
+  const double dn = (double)N;
+  double lo = gl, hi = gu;
+  double x = 0.5 * (lo + hi);
+  for (int it = 0; it < 160; ++it) {
+    double p, dp, ddp;
+    const int c = sturm_poly(d, esq, N, x, pivmin, p, dp, ddp);
+    if (c >= k + 1)
+      hi = x;
+    else
+      lo = x;
+    const double tol = 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)) + atol;
+    if (hi - lo <= tol) {
+      x = 0.5 * (lo + hi);
+      break;
+    }
+    double xn = 0.5 * (lo + hi);
+    if (c == k || c == k + 1) {
+      // u = p/p', w = p p''/p'^2; step = N u / (1 + sigma sqrt((N-1)(N(1-w)-1)))
+      // with sigma chosen so that the step moves toward eigenvalue k.
+      const double u = p / dp;
+      const double w = (p * ddp) / (dp * dp);
+      const double sq = sqrt((dn - 1.0) * (dn * (1.0 - w) - 1.0));
+      const bool up = (c == k);
+      const double sigma = ((u > 0.0) == up) ? -1.0 : 1.0;
+      const double step = dn * u / (1.0 + sigma * sq);
+      const double xt = x - step;
+      // The Newton ratio u points to the nearest eigenvalue: when it points
+      // away from eigenvalue k, x sits next to the neighbour on the other
+      // side, where the Laguerre step is tiny and proves nothing.
+      const bool nearest = up ? (u < 0.0) : (u > 0.0);
+      if (nearest && fabs(step) <= 32.0 * tol) {  // cubic convergence: the step bounds the error
+        x = fmin(fmax(xt, lo), hi);
+        break;
+      }
+      if (xt > lo && xt < hi && (nearest || fabs(step) >= 0.125 * (hi - lo))) xn = xt;
+    }
+    if (xn <= lo || xn >= hi) break;
+    x = xn;
+  }
+  return x;
+}
+
 template <int NT>
 __device__ void eigenvalues(const double* d, const double* esq, int N, int nneed, double gl, double gu,
                             double pivmin, double atol, double* eps) {
   const int nlist = (nneed < N) ? nneed + 1 : N;
-  const double dn = (double)N;
   for (int slot = threadIdx.x; slot < nlist; slot += NT) {
     const int k = (slot < nneed) ? slot : N - 1;
-    double lo = gl, hi = gu;
-    double x = 0.5 * (lo + hi);
-    for (int it = 0; it < 160; ++it) {
-      double p, dp, ddp;
-      const int c = sturm_poly(d, esq, N, x, pivmin, p, dp, ddp);
-      if (c >= k + 1)
-        hi = x;
-      else
-        lo = x;
-      const double tol = 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)) + atol;
-      if (hi - lo <= tol) {
-        x = 0.5 * (lo + hi);
-        break;
-      }
-      double xn = 0.5 * (lo + hi);
-      if (c == k || c == k + 1) {
-        // u = p/p', w = p p''/p'^2; step = N u / (1 + sigma sqrt((N-1)(N(1-w)-1)))
-        // with sigma chosen so that the step moves toward eigenvalue k.
-        const double u = p / dp;
-        const double w = (p * ddp) / (dp * dp);
-        const double sq = sqrt((dn - 1.0) * (dn * (1.0 - w) - 1.0));
-        const bool up = (c == k);
-        const double sigma = ((u > 0.0) == up) ? -1.0 : 1.0;
-        const double step = dn * u / (1.0 + sigma * sq);
-        const double xt = x - step;
-        // The Newton ratio u points to the nearest eigenvalue: when it points
-        // away from eigenvalue k, x sits next to the neighbour on the other
-        // side, where the Laguerre step is tiny and proves nothing.
-        const bool nearest = up ? (u < 0.0) : (u > 0.0);
-        if (nearest && fabs(step) <= 32.0 * tol) {  // cubic convergence: the step bounds the error
-          x = fmin(fmax(xt, lo), hi);
-          break;
-        }
-        if (xt > lo && xt < hi && (nearest || fabs(step) >= 0.125 * (hi - lo))) xn = xt;
-      }
-      if (xn <= lo || xn >= hi) break;
-      x = xn;
-    }
-    eps[k] = x;
+    eps[k] = eigenvalue_k(d, esq, N, k, gl, gu, pivmin, atol);
   }
   __syncthreads();
 }
@@ -1898,18 +1902,8 @@ __global__ void __launch_bounds__(NT, 512 / NT) scc_kernel(Batch B, Model M, Scc
 }
 
 // ============================================================ large molecules
-// Molecules too large for one SM run the same SCC (same stage functions for
-// potential, charges, energies, mixing and results) with the matrix algebra
-// spread over the whole GPU: cuSOLVER Cholesky and symmetric eigensolver,
-// cuBLAS triangular products and GEMMs, and element-wise kernels.  All
-// matrices are column-major; S, H0, P and W are symmetric, so the batch's
-// row-major copies are used as they are.
-
-struct DenseState {
-  int status, nocc, converged, iter, bro_iter, have_e, spin;
-  double last_e, e_el, e2, e3, ts, mu, rms, nelec, kt, nalpha, nbeta;
-};
-constexpr int kDenseNT = 512;
+// Molecules too large for one SM run on many SMs: the kernels of wide.cuh
+// (included at the end of this file) share the stage functions above.
 
 __host__ __device__ inline size_t dense_table_bytes(int maxnsh, int maxn, int maxnat) {
   return ((size_t)4 * scc_ints(maxnsh, maxn, maxnat) + 15) & ~(size_t)15;
@@ -1926,291 +1920,6 @@ __device__ DenseTables dense_tables(unsigned char* raw, int maxnsh, int maxn) {
   t.ao_sh = t.sh_ao0 + maxnsh;
   t.atom_sh = t.ao_sh + maxn;
   return t;
-}
-
-// Index tables in shared memory and the molecule context, for the one-CTA
-// kernels of the large path.
-__device__ MolCtx dense_context(const Batch& B, const Model& M, int m, const DenseWork& dw, unsigned char* raw) {
-  const int a0 = B.atom_off[m], nat = B.atom_off[m + 1] - a0;
-  const int sh0 = B.shell_off[m], nsh = B.shell_off[m + 1] - sh0;
-  const int N = B.ao_off[m + 1] - B.ao_off[m];
-  DenseTables t = dense_tables(raw, dw.maxnsh, dw.maxn);
-  if (threadIdx.x == 0) build_index_tables(B, M, a0, nat, t.sh_atom, t.sh_k, t.sh_ao0, t.ao_sh, t.atom_sh);
-  __syncthreads();
-  return MolCtx{m, a0, nat, sh0, nsh, N, t.sh_atom, t.sh_k, t.sh_ao0, t.ao_sh, t.atom_sh, B.gam + B.gam_off[m]};
-}
-
-__global__ void __launch_bounds__(kDenseNT, 1) dense_init_kernel(Batch B, Model M, SccOptions opt, int m, DenseWork dw) {
-  extern __shared__ __align__(16) unsigned char raw[];
-  const MolCtx c = dense_context(B, M, m, dw, raw);
-  DenseState* st = (DenseState*)dw.state;
-  CtaWs w = cta_ws(dw.ws, 1, dw.maxnsh, dw.cap);
-  for (int s = threadIdx.x; s < c.nsh; s += kDenseNT) w.qin[s] = B.init_q ? B.init_q[c.sh0 + s] : 0.0;
-  if (threadIdx.x == 0) {
-    double nref = 0.0;
-    for (int s = 0; s < c.nsh; ++s) nref += M.elem[B.z[c.a0 + c.sh_atom[s]]].refocc[c.sh_k[s]];
-    // the reference rejects overlaps with an eigenvalue <= 1e-12; here a Cholesky pivot <= 1e-12
-    bool ok = dw.info[0] == 0;
-    for (int k = 0; k < c.N && ok; ++k) {
-      const double l = dw.L[(long long)k * c.N + k];
-      ok = l * l > 1e-12;
-    }
-    st->status = ok ? kOk : kErrInvalidInput;
-    st->nocc = 0;
-    st->converged = 0;
-    st->iter = 0;
-    st->bro_iter = 0;
-    st->have_e = 0;
-    st->last_e = st->e_el = st->e2 = st->e3 = st->ts = st->mu = st->rms = 0.0;
-    st->nelec = nref - B.charge[m];
-    st->kt = fmax(opt.etemp, 0.0) * kBoltzmann;
-    st->spin = opt.spin_mult > 0;
-    st->nalpha = st->spin ? 0.5 * (rint(st->nelec) + (opt.spin_mult - 1)) : 0.0;
-    st->nbeta = st->spin ? 0.5 * (rint(st->nelec) - (opt.spin_mult - 1)) : 0.0;
-    if (!ok) {
-      B.status[m] = kErrInvalidInput;
-      B.iterations[m] = 0;
-    }
-  }
-}
-
-__global__ void __launch_bounds__(kDenseNT, 1) dense_potential_kernel(Batch B, Model M, int m, DenseWork dw) {
-  extern __shared__ __align__(16) unsigned char raw[];
-  const MolCtx c = dense_context(B, M, m, dw, raw);
-  CtaWs w = cta_ws(dw.ws, 1, dw.maxnsh, dw.cap);
-  stage_potential<kDenseNT>(B, M, c, w, dw.vao);
-}
-
-// Mm = diag(v) L (lower triangle of L, column-major)
-__global__ void dense_scale_rows_kernel(int N, const double* __restrict__ L, const double* __restrict__ v,
-                                        double* __restrict__ Mm) {
-  const long long n2 = (long long)N * N;
-  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n2; idx += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(idx % N), j = (int)(idx / N);
-    Mm[idx] = i >= j ? v[i] * L[idx] : 0.0;
-  }
-}
-
-// F' = H0' - (Mm + Mm^T)/2 with Mm = L^-1 diag(v) L
-__global__ void dense_fock_kernel(int N, const double* __restrict__ Hp, const double* __restrict__ Mm,
-                                  double* __restrict__ F) {
-  const long long n2 = (long long)N * N;
-  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n2; idx += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(idx % N), j = (int)(idx / N);
-    F[idx] = Hp[idx] - 0.5 * (Mm[idx] + Mm[(long long)i * N + j]);
-  }
-}
-
-__global__ void __launch_bounds__(kDenseNT, 1) dense_fermi_kernel(int N, DenseWork dw) {
-  __shared__ SccShared sh;
-  DenseState* st = (DenseState*)dw.state;
-  const double nelec = st->nelec, kt = st->kt;
-  const int tid = threadIdx.x;
-  if (st->spin) {
-    spin_channel_occupations<kDenseNT>(dw.eps, N, N, st->nalpha, st->nbeta, kt, dw.occ, dw.pop, sh);
-  } else if (kt > 0.0 && nelec > 0.0 && nelec < 2.0 * N) {
-    double fm, ft;
-    bool amb;
-    fermi_cta<kDenseNT, 2>(dw.eps, N, N, nelec, kt, dw.occ, sh, fm, ft, amb);
-    if (tid == 0) {
-      sh.scal[1] = fm;
-      sh.scal[2] = ft;
-    }
-  } else if (tid < 32) {
-    double fm, ft;
-    bool amb;
-    fermi_warp<2>(dw.eps, N, N, nelec, kt, dw.occ, fm, ft, amb);
-    if (tid == 0) {
-      sh.scal[1] = fm;
-      sh.scal[2] = ft;
-    }
-  }
-  __syncthreads();
-  int nocc_loc = 0;
-  for (int i = tid; i < N; i += kDenseNT)
-    if (dw.occ[i] > 1e-30) nocc_loc = max(nocc_loc, i + 1);
-  const int nocc = (int)block_max((double)nocc_loc, sh.red);
-  if (tid == 0) {
-    st->mu = sh.scal[1];
-    st->ts = sh.scal[2];
-    st->nocc = nocc;
-  }
-}
-
-// pop_mu = sum_i occ_i C_mu,i D_mu,i, C = L^-T Z, D = L Z (column-major, ld N)
-__global__ void dense_pop_kernel(int N, int nocc, const double* __restrict__ occ, const double* __restrict__ C,
-                                 const double* __restrict__ D, double* __restrict__ pop) {
-  const int mu = blockIdx.x * blockDim.x + threadIdx.x;
-  if (mu >= N) return;
-  double p = 0.0;
-  for (int i = 0; i < nocc; ++i) p += occ[i] * C[(long long)i * N + mu] * D[(long long)i * N + mu];
-  pop[mu] = p;
-}
-
-__global__ void __launch_bounds__(kDenseNT, 1) dense_energy_mix_kernel(Batch B, Model M, SccOptions opt, int m,
-                                                                       int iter, DenseWork dw) {
-  extern __shared__ __align__(16) unsigned char raw[];
-  __shared__ SccShared sh;
-  const MolCtx c = dense_context(B, M, m, dw, raw);
-  CtaWs w = cta_ws(dw.ws, 1, dw.maxnsh, dw.cap);
-  DenseState* st = (DenseState*)dw.state;
-  double e_el, e2, e3, rms;
-  stage_charges_energy<kDenseNT>(B, M, c, w, dw.pop, dw.occ, dw.eps, dw.vao, st->nocc, sh, e_el, e2, e3, rms);
-  const double escc = e_el + e2 + e3 + st->ts;
-  const double err = st->have_e ? fabs(escc - st->last_e) : INFINITY;
-  const bool converged = err < opt.energy_tol && rms < opt.charge_tol;
-  __syncthreads();
-  if (!converged) {
-    int bro = st->bro_iter;
-    stage_mix<kDenseNT>(opt, c, w, dw.cap, bro, sh);
-    if (threadIdx.x == 0) st->bro_iter = bro;
-  }
-  if (threadIdx.x == 0) {
-    st->e_el = e_el;
-    st->e2 = e2;
-    st->e3 = e3;
-    st->rms = rms;
-    st->iter = iter;
-    st->converged = converged ? 1 : 0;
-    if (!converged) {
-      st->last_e = escc;
-      st->have_e = 1;
-    }
-  }
-}
-
-__global__ void __launch_bounds__(kDenseNT, 1) dense_results_kernel(Batch B, Model M, int m, DenseWork dw) {
-  extern __shared__ __align__(16) unsigned char raw[];
-  const MolCtx c = dense_context(B, M, m, dw, raw);
-  CtaWs w = cta_ws(dw.ws, 1, dw.maxnsh, dw.cap);
-  const DenseState* st = (const DenseState*)dw.state;
-  stage_results<kDenseNT>(B, c, w, st->iter, st->converged != 0, st->e_el, st->e2, st->e3, st->ts, st->mu);
-  if (B.orb_eps) {  // the full spectrum from the library eigensolver
-    const int ao0 = B.ao_off[m];
-    for (int i = threadIdx.x; i < c.N; i += blockDim.x) {
-      B.orb_eps[ao0 + i] = dw.eps[i];
-      B.orb_occ[ao0 + i] = dw.occ[i];
-    }
-  }
-}
-
-// out[:, i] = scale_i * in[:, i] with scale = occ (weight 0) or occ * eps (weight 1)
-__global__ void dense_scale_cols_kernel(int N, int nocc, const double* __restrict__ in, const double* __restrict__ occ,
-                                        const double* __restrict__ eps, int weight, double* __restrict__ out) {
-  const long long n2 = (long long)N * nocc;
-  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n2; idx += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(idx / N);
-    out[idx] = in[idx] * (weight ? occ[i] * eps[i] : occ[i]);
-  }
-}
-
-long long dense_ws_doubles(int maxnsh, int cap, int maxnat) { return cta_ws_size(1, maxnsh, cap, maxnat); }
-size_t dense_smem_bytes(int maxnsh, int maxn, int maxnat) { return dense_table_bytes(maxnsh, maxn, maxnat); }
-size_t dense_state_bytes() { return sizeof(DenseState); }
-
-// Solver workspace (doubles) for N: max of potrf and syevd.
-long long dense_solver_lwork(void* solver, int N) {
-  cusolverDnHandle_t hs = (cusolverDnHandle_t)solver;
-  int l1 = 0, l2 = 0;
-  if (cusolverDnDpotrf_bufferSize(hs, CUBLAS_FILL_MODE_LOWER, N, nullptr, N, &l1) != CUSOLVER_STATUS_SUCCESS) return -1;
-  if (cusolverDnDsyevd_bufferSize(hs, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, N, nullptr, N, nullptr, &l2) !=
-      CUSOLVER_STATUS_SUCCESS)
-    return -1;
-  return (long long)(l1 > l2 ? l1 : l2);
-}
-
-// One large molecule, start to finish, on stream st.  Synchronises st once per
-// SCC iteration (the occupied count and the convergence flag).  Returns
-// cudaErrorUnknown when a library call fails.
-cudaError_t run_dense_molecule(const Batch& B, const Model& M, const SccOptions& opt, int m, int N, long long mo,
-                               DenseWork& dw, cudaStream_t st) {
-  cublasHandle_t hb = (cublasHandle_t)dw.blas;
-  cusolverDnHandle_t hs = (cusolverDnHandle_t)dw.solver;
-  if (cublasSetStream(hb, st) != CUBLAS_STATUS_SUCCESS || cusolverDnSetStream(hs, st) != CUSOLVER_STATUS_SUCCESS)
-    return cudaErrorUnknown;
-  const size_t n2b = sizeof(double) * (size_t)N * N;
-  const size_t smem = dense_table_bytes(dw.maxnsh, dw.maxn, dw.maxnat);
-  const int ew_blocks = 4 * 148, ew_threads = 256;
-  const double one = 1.0, zero = 0.0;
-  cudaError_t e;
-  static int configured_dev = -1;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (configured_dev != dev) {
-    for (const void* k : {(const void*)dense_init_kernel, (const void*)dense_potential_kernel,
-                          (const void*)dense_energy_mix_kernel, (const void*)dense_results_kernel})
-      if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024)) != cudaSuccess)
-        return e;
-    configured_dev = dev;
-  }
-  if (smem > 200 * 1024) return cudaErrorInvalidValue;
-  // orthogonaliser: S = L L^T, H0' = L^-1 H0 L^-T
-  if ((e = cudaMemcpyAsync(dw.L, B.S + mo, n2b, cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e;
-  if ((e = cudaMemcpyAsync(dw.Hp, B.H0 + mo, n2b, cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e;
-  if (cusolverDnDpotrf(hs, CUBLAS_FILL_MODE_LOWER, N, dw.L, N, dw.solver_work, (int)dw.lwork, dw.info) !=
-      CUSOLVER_STATUS_SUCCESS)
-    return cudaErrorUnknown;
-  if (cublasDtrsm(hb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, N, N, &one, dw.L, N,
-                  dw.Hp, N) != CUBLAS_STATUS_SUCCESS ||
-      cublasDtrsm(hb, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, N, N, &one, dw.L,
-                  N, dw.Hp, N) != CUBLAS_STATUS_SUCCESS)
-    return cudaErrorUnknown;
-  // status, nocc, converged: the first three ints of DenseState, read back at each sync point
-  auto read_flags = [&]() -> cudaError_t {
-    cudaError_t r = cudaGetLastError();
-    if (r == cudaSuccess) r = cudaMemcpyAsync(dw.h_state, dw.state, 3 * sizeof(int), cudaMemcpyDeviceToHost, st);
-    if (r == cudaSuccess) r = cudaStreamSynchronize(st);
-    return r;
-  };
-  dense_init_kernel<<<1, kDenseNT, smem, st>>>(B, M, opt, m, dw);
-  if ((e = read_flags()) != cudaSuccess) return e;
-  if (dw.h_state[0] != kOk) return cudaSuccess;  // status already written
-  int iter = 1;
-  for (; iter <= opt.max_scc; ++iter) {
-    dense_potential_kernel<<<1, kDenseNT, smem, st>>>(B, M, m, dw);
-    dense_scale_rows_kernel<<<ew_blocks, ew_threads, 0, st>>>(N, dw.L, dw.vao, dw.Mm);
-    if (cublasDtrsm(hb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, N, N, &one, dw.L,
-                    N, dw.Mm, N) != CUBLAS_STATUS_SUCCESS)
-      return cudaErrorUnknown;
-    dense_fock_kernel<<<ew_blocks, ew_threads, 0, st>>>(N, dw.Hp, dw.Mm, dw.F);
-    if (cusolverDnDsyevd(hs, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, N, dw.F, N, dw.eps, dw.solver_work,
-                         (int)dw.lwork, dw.info) != CUSOLVER_STATUS_SUCCESS)
-      return cudaErrorUnknown;
-    dense_fermi_kernel<<<1, kDenseNT, 0, st>>>(N, dw);
-    if ((e = read_flags()) != cudaSuccess) return e;
-    const int nocc = dw.h_state[1];
-    if (nocc > 0) {
-      if ((e = cudaMemcpyAsync(dw.C, dw.F, sizeof(double) * (size_t)N * nocc, cudaMemcpyDeviceToDevice, st)) !=
-          cudaSuccess)
-        return e;
-      if (cublasDtrsm(hb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, N, nocc, &one,
-                      dw.L, N, dw.C, N) != CUBLAS_STATUS_SUCCESS ||
-          cublasDtrmm(hb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, N, nocc, &one,
-                      dw.L, N, dw.F, N, dw.D, N) != CUBLAS_STATUS_SUCCESS)
-        return cudaErrorUnknown;
-    }
-    dense_pop_kernel<<<(N + 255) / 256, 256, 0, st>>>(N, nocc, dw.occ, dw.C, dw.D, dw.pop);
-    dense_energy_mix_kernel<<<1, kDenseNT, smem, st>>>(B, M, opt, m, iter, dw);
-    if ((e = read_flags()) != cudaSuccess) return e;
-    if (dw.h_state[2]) break;
-  }
-  dense_results_kernel<<<1, kDenseNT, smem, st>>>(B, M, m, dw);
-  // P = C diag(f) C^T and W = C diag(f eps) C^T of the last diagonalisation
-  const int nocc = dw.h_state[1];
-  if (nocc > 0) {
-    dense_scale_cols_kernel<<<ew_blocks, ew_threads, 0, st>>>(N, nocc, dw.C, dw.occ, dw.eps, 0, dw.D);
-    if (cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, N, N, nocc, &one, dw.D, N, dw.C, N, &zero, B.P + mo, N) !=
-        CUBLAS_STATUS_SUCCESS)
-      return cudaErrorUnknown;
-    dense_scale_cols_kernel<<<ew_blocks, ew_threads, 0, st>>>(N, nocc, dw.C, dw.occ, dw.eps, 1, dw.D);
-    if (cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, N, N, nocc, &one, dw.D, N, dw.C, N, &zero, B.W + mo, N) !=
-        CUBLAS_STATUS_SUCCESS)
-      return cudaErrorUnknown;
-  } else {
-    if ((e = cudaMemsetAsync(B.P + mo, 0, n2b, st)) != cudaSuccess || (e = cudaMemsetAsync(B.W + mo, 0, n2b, st)) != cudaSuccess)
-      return e;
-  }
-  return cudaGetLastError();
 }
 
 long long scc_workspace_doubles(int maxn, int maxnsh, int cap, int maxnat) {
@@ -2267,3 +1976,5 @@ cudaError_t launch_scc_robust(int nt, int grid, size_t smem, cudaStream_t st, co
 }
 
 }  // namespace gfn1
+
+#include "wide.cuh"

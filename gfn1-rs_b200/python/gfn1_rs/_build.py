@@ -11,7 +11,7 @@ LIB_PATH = os.path.join(LIB_DIR, "libgfn1_b200.so")
 SOURCES = ("setup.cu", "scc.cu", "grad.cu", "guess.cu", "capi.cu")
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
-    "-Xcompiler", "-fPIC", "-shared", "-lcublas", "-lcusolver",
+    "-Xcompiler", "-fPIC", "-shared",
 ]
 
 

@@ -1,6 +1,7 @@
-"""The large-molecule path (cuSOLVER eigensolver, cuBLAS triangular products,
-the same SCC stage functions) against the one-CTA-per-molecule path and the
-oracle.
+"""The large-molecule path (each molecule on a group of SMs: blocked Cholesky,
+cooperative Householder reduction, Sturm/Laguerre eigenvalues, inverse
+iteration, tensor-core back-transformation; the same SCC stage functions)
+against the one-CTA-per-molecule path and the oracle.
 
 Tolerances: between the two device paths |dE| <= 1e-9 Eh, |dg| <= 1e-8 Eh/bohr,
 |dq| <= 1e-8 e at tight convergence; against the oracle the parity bar
@@ -93,3 +94,47 @@ def test_large_systems_match_oracle(gpu_calc):
         dq = np.abs(r.shell_charges - np.array(rec["shell_charges"])).max()
         print(f"{len(z)} atoms: dE {de:.2e} dg {dg:.2e} dq {dq:.2e} iterations {r.iterations[0]} vs {rec['iterations']}")
         assert de <= 1e-6 and dg <= 1e-5 and dq <= 1e-5
+
+
+def test_mixed_sizes_in_one_call_match_the_cta_path(gpu_calc):
+    """Large molecules of different sizes in one call run in lockstep on the
+    many-SM path (threshold 100 AOs) next to small ones on the one-CTA path;
+    every molecule equals its one-CTA result."""
+    from gfn1_rs import workloads
+    zs, xs, off = [], [], [0]
+    for k, seed in ((13, 5), (3, 6), (20, 7), (9, 8), (17, 9)):
+        z, x = workloads.water_cluster(k, seed)
+        zs.append(z), xs.append(x * A2B), off.append(off[-1] + len(z))
+    off = np.asarray(off, np.int32)
+    z, x = np.concatenate(zs), np.concatenate(xs)
+    ref = _run(off, z, x, **TIGHT)
+    got = _run(off, z, x, dense_n=100, **TIGHT)
+    assert np.all(ref.status == 0) and np.all(got.status == 0)
+    assert np.abs(got.energy - ref.energy).max() <= 1e-9
+    assert np.abs(got.gradient - ref.gradient).max() <= 1e-8
+    assert np.abs(got.shell_charges - ref.shell_charges).max() <= 1e-8
+    assert np.array_equal(got.iterations, ref.iterations)
+
+
+def test_fallback_ladder_on_the_large_molecule_path(gpu_calc, oracle_mod, fixtures):
+    """C-Br...O needs rung 1 of the reference's ladder (linear mixing with a
+    level shift, src/electronic.rs:1413-1447); on the many-SM path it takes the
+    same rung as the oracle and lands on the oracle's energy."""
+    from gfn1_rs import BatchCalculator
+    rec = fixtures["halogen_tests"]["CBr...O"]
+    z, x = np.array(rec["numbers"]), np.array(rec["positions_angstrom"]) * A2B
+    off = np.array([0, len(z)], np.int32)
+    old = os.environ.get("GFN1_DENSE_N")
+    os.environ["GFN1_DENSE_N"] = "8"
+    try:
+        r = BatchCalculator().calculate_flat(off, z, x)
+    finally:
+        if old is None:
+            os.environ.pop("GFN1_DENSE_N", None)
+        else:
+            os.environ["GFN1_DENSE_N"] = old
+    o = oracle_mod.run(z, x)
+    assert r.status[0] == 0 and r.rung[0] == o.rung == 1
+    assert abs(r.energy[0] - o.energy) <= 1e-6
+    assert np.abs(r.gradient - o.gradient).max() <= 1e-5
+

@@ -112,8 +112,8 @@ def test_every_element_in_one_batch(calc, oracle_mod):
 
 
 def test_d_elements_on_the_large_molecule_path(oracle_mod, fixtures):
-    """The same molecules through the cuSOLVER path (size threshold lowered to
-    16 AOs) agree with the one-CTA path and the oracle."""
+    """The same molecules through the many-SM large-molecule path (size
+    threshold lowered to 16 AOs) agree with the one-CTA path and the oracle."""
     from gfn1_rs import BatchCalculator
 
     names = ["ferrocene", "phosphine"]

@@ -40,8 +40,11 @@ def test_level_shift_matches_oracle(gpu_calc, oracle_mod, fixtures, shift):
         assert r.rung[m] == o.rung and plain.rung[m] == 0, NAMES[m]
 
 
-def test_level_shift_rejected_on_the_large_molecule_path(gpu_calc, fixtures):
-    from gfn1_rs import BatchCalculator, Gfn1Error
+def test_level_shift_on_the_large_molecule_path(gpu_calc, oracle_mod, fixtures):
+    """A requested level shift on the many-SM path (caffeine above a lowered
+    threshold, water below it) lands on the oracle's level-shifted energy on
+    rung 0, like the one-CTA path."""
+    from gfn1_rs import BatchCalculator
 
     mols = [smoke_molecule(fixtures, n) for n in ("water", "caffeine")]
     off, z, x = _flat(mols)
@@ -50,14 +53,19 @@ def test_level_shift_rejected_on_the_large_molecule_path(gpu_calc, fixtures):
     os.environ["GFN1_DENSE_N"] = "16"  # caffeine above the threshold, water below
     try:
         r = calc.calculate_flat(off, z, x)
-        with pytest.raises(Gfn1Error, match="level shift"):
-            calc.calculate_flat(off, z, x, raise_on_error=True)
     finally:
         if old is None:
             os.environ.pop("GFN1_DENSE_N", None)
         else:
             os.environ["GFN1_DENSE_N"] = old
-    assert r.status[0] == 0 and r.status[1] == 3
+    ref = calc.calculate_flat(off, z, x)
+    assert np.all(r.status == 0) and np.all(ref.status == 0)
+    for m, (zm, xm) in enumerate(mols):
+        o = oracle_mod.run(zm, xm, options=oracle_mod.make_options(level_shift=0.2, **TIGHT))
+        assert r.rung[m] == o.rung == 0
+        assert abs(r.energy[m] - o.energy) <= 1e-6
+        assert abs(r.energy[m] - ref.energy[m]) <= 1e-9
+        assert np.abs(r.gradient - ref.gradient).max() <= 1e-7
 
 
 def test_native_calculator_level_shift(gpu_calc, oracle_mod, fixtures):

