@@ -709,12 +709,15 @@ __device__ void tridiagonalize_blocked(double* A, int lda, int N, double* d, dou
 // tridiagonal eigenproblem - revisited", SIAM J. Sci. Comput. 15, 1994).
 // Every evaluation also tightens the bisection bracket, and a step that leaves
 // it falls back to bisection.
-// Eigenvalue k of the tridiagonal (one thread).
+// Eigenvalue k of the tridiagonal (one thread).  x0: a first iterate inside
+// (gl, gu), e.g. the eigenvalue of the previous SCC iteration (the search then
+// usually starts next to eigenvalue k and takes Laguerre steps at once);
+// otherwise the midpoint.
 __device__ __forceinline__ double eigenvalue_k(const double* d, const double* esq, int N, int k, double gl, double gu,
-                                              double pivmin, double atol) {
+                                              double pivmin, double atol, double x0 = 0.0, bool warm = false) {
   const double dn = (double)N;
   double lo = gl, hi = gu;
-  double x = 0.5 * (lo + hi);
+  double x = (warm && x0 > lo && x0 < hi) ? x0 : 0.5 * (lo + hi);
   for (int it = 0; it < 160; ++it) {
     double p, dp, ddp;
     const int c = sturm_poly(d, esq, N, x, pivmin, p, dp, ddp);

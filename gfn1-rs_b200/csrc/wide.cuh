@@ -161,6 +161,7 @@ struct GroupSync {
   int err;
   int pad;
 };
+constexpr int kFlagSlots = 1024;  // per-CTA flags of one molecule's group (at least kWideMaxG)
 constexpr long long kSpinCycles = 2000000000LL;
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
@@ -172,6 +173,51 @@ __device__ __forceinline__ int ld_relaxed_i32(const int* p) {
   int v;
   asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Barrier among CTAs 0..n-1 of a group by per-CTA flags: CTA c publishes
+// `target` in flags[c] (a release store after its writes), and thread t of
+// every CTA waits for flags[t], flags[t + blockDim.x], ... to reach `target`
+// (acquire loads), so that no counter is contended.  `target` grows with every
+// barrier of every launch (the launch number in the high bits), so flags left
+// by earlier launches never satisfy it.  The waits are bounded like those of
+// group_barrier; `each(t)` runs in the waiting thread once peer t has arrived
+// (the caller reads that peer's published data there).
+template <class F>
+__device__ __forceinline__ bool flag_barrier(unsigned long long* flags, GroupSync* gs, int c, int n,
+                                             unsigned long long target, const F& each) {
+  __shared__ int bad_sh;
+  if (threadIdx.x == 0) bad_sh = 0;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    st_release_u64(flags + c, target);
+  }
+  for (int t = threadIdx.x; t < n; t += blockDim.x) {
+    if (t != c) {
+      const long long t0 = clock64();
+      while (ld_acquire_u64(flags + t) < target) {
+        if (ld_relaxed_i32(&gs->err) != 0 || clock64() - t0 > kSpinCycles) {
+          atomicExch(&gs->err, 1);
+          bad_sh = 1;
+          break;
+        }
+        __nanosleep(20);
+      }
+    }
+    each(t);
+  }
+  __syncthreads();
+  return bad_sh == 0;
 }
 
 __device__ __forceinline__ bool group_barrier(GroupSync* gs, int n) {
@@ -238,7 +284,8 @@ struct WideMol {
   double *xbuf, *d, *e, *tau, *esq, *eps, *occ, *pop, *vao, *part, *Tf, *Xp, *popp, *eshift;
   double* ws;   // CtaWs layout with maxn = 1: SCC vectors and Broyden history
   WideState* st;
-  GroupSync* sync;  // [2]: column barriers, panel barriers
+  GroupSync* sync;  // [2]: column barriers, panel barriers (error flags)
+  unsigned long long* flags;  // [2 * kFlagSlots]: per-CTA barrier flags (column, panel)
 };
 
 // Per-launch parameters shared by the kernels of the wide path.
@@ -494,7 +541,7 @@ __host__ __device__ inline int tridiag_min_group(int N, int nb) {
 }
 
 __global__ void __launch_bounds__(kRedNT) wide_tridiag_kernel(WideCtx X, int G, int nb, int min_rows,
-                                                               long long* prof) {
+                                                               long long* prof, unsigned long long epoch) {
   extern __shared__ __align__(16) double sm[];
   __shared__ TridiagSmall ss;
   constexpr int NW = kRedNT / 32;
@@ -513,6 +560,9 @@ __global__ void __launch_bounds__(kRedNT) wide_tridiag_kernel(WideCtx X, int G, 
   const int pcap = X.maxn + 8 + (int)(kTileSmemBytes / sizeof(double));  // staging room for partial sums (vs + tsm)
   GroupSync* cs = w.sync;
   GroupSync* ps = w.sync + 1;
+  unsigned long long* cflags = w.flags;
+  unsigned long long* pflags = w.flags + kFlagSlots;
+  unsigned long long cgen = epoch << 24, pgen = epoch << 24;  // barrier targets of this launch
   // optional phase clocks of thread 0 of the first molecule's CTA 0
   const bool timing = prof && blockIdx.x == 0 && tid == 0;
   long long tclk = timing ? clock64() : 0, tph[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -587,12 +637,29 @@ __global__ void __launch_bounds__(kRedNT) wide_tridiag_kernel(WideCtx X, int G, 
           if (lane == 0) part[(long long)c * PS + q] = sacc;
         }
         mark(0);
-        if (!(ok = group_barrier(cs, Ga))) break;
-        mark(1);
-        // ---- (B) totals: the Ga x (2l+1) partials read coalesced into shared
-        // memory (vs and the tile area are free here), in chunks of CTAs
+        // ---- (B) totals of the partials: each waiting thread copies its peer's
+        // row into shared memory (vs and the tile area are free here) as soon
+        // as that peer has arrived
         const int nq = 2 * l + 1;
+        const bool fused = Ga * nq <= pcap;
         {
+          double* pbuf = vs;
+          ok = flag_barrier(cflags, cs, c, Ga, ++cgen, [&](int t) {
+            if (!fused) return;
+            const double* src = part + (long long)t * PS;
+#pragma unroll 8
+            for (int q = 0; q < nq; ++q) pbuf[t * nq + q] = ldcg(src + q);
+          });
+          if (!ok) break;
+          if (fused && tid < nq) {
+            double sacc = 0.0;
+            for (int cc = 0; cc < Ga; ++cc) sacc += pbuf[cc * nq + tid];
+            ss.tot[tid] = sacc;
+          }
+          __syncthreads();
+        }
+        mark(1);
+        if (!fused) {
           double* pbuf = vs;
           const int per = max(1, pcap / nq);  // CTAs' partials per chunk
           double sacc = 0.0;
@@ -742,16 +809,19 @@ __global__ void __launch_bounds__(kRedNT) wide_tridiag_kernel(WideCtx X, int G, 
           part[(long long)c * PS + PS - 1] = sacc;
         }
         mark(4);
-        if (!(ok = group_barrier(cs, Ga))) break;
-        mark(5);
-        // ---- (C) alpha = -tau (p.v) / 2 from the Ga partial sums (one warp)
-        if (wid == 0) {
-          double sacc = 0.0;
-          for (int cc = lane; cc < Ga; cc += 32) sacc += ldcg(part + (long long)cc * PS + PS - 1);
-          sacc = warp_sum(sacc);
-          if (lane == 0) ss.alpha2[l] = -0.5 * tau * sacc;
+        {  // ---- (C) alpha = -tau (p.v) / 2 from the Ga partial sums
+          double* pbuf = tsm;  // the tile area is free here
+          ok = flag_barrier(cflags, cs, c, Ga, ++cgen, [&](int t) { pbuf[t] = ldcg(part + (long long)t * PS + PS - 1); });
+          if (!ok) break;
+          mark(5);
+          if (wid == 0) {
+            double sacc = 0.0;
+            for (int cc = lane; cc < Ga; cc += 32) sacc += pbuf[cc];
+            sacc = warp_sum(sacc);
+            if (lane == 0) ss.alpha2[l] = -0.5 * tau * sacc;
+          }
+          __syncthreads();
         }
-        __syncthreads();
         mark(6);
       }
       if (ok) {  // finish W for the CTA's rows: w = p + alpha v
@@ -762,7 +832,7 @@ __global__ void __launch_bounds__(kRedNT) wide_tridiag_kernel(WideCtx X, int G, 
       }
     }
     mark(6);
-    if (!ok || !(ok = group_barrier(ps, G))) break;
+    if (!ok || !(ok = flag_barrier(pflags, ps, c, G, ++pgen, [](int) {}))) break;
     mark(7);
     // ---- trailing update A22 -= V W^T + W V^T (rows and columns >= k1)
     const int k1 = k0 + nbc;
@@ -787,7 +857,7 @@ __global__ void __launch_bounds__(kRedNT) wide_tridiag_kernel(WideCtx X, int G, 
       });
     }
     mark(8);
-    if (!(ok = group_barrier(ps, G))) break;
+    if (!(ok = flag_barrier(pflags, ps, c, G, ++pgen, [](int) {}))) break;
     mark(7);
   }
   if (timing)
@@ -894,14 +964,88 @@ __global__ void __launch_bounds__(kWideNT, 1) wide_rung_kernel(Batch B, Model M,
 }
 
 // ------------------------------------------------------------------ per iteration
-// (1) shell potential of the input charges (src/coulomb.rs:140-193)
+// out[i] = sum_j G[i][j] q[j] over the molecule's nsh x nsh Coulomb matrix, one
+// warp per row with the lanes along the row (coalesced), the whole CTA.
+__device__ __forceinline__ void coulomb_matvec(const double* G, const double* q, int nsh, double* out) {
+  constexpr int NW = kWideNT / 32;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int i = wid; i < nsh; i += NW) {
+    const double* gi = G + (long long)i * nsh;
+    double s0 = 0.0, s1 = 0.0;
+    int j = lane;
+    for (; j + 32 < nsh; j += 64) {
+      s0 += gi[j] * q[j];
+      s1 += gi[j + 32] * q[j + 32];
+    }
+    if (j < nsh) s0 += gi[j] * q[j];
+    const double s = warp_sum(s0 + s1);
+    if (lane == 0) out[i] = s;
+  }
+  __syncthreads();
+}
+
+// (1) shell potential of the input charges (src/coulomb.rs:140-193), as
+// stage_potential with the coalesced Coulomb product.
 __global__ void __launch_bounds__(kWideNT, 1) wide_potential_kernel(Batch B, Model M, WideCtx X) {
   extern __shared__ __align__(16) unsigned char raw[];
   const WideMol& w = X.mols[X.act[blockIdx.x]];
   if (w.st->status != kOk) return;
   const MolCtx c = wide_context(B, M, w.m, X.maxnsh, X.maxn, raw);
   CtaWs ws = cta_ws(w.ws, 1, X.maxnsh, X.cap);
-  stage_potential<kWideNT>(B, M, c, ws, w.vao);
+  const int tid = threadIdx.x;
+  for (int a = tid; a < c.nat; a += kWideNT) {
+    double q = 0.0;
+    for (int s = c.atom_sh[a]; s < c.atom_sh[a + 1]; ++s) q += ws.qin[s];
+    ws.qat[a] = q;
+  }
+  coulomb_matvec(c.G, ws.qin, c.nsh, ws.vsh);
+  for (int i = tid; i < c.nsh; i += kWideNT) {
+    const double qa = ws.qat[c.sh_atom[i]];
+    ws.vsh[i] += qa * qa * M.elem[B.z[c.a0 + c.sh_atom[i]]].gam3;
+  }
+  __syncthreads();
+  for (int i = tid; i < c.N; i += kWideNT) w.vao[i] = ws.vsh[c.ao_sh[i]];
+}
+
+// (9) output charges, energies and rms (src/electronic.rs:2173-2191,
+// :3160-3200), as stage_charges_energy with the coalesced Coulomb product.
+__device__ void wide_charges_energy(const Batch& B, const Model& M, const MolCtx& c, CtaWs& w, const double* pop,
+                                    const double* occ, const double* eps, const double* vao, int nocc, SccShared& sh,
+                                    double& e_el, double& e2, double& e3, double& rms) {
+  const int tid = threadIdx.x;
+  for (int s = tid; s < c.nsh; s += kWideNT) {
+    const ElemTable& el = M.elem[B.z[c.a0 + c.sh_atom[s]]];
+    const int k = c.sh_k[s];
+    double p = 0.0;
+    for (int q = 0; q < 2 * el.l[k] + 1; ++q) p += pop[c.sh_ao0[s] + q];
+    w.qout[s] = el.refocc[k] - p;
+  }
+  double part = 0.0;
+  for (int i = tid; i < c.N; i += kWideNT) part += (i < nocc ? occ[i] * eps[i] : 0.0) + vao[i] * pop[i];
+  e_el = block_sum(part, sh.red);
+  for (int a = tid; a < c.nat; a += kWideNT) {
+    double q = 0.0;
+    for (int s = c.atom_sh[a]; s < c.atom_sh[a + 1]; ++s) q += w.qout[s];
+    w.qat[a] = q;
+  }
+  coulomb_matvec(c.G, w.qout, c.nsh, w.vout);  // G q_out (the third-order part is added below)
+  double p2 = 0.0, p3 = 0.0, pr = 0.0;
+  for (int i = tid; i < c.nsh; i += kWideNT) {
+    const double v = w.vout[i];
+    p2 += w.qout[i] * v;
+    const int a = c.sh_atom[i];
+    const double qa = w.qat[a];
+    w.vout[i] = v + qa * qa * M.elem[B.z[c.a0 + a]].gam3;
+    const double r = w.qout[i] - w.qin[i];
+    pr += r * r;
+  }
+  for (int a = tid; a < c.nat; a += kWideNT) {
+    const double qa = w.qat[a];
+    p3 += qa * qa * qa * M.elem[B.z[c.a0 + a]].gam3 / 3.0;
+  }
+  e2 = 0.5 * block_sum(p2, sh.red);
+  e3 = block_sum(p3, sh.red);
+  rms = c.nsh ? sqrt(block_sum(pr, sh.red) / c.nsh) : 0.0;
 }
 
 // (2) F' = H0' - 1/2 (M + M^T), M = L^-1 diag(v) L lower triangular
@@ -963,25 +1107,27 @@ __global__ void __launch_bounds__(kGemmNT) wide_shift_kernel(WideCtx X, double l
 
 // (4) eigenvalues 0..nneed-1 and N-1 (one thread each), d and e^2 staged in
 // shared memory.
-__global__ void __launch_bounds__(128) wide_eigval_kernel(WideCtx X) {
+constexpr int kEigNT = 32;  // one warp per CTA: the searches spread over the SMs
+__global__ void __launch_bounds__(kEigNT) wide_eigval_kernel(WideCtx X) {
   extern __shared__ __align__(16) double dsm[];
   const WideMol& w = X.mols[X.act[blockIdx.y]];
   const WideState* st = w.st;
   if (st->status != kOk) return;
   const int N = w.N, nneed = st->nneed;
   const int nlist = nneed < N ? nneed + 1 : N;
-  if (blockIdx.x * 128 >= nlist) return;
+  if (blockIdx.x * kEigNT >= nlist) return;
   double* d = dsm;
   double* esq = dsm + N;
-  for (int i = threadIdx.x; i < N; i += 128) {
+  for (int i = threadIdx.x; i < N; i += kEigNT) {
     d[i] = w.d[i];
     esq[i] = i < N - 1 ? w.esq[i] : 0.0;
   }
   __syncthreads();
-  const int slot = blockIdx.x * 128 + threadIdx.x;
-  if (slot < nlist) {
+  const int slot = blockIdx.x * kEigNT + threadIdx.x;
+  if (slot < nlist) {  // from the previous iteration's eigenvalue once the rung has one
     const int k = slot < nneed ? slot : N - 1;
-    w.eps[k] = eigenvalue_k(d, esq, N, k, st->gl, st->gu, st->pivmin, 4.0 * DBL_EPSILON * st->onenrm);
+    w.eps[k] = eigenvalue_k(d, esq, N, k, st->gl, st->gu, st->pivmin, 4.0 * DBL_EPSILON * st->onenrm, w.eps[k],
+                            st->iter > 0);
   }
 }
 
@@ -1316,7 +1462,7 @@ __global__ void __launch_bounds__(kWideNT, 1) wide_energy_mix_kernel(Batch B, Mo
   }
   __syncthreads();
   double e_el, e2, e3, rms;
-  stage_charges_energy<kWideNT>(B, M, c, ws, w.pop, w.occ, w.eps, w.vao, nocc, sh, e_el, e2, e3, rms);
+  wide_charges_energy(B, M, c, ws, w.pop, w.occ, w.eps, w.vao, nocc, sh, e_el, e2, e3, rms);
   if (lshift != 0.0) {
     const int ntile = ((N + 63) / 64) * nit;
     double part = 0.0;
@@ -1408,6 +1554,7 @@ __global__ void __launch_bounds__(kWideNT, 1) wide_results_kernel(Batch B, Model
 }  // namespace gfn1
 
 // ================================================================== host side
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <map>
@@ -1483,6 +1630,7 @@ struct WideRuntime {
   WideState* d_state = nullptr;
   WideState* h_state = nullptr;
   GroupSync* d_sync = nullptr;
+  unsigned long long* d_flags = nullptr;  // [2 * kFlagSlots] per slot, zero at bind
   int* d_stats = nullptr;  // timing mode: cluster statistics and reduction phase clocks
   int capacity = 0;  // slots the buffers above hold
   WidePlan plan;     // plan of the last run
@@ -1514,10 +1662,13 @@ static cudaError_t wide_configure(int dev) {
   return cudaSuccess;
 }
 
+static std::atomic<unsigned long long> g_tridiag_epoch{0};  // launches of the reduction (barrier flag generations)
+
 static cudaError_t launch_tridiag(const WideCtx& X, int na, int G, int nb, int min_rows, size_t smem, cudaStream_t st,
                                   long long* prof) {
   WideCtx x = X;
-  void* args[] = {(void*)&x, (void*)&G, (void*)&nb, (void*)&min_rows, (void*)&prof};
+  unsigned long long epoch = g_tridiag_epoch.fetch_add(1) + 1;
+  void* args[] = {(void*)&x, (void*)&G, (void*)&nb, (void*)&min_rows, (void*)&prof, (void*)&epoch};
   return cudaLaunchCooperativeKernel((const void*)wide_tridiag_kernel, dim3(na * G), dim3(kRedNT), args, smem, st);
 }
 
@@ -1744,7 +1895,7 @@ cudaError_t run_wide(const Batch& B, const Model& M, const SccOptions& opt, Wide
                            tm.on ? (long long*)(R.d_stats + 32) : nullptr)) != cudaSuccess)
         return e;
       tm.mark("tridiag");
-      wide_eigval_kernel<<<dim3((maxn + 1 + 127) / 128, na), 128, sizeof(double) * 2 * maxn, st>>>(X);
+      wide_eigval_kernel<<<dim3((maxn + kEigNT) / kEigNT, na), kEigNT, sizeof(double) * 2 * maxn, st>>>(X);
       tm.mark("eigval");
       wide_fermi_kernel<<<na, kWideNT, 0, st>>>(X);
       tm.mark("fermi");
@@ -1811,8 +1962,10 @@ cudaError_t wide_bind(WideRuntime& R, const std::vector<int>& ids, const std::ve
     if (R.d_act) cudaFree(R.d_act);
     if (R.d_state) cudaFree(R.d_state);
     if (R.d_sync) cudaFree(R.d_sync);
+    if (R.d_flags) cudaFree(R.d_flags);
     if (R.h_act) cudaFreeHost(R.h_act);
     if (R.h_state) cudaFreeHost(R.h_state);
+    R.d_flags = nullptr;
     R.d_mols = nullptr;
     R.d_act = nullptr;
     R.d_state = nullptr;
@@ -1824,6 +1977,7 @@ cudaError_t wide_bind(WideRuntime& R, const std::vector<int>& ids, const std::ve
         (e = cudaMalloc(&R.d_act, sizeof(int) * n)) != cudaSuccess ||
         (e = cudaMalloc(&R.d_state, sizeof(WideState) * n)) != cudaSuccess ||
         (e = cudaMalloc(&R.d_sync, sizeof(GroupSync) * 2 * n)) != cudaSuccess ||
+        (e = cudaMalloc(&R.d_flags, sizeof(unsigned long long) * 2 * kFlagSlots * n)) != cudaSuccess ||
         (e = cudaHostAlloc((void**)&R.h_act, sizeof(int) * n, cudaHostAllocDefault)) != cudaSuccess ||
         (e = cudaHostAlloc((void**)&R.h_state, sizeof(WideState) * n, cudaHostAllocDefault)) != cudaSuccess)
       return e;
@@ -1864,14 +2018,17 @@ cudaError_t wide_bind(WideRuntime& R, const std::vector<int>& ids, const std::ve
     w.ws = p + s.ws;
     w.st = R.d_state + q;
     w.sync = R.d_sync + 2 * q;
+    w.flags = R.d_flags + (size_t)2 * kFlagSlots * q;
   }
   if ((e = cudaMemcpy(R.d_mols, R.mols.data(), sizeof(WideMol) * n, cudaMemcpyHostToDevice)) != cudaSuccess) return e;
   if ((e = cudaMemset(R.d_sync, 0, sizeof(GroupSync) * 2 * n)) != cudaSuccess) return e;
+  if ((e = cudaMemset(R.d_flags, 0, sizeof(unsigned long long) * 2 * kFlagSlots * n)) != cudaSuccess) return e;
   return cudaMemset(R.d_state, 0, sizeof(WideState) * n);
 }
 
 void wide_release(WideRuntime& R) {
   if (R.d_stats) cudaFree(R.d_stats);
+  if (R.d_flags) cudaFree(R.d_flags);
   if (R.d_mols) cudaFree(R.d_mols);
   if (R.d_act) cudaFree(R.d_act);
   if (R.d_state) cudaFree(R.d_state);
