@@ -21,6 +21,7 @@
 #include "../../include/gfn1_b200.h"
 #include "common.cuh"
 #include "guess.cuh"
+#include "optimize.cuh"
 #include "model.cuh"
 
 namespace gfn1 {
@@ -317,6 +318,11 @@ struct gfn1_batch {
   DevBuf<unsigned char> d_in, d_out; // device blobs
   DevBuf<double> S, H0, P, W, ws, gam, pairbuf, cn, shell_pot, shell_pot_in, se, grad_classic, orb_eps, orb_occ;
   DevBuf<int> queue;
+  // geometry optimisation on the device (gfn1_batch_optimize)
+  const int* opt_skip = nullptr;  // molecules the engine kernels skip this round, or null
+  DevBuf<unsigned char> opt_mol;
+  DevBuf<double> opt_x, opt_g, opt_d, opt_S, opt_Y, opt_q;
+  DevBuf<int> opt_flags;          // skip[nmol] | active count
   DevBuf<unsigned long long> stage;
   template <class T>
   T* din(size_t off) const { return (T*)(d_in.p + off); }
@@ -388,6 +394,9 @@ struct gfn1_batch {
     gy.release();
     gq.release();
     wide_buf.release();
+    opt_mol.release();
+    for (DevBuf<double>* d : {&opt_x, &opt_g, &opt_d, &opt_S, &opt_Y, &opt_q}) d->release();
+    opt_flags.release();
     if (wide) wide_runtime_delete(wide);
     wide = nullptr;
     if (ev_fork) cudaEventDestroy(ev_fork);
@@ -932,6 +941,8 @@ int launch_stage(gfn1_batch* b, int stage, cudaStream_t st) {
         (e = cudaMemsetAsync(b->queue.p, 0, sizeof(int) * 4, st)) != cudaSuccess ||
         (e = cudaMemsetAsync(B.rung, 0, sizeof(int) * b->nmol, st)) != cudaSuccess)
       return cuda_fail(eng, e, "batch reset");
+    if (b->opt_skip && (e = launch_opt_skip(b->nmol, b->opt_skip, B.status, st)) != cudaSuccess)
+      return cuda_fail(eng, e, "optimiser skip list");
     if (b->profiling && (e = cudaMemsetAsync(b->stage.p, 0, sizeof(unsigned long long) * kStages, st)) != cudaSuccess)
       return cuda_fail(eng, e, "batch reset");
     if (b->guess && !b->has_init_q) {  // learned initial shell charges from the device coordinates
@@ -1756,3 +1767,110 @@ extern "C" int gfn1_run_noalloc(gfn1_engine* eng, int nat, const uint8_t* z, con
                                                                  : "molecule failed with status " + std::to_string(status));
   return GFN1_OK;
 }
+
+// ============================================================== geometry optimisation
+extern "C" void gfn1_default_opt_options(gfn1_opt_options* o) {
+  if (!o) return;
+  o->max_iterations = 250;  // GeometryOptimizationOptions defaults (src/optimizer.rs:27-50)
+  o->gradient_tolerance = 1.0e-4;
+  o->step_tolerance = 1.0e-7;
+  o->history = 12;
+  o->initial_step = 1.0;
+  o->max_atom_step = 0.30;
+  o->max_rounds = 100000;
+}
+
+extern "C" int gfn1_batch_optimize(gfn1_batch* b, const gfn1_opt_options* opt, double* xyz_out, double* energy,
+                                   double* max_gradient, int32_t* iterations, int32_t* converged, int32_t* status,
+                                   int32_t* rounds) {
+  if (!b) return fail(nullptr, GFN1_E_INVALID_INPUT, "null batch");
+  gfn1_engine* eng = b->eng;
+  if (!b->opt.compute_gradient) return fail(eng, GFN1_E_INVALID_INPUT, "the batch was created without gradients");
+  gfn1_opt_options o;
+  if (opt) o = *opt;
+  else gfn1_default_opt_options(&o);
+  if (o.history < 1 || o.history > 12 || o.max_iterations < 0 || o.max_rounds < 1)
+    return fail(eng, GFN1_E_INVALID_INPUT, "optimiser options out of range (history 1..12)");
+  DeviceGuard dg(eng->device);
+  cudaStream_t st = eng->stream;
+  const int nmol = b->nmol;
+  const long long n3 = 3 * b->natoms;
+  const int H = o.history;
+  if (!b->opt_mol.ensure(opt_mol_bytes() * nmol) || !b->opt_x.ensure(n3) || !b->opt_g.ensure(n3) ||
+      !b->opt_d.ensure(n3) || !b->opt_S.ensure((size_t)H * n3) || !b->opt_Y.ensure((size_t)H * n3) ||
+      !b->opt_q.ensure((size_t)std::max<long long>(b->nshells, 1)) || !b->opt_flags.ensure((size_t)nmol + 1))
+    return fail(eng, GFN1_E_DEVICE, "device allocation failed for the optimiser");
+  OptArrays A;
+  A.mol = (OptMol*)b->opt_mol.p;
+  A.x = b->opt_x.p;
+  A.g = b->opt_g.p;
+  A.d = b->opt_d.p;
+  A.S = b->opt_S.p;
+  A.Y = b->opt_Y.p;
+  A.q = b->opt_q.p;
+  A.x_in = b->din<double>(b->lay.xyz);
+  A.q_in = b->din<double>(b->lay.init_q);
+  A.skip = b->opt_flags.p;
+  A.active = b->opt_flags.p + nmol;
+  A.n3 = n3;
+  OptParams P;
+  P.max_iterations = o.max_iterations;
+  P.history = H;
+  P.gradient_tolerance = o.gradient_tolerance;
+  P.step_tolerance = o.step_tolerance;
+  P.initial_step = o.initial_step;
+  P.max_atom_step = o.max_atom_step;
+  const bool had_init_q = b->has_init_q;
+  b->opt_skip = nullptr;
+  int rc = GFN1_OK;
+  int nround = 0;
+  cudaError_t e = cudaSuccess;
+  auto run_engine = [&]() {
+    for (int s = 0; s < 3 && rc == GFN1_OK; ++s) rc = launch_stage(b, s, st);
+  };
+  // the starting geometries
+  run_engine();
+  if (rc == GFN1_OK && (e = cudaMemsetAsync(A.active, 0, sizeof(int), st)) != cudaSuccess) rc = cuda_fail(eng, e, "optimiser");
+  if (rc == GFN1_OK && (e = launch_opt_round(b->dev(), A, P, nmol, 1, st)) != cudaSuccess) rc = cuda_fail(eng, e, "optimiser");
+  // rounds: every pending trial geometry of every molecule in one engine pass
+  while (rc == GFN1_OK) {
+    int act = 0;
+    if ((e = cudaMemcpyAsync(&act, A.active, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+      rc = cuda_fail(eng, e, "optimiser round");
+      break;
+    }
+    if (act == 0 || nround >= o.max_rounds) break;
+    ++nround;
+    b->has_init_q = true;  // trials start from the current geometries' converged charges
+    b->opt_skip = A.skip;
+    run_engine();
+    if (rc != GFN1_OK) break;
+    if ((e = cudaMemsetAsync(A.active, 0, sizeof(int), st)) != cudaSuccess ||
+        (e = launch_opt_round(b->dev(), A, P, nmol, 0, st)) != cudaSuccess)
+      rc = cuda_fail(eng, e, "optimiser round");
+  }
+  b->opt_skip = nullptr;
+  b->has_init_q = had_init_q;
+  if (rc != GFN1_OK) return rc;
+  if ((e = launch_opt_final(b->dev(), A, nmol, st)) != cudaSuccess) return cuda_fail(eng, e, "optimiser results");
+  std::vector<unsigned char> hm(opt_mol_bytes() * nmol);
+  if ((e = cudaMemcpyAsync(hm.data(), A.mol, hm.size(), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+      (xyz_out && (e = cudaMemcpyAsync(xyz_out, A.x, sizeof(double) * n3, cudaMemcpyDeviceToHost, st)) != cudaSuccess) ||
+      (e = cudaStreamSynchronize(st)) != cudaSuccess)
+    return cuda_fail(eng, e, "optimiser results");
+  int worst = GFN1_OK;
+  for (int m = 0; m < nmol; ++m) {
+    const OptMol& mm = *(const OptMol*)(hm.data() + opt_mol_bytes() * m);
+    if (energy) energy[m] = mm.error == kOk ? mm.energy : NAN;
+    if (max_gradient) max_gradient[m] = mm.error == kOk ? mm.maxg : NAN;
+    if (iterations) iterations[m] = mm.iterations;
+    if (converged) converged[m] = mm.converged;
+    if (status) status[m] = mm.error;
+    worst = std::max(worst, mm.error);
+  }
+  if (rounds) *rounds = nround;
+  if (worst != GFN1_OK) return fail(eng, worst, "geometry optimisation failed for at least one molecule (see status)");
+  return GFN1_OK;
+}
+

@@ -23,6 +23,7 @@ enum Status : int {
   kErrTimeout = 10,
   kErrNan = 11,
   kErrUnsupported = 12,
+  kOptSkipped = 13,  // internal: a molecule the geometry optimiser has finished (the engine kernels skip it)
 };
 
 constexpr int kMaxZ = 86;

@@ -8,7 +8,7 @@ PKG_ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__fil
 CSRC = os.path.join(PKG_ROOT, "csrc")
 LIB_DIR = os.path.join(PKG_ROOT, "lib")
 LIB_PATH = os.path.join(LIB_DIR, "libgfn1_b200.so")
-SOURCES = ("setup.cu", "scc.cu", "grad.cu", "guess.cu", "capi.cu")
+SOURCES = ("setup.cu", "scc.cu", "grad.cu", "guess.cu", "optimize.cu", "capi.cu")
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
     "-Xcompiler", "-fPIC", "-shared",

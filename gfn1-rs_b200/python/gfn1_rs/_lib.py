@@ -44,6 +44,18 @@ class Options(ctypes.Structure):
     ]
 
 
+class OptOptions(ctypes.Structure):
+    _fields_ = [
+        ("max_iterations", ctypes.c_int32),
+        ("gradient_tolerance", ctypes.c_double),
+        ("step_tolerance", ctypes.c_double),
+        ("history", ctypes.c_int32),
+        ("initial_step", ctypes.c_double),
+        ("max_atom_step", ctypes.c_double),
+        ("max_rounds", ctypes.c_int32),
+    ]
+
+
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int32)
 
@@ -107,6 +119,9 @@ def load():
         L.gfn1_last_molecule_matrices.argtypes = [vp, ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp]
         L.gfn1_batch_molecule_matrices.argtypes = [vp, ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp]
         L.gfn1_last_molecule_fock.argtypes = [vp, ctypes.c_int, _dp, _dp, _dp]
+        L.gfn1_default_opt_options.argtypes = [ctypes.POINTER(OptOptions)]
+        L.gfn1_default_opt_options.restype = None
+        L.gfn1_batch_optimize.argtypes = [vp, ctypes.POINTER(OptOptions), _dp, _dp, _dp, _ip, _ip, _ip, _ip]
         L.gfn1_batch_molecule_fock.argtypes = [vp, ctypes.c_int, _dp, _dp, _dp]
         L.gfn1_run_noalloc.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_uint8), _dp, ctypes.c_double, _dp,
                                        ctypes.POINTER(Options), ctypes.POINTER(Outputs), vp]
@@ -136,7 +151,7 @@ def load():
                      "gfn1_mlp_reduce", "gfn1_mlp_colsum", "gfn1_mlp_project_loss", "gfn1_mlp_adam"):
             getattr(L, name).restype = ctypes.c_int
         for name in ("gfn1_last_molecule_matrices", "gfn1_batch_molecule_matrices", "gfn1_run_noalloc",
-                     "gfn1_last_molecule_fock", "gfn1_batch_molecule_fock",
+                     "gfn1_last_molecule_fock", "gfn1_batch_molecule_fock", "gfn1_batch_optimize",
                      "gfn1_batch_launch_stage", "gfn1_batch_stage_cycles", "gfn1_batch_io_bytes",
                      "gfn1_engine_create", "gfn1_basis_size", "gfn1_run", "gfn1_batch_energy_gradient",
                      "gfn1_batch_create", "gfn1_batch_set_positions", "gfn1_batch_set_initial_charges",

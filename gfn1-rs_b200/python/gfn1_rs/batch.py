@@ -192,6 +192,33 @@ class ResidentBatch:
                          lambda *p: L.gfn1_batch_molecule_matrices(self.handle, int(m), *p),
                          lambda *p: L.gfn1_batch_molecule_fock(self.handle, int(m), *p))
 
+    def optimize(self, max_iterations=250, gradient_tolerance=1.0e-4, step_tolerance=1.0e-7, history=12,
+                 initial_step=1.0, max_atom_step=0.30, max_rounds=100000) -> dict:
+        """Geometry optimisation of every molecule on the device
+        (gfn1_batch_optimize; the reference's optimize_geometry) from the
+        positions set with set_positions.  Returns final coordinates (bohr),
+        energies, largest gradient components, accepted steps, converged flags,
+        statuses and the number of engine passes."""
+        L = _lib.load()
+        o = _lib.OptOptions()
+        L.gfn1_default_opt_options(ctypes.byref(o))
+        o.max_iterations, o.gradient_tolerance, o.step_tolerance = int(max_iterations), gradient_tolerance, step_tolerance
+        o.history, o.initial_step, o.max_atom_step, o.max_rounds = int(history), initial_step, max_atom_step, int(max_rounds)
+        xyz = np.zeros((self.natoms, 3))
+        energy = np.zeros(self.nmol)
+        maxg = np.zeros(self.nmol)
+        iters = np.zeros(self.nmol, dtype=np.int32)
+        conv = np.zeros(self.nmol, dtype=np.int32)
+        status = np.zeros(self.nmol, dtype=np.int32)
+        rounds = ctypes.c_int32()
+        rc = L.gfn1_batch_optimize(self.handle, ctypes.byref(o), _lib.ptr(xyz), _lib.ptr(energy), _lib.ptr(maxg),
+                                   _lib.ptr(iters, ctypes.c_int32), _lib.ptr(conv, ctypes.c_int32),
+                                   _lib.ptr(status, ctypes.c_int32), ctypes.byref(rounds))
+        if rc not in (0, 3, 8):
+            _lib.check(rc, self.calc.engine.handle)
+        return {"xyz": xyz, "energy": energy, "max_gradient": maxg, "iterations": iters,
+                "converged": conv.astype(bool), "status": status, "engine_calls": rounds.value + 1}
+
     def close(self):
         if getattr(self, "handle", None):
             _lib.load().gfn1_batch_destroy(self.handle)

@@ -337,6 +337,72 @@ class GuessTrainer:
         return out
 
 
+def allreduce_weighted(grad, weight: float, total: float, group=None):
+    """Data-parallel gradient: grad <- sum over ranks of (weight_r / total) grad_r,
+    in place (one all_reduce).  With weight_r the shells of rank r's batch and
+    total their sum over ranks, the result is the gradient of the mean loss over
+    the union of the ranks' batches, as a single rank computes it."""
+    import torch.distributed as dist
+
+    grad.mul_(float(weight) / float(total))
+    dist.all_reduce(grad, op=dist.ReduceOp.SUM, group=group)
+    return grad
+
+
+def shard_training_set(nmol: int, rank: int, world: int, seed: int = 0):
+    """Molecule indices of rank `rank`: a common shuffle split into `world`
+    contiguous parts of equal size (the remainder is dropped so that every rank
+    takes the same number of steps)."""
+    perm = np.random.default_rng(seed).permutation(nmol)
+    per = nmol // world
+    return np.sort(perm[rank * per:(rank + 1) * per])
+
+
+class DataParallelGuessTrainer(GuessTrainer):
+    """GuessTrainer over several ranks (one process per GPU, torch.distributed):
+    every rank holds its shard of the training set, computes the gradients of
+    its batches with the library's kernels, and the ranks average them with one
+    all-reduce per step (weighted by shells, allreduce_weighted) before the
+    identical Adam step, so all ranks keep the same parameters."""
+
+    def __init__(self, params=None, device: int = 0, seed: int = 0, group=None):
+        import torch.distributed as dist
+
+        super().__init__(params, device, seed)
+        self.group = group
+        self.world = dist.get_world_size(group)
+        dist.broadcast(self.P, src=0, group=group)  # one starting point
+
+    def train(self, epochs: int = 30, batch_mols: int = 128, lr: float = 2e-3, lr_final: float = 5e-5,
+              seed: int = 0, log=None) -> list[float]:
+        import torch.distributed as dist
+
+        rng = np.random.default_rng(seed)  # the same step order on every rank
+        starts = np.arange(0, self.nmol, batch_mols)
+        total = epochs * len(starts)
+        step = 0
+        hist = []
+        for ep in range(epochs):
+            for s in rng.permutation(starts):
+                frac = step / max(total - 1, 1)
+                cur = lr_final + 0.5 * (lr - lr_final) * (1.0 + np.cos(np.pi * frac))
+                m0, m1 = int(s), int(min(self.nmol, s + batch_mols))
+                self.forward_backward(m0, m1)
+                rows = float(self.off_h[m1] - self.off_h[m0])
+                tot = self.torch.tensor([rows], dtype=self.torch.float64, device=self.dev)
+                dist.all_reduce(tot, group=self.group)
+                allreduce_weighted(self.G, rows, float(tot.item()), self.group)
+                self.adam_step(cur)
+                step += 1
+            l = self.loss()
+            lt = self.torch.tensor([l], dtype=self.torch.float64, device=self.dev)
+            dist.all_reduce(lt, group=self.group)
+            hist.append(float(lt.item()) / self.world)
+            if log:
+                log(f"epoch {ep + 1}/{epochs}: mse {hist[-1]:.3e} (mean over ranks)")
+        return hist
+
+
 def label_molecules(calc, atom_offsets, numbers, xyz_bohr, chunk: int = 4096, log=None):
     """Converged shell charges [natoms, 2] and a per-molecule OK mask, from the engine."""
     off = np.asarray(atom_offsets, dtype=np.int32)
@@ -368,21 +434,34 @@ def select_molecules(atom_offsets, numbers, xyz, mask):
 
 def train_guess(n_train: int = 50000, seed0: int = 10**6, epochs: int = 30, batch_mols: int = 128,
                 lr: float = 2e-3, out: str | None = DEFAULT_PATH, device: int = 0, log=print) -> np.ndarray:
-    """Label n_train seed-generated molecules with the engine and train the network."""
+    """Label n_train seed-generated molecules with the engine and train the
+    network.  Under torch.distributed (one process per GPU) each rank labels
+    and trains on its shard of the training set (DataParallelGuessTrainer);
+    rank 0 writes the parameters."""
+    import torch.distributed as dist
+
     from . import workloads
     from .batch import BatchCalculator
     from .native import ANGSTROM_TO_BOHR
+    dp = dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1
+    rank, world = (dist.get_rank(), dist.get_world_size()) if dp else (0, 1)
     calc = BatchCalculator(device=device)
     off, z, x = workloads.mixed_batch(n_train, seed0)
+    if dp:  # this rank's shard
+        from .shard import take
+        off, z, x, _, _ = take(off, z, x, shard_training_set(n_train, rank, world, seed=seed0))
     xb = x * ANGSTROM_TO_BOHR
     labels, ok, _ = label_molecules(calc, off, z, xb, log=log)
     off2, z2, x2, atoms = select_molecules(off, z, xb, ok)
-    tr = GuessTrainer(device=device)
+    tr = DataParallelGuessTrainer(device=device) if dp else GuessTrainer(device=device)
     tr.set_data(off2, z2, x2, None, labels[atoms])
+    if dp:  # the normalisation of the descriptors: rank 0's, so that every rank feeds the same network
+        dist.broadcast(tr.P, src=0)
+        tr._refeaturize()
     log(f"training on {len(off2) - 1} molecules, {int(off2[-1])} atoms; initial mse {tr.loss():.3e}")
     tr.train(epochs=epochs, batch_mols=batch_mols, lr=lr, log=log)
     p = tr.params()
-    if out:
+    if out and rank == 0:
         save_params(out, p)
         log(f"wrote {out}")
     return p
@@ -397,4 +476,19 @@ if __name__ == "__main__":
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--out", default=DEFAULT_PATH)
     a = ap.parse_args()
-    train_guess(a.n_train, epochs=a.epochs, batch_mols=a.batch_mols, lr=a.lr, out=a.out)
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:  # torchrun: one process per GPU, NCCL
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+        try:
+            train_guess(a.n_train, epochs=a.epochs, batch_mols=a.batch_mols, lr=a.lr, out=a.out, device=local)
+        finally:
+            dist.destroy_process_group()
+    else:
+        train_guess(a.n_train, epochs=a.epochs, batch_mols=a.batch_mols, lr=a.lr, out=a.out)

@@ -181,3 +181,23 @@ def optimize_batch(calc, atom_offsets, numbers, xyz_bohr, charges=None, options:
             "errors": [m.error for m in mols], "engine_calls": calls[0],
             "trajectories": [m.trajectory for m in mols], "frames": [m.frames for m in mols],
             "gradient": [m.grad for m in mols], "shell_offsets": shoff}
+
+
+def optimize_batch_device(calc, atom_offsets, numbers, xyz_bohr, charges=None,
+                          options: OptimizeOptions | None = None) -> dict:
+    """The same optimisation with the L-BFGS state on the device
+    (gfn1_batch_optimize): the batch's topology and the optimiser's history,
+    geometries, gradients and charges stay in device memory, one engine pass
+    and one kernel per round, and the host reads only the number of molecules
+    still optimising.  Every trial's SCC starts from the converged charges of
+    the molecule's current geometry, as optimize_batch(warm_start=True)."""
+    opt = options or OptimizeOptions()
+    rb = calc.resident(atom_offsets, numbers, charges=charges)
+    try:
+        rb.set_positions(np.asarray(xyz_bohr, dtype=np.float64).reshape(-1, 3))
+        return rb.optimize(max_iterations=opt.max_iterations, gradient_tolerance=opt.gradient_tolerance,
+                           step_tolerance=opt.step_tolerance, history=opt.history, initial_step=opt.initial_step,
+                           max_atom_step=opt.max_atom_step)
+    finally:
+        rb.close()
+

@@ -197,6 +197,36 @@ int gfn1_batch_info(const gfn1_batch* b, int64_t* natoms, int64_t* nshells, int6
 int gfn1_run_noalloc(gfn1_engine* eng, int nat, const uint8_t* z, const double* xyz_bohr, double charge,
                      const double* init_shell_q, const gfn1_options* opt, const gfn1_outputs* out, void* stream);
 
+/* ---- Geometry optimisation on the device: the reference's
+ * optimize_geometry (gfn1-rs src/optimizer.rs:78-320: L-BFGS with history,
+ * Armijo backtracking, per-atom step cap, convergence on the largest gradient
+ * component or the step norm) for every molecule of a resident batch at once.
+ * Options mirror GeometryOptimizationOptions (src/optimizer.rs:17-50). */
+typedef struct gfn1_opt_options {
+  int32_t max_iterations;     /* 250 */
+  double gradient_tolerance;  /* 1e-4 Eh/bohr (largest component) */
+  double step_tolerance;      /* 1e-7 bohr */
+  int32_t history;            /* 12 (at most 12) */
+  double initial_step;        /* 1.0 */
+  double max_atom_step;       /* 0.30 bohr */
+  int32_t max_rounds;         /* bound on engine passes, 100000 */
+} gfn1_opt_options;
+
+void gfn1_default_opt_options(gfn1_opt_options* o);
+/* Optimises every molecule of a resident batch from its current positions
+ * (gfn1_batch_set_positions; the batch must compute gradients).  Each round
+ * evaluates all pending trial geometries in one engine pass on the engine's
+ * stream; the L-BFGS state stays on the device and every trial's SCC starts
+ * from the converged charges of the molecule's current geometry.  Outputs
+ * (host, any may be NULL): final coordinates [natoms*3] (also left in the
+ * batch's positions), energies and largest gradient components [nmol]
+ * (NaN where status is not 0), accepted steps, converged flags and statuses
+ * [nmol] (GFN1_E_INVALID_INPUT where the line search found no downhill step,
+ * as the reference's error), and the number of engine passes.  Synchronous. */
+int gfn1_batch_optimize(gfn1_batch* b, const gfn1_opt_options* opt, double* xyz_out, double* energy,
+                        double* max_gradient, int32_t* iterations, int32_t* converged, int32_t* status,
+                        int32_t* rounds);
+
 /* ---- Learned SCC initial guess.  No counterpart in the reference, whose SCC
  * starts from zero shell charges or a caller-supplied vector (the Rust
  * `init_shell_q` hook, gfn1-rs src/electronic.rs:1231-1239); the guess fills

@@ -50,3 +50,24 @@ def test_batched_optimisation_converges_like_single_runs(gpu_calc):
     # largest gradient of 1e-4 Eh/bohr, which along soft modes leaves the
     # energy uncertain to about 1e-5 Eh
     assert np.abs(warm["energy"][both] - r["energy"][both]).max() <= 1e-5
+
+
+def test_device_optimiser_matches_host_optimiser(gpu_calc):
+    """The L-BFGS on the device (gfn1_batch_optimize: history, line search and
+    geometries in device memory, one engine pass and one kernel per round)
+    follows the host driver with warm starts (the same trial SCC starting
+    charges): the same accepted steps and energies, with the only difference
+    the summation order of the L-BFGS dot products (1e-16 relative)."""
+    from gfn1_rs import BatchCalculator
+    from gfn1_rs.optimize import optimize_batch, optimize_batch_device
+    off, z, x = _batch()
+    calc = BatchCalculator()
+    host = optimize_batch(calc, off, z, x, warm_start=True)
+    dev = optimize_batch_device(calc, off, z, x)
+    print("host iterations", host["iterations"], "device", dev["iterations"], "passes", dev["engine_calls"])
+    assert np.all(dev["status"] == 0)
+    assert np.array_equal(dev["converged"], host["converged"])
+    assert np.array_equal(dev["iterations"], host["iterations"])
+    assert np.abs(dev["energy"] - host["energy"]).max() <= 1e-10
+    assert np.abs(dev["max_gradient"] - host["max_gradient"]).max() <= 1e-8
+    assert np.abs(dev["xyz"] - host["xyz"]).max() <= 1e-6
