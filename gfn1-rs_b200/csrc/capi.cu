@@ -25,8 +25,8 @@
 #include "model.cuh"
 
 namespace gfn1 {
-__global__ void setup_kernel(Batch B, Model M, int enable_dispersion, int max_nsh);
-__global__ void grad_kernel(Batch B, Model M);
+__global__ void setup_kernel(Batch B, Model M, int enable_dispersion, int max_nsh, const int* mols);
+__global__ void grad_kernel(Batch B, Model M, const int* mols, int phases);
 long long scc_workspace_doubles(int maxn, int maxnsh, int cap, int maxnat);
 size_t scc_smem_bytes(int maxnsh, int maxn, int maxnat, int matrix_n);
 size_t scc_max_dynamic_smem(int nt);
@@ -310,6 +310,7 @@ struct gfn1_batch {
   DevBuf<double> gq;                 // guessed initial shell charges [nshells]
   // molecules above the wide threshold: SCC with each molecule on a group of SMs
   std::vector<int> wide_ids;
+  int n_dense = 0;  // leading entries of the processing order above the threshold (their setup and gradient split over CTAs)
   int wide_maxn = 0, wide_maxnsh = 0, wide_maxnat = 0;
   WideRuntime* wide = nullptr;
   DevBuf<double> wide_buf;
@@ -790,6 +791,7 @@ int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t*
   constexpr int kWideMaxN = 8192;  // the reduction keeps two N-vectors per CTA in shared memory
   int n_dense = 0;
   while (n_dense < nmol && n_m[h_order[n_dense]] > kDenseN) ++n_dense;
+  b->n_dense = n_dense;
   b->wide_ids.clear();
   b->wide_maxn = b->wide_maxnsh = b->wide_maxnat = 0;
   for (int q = 0; q < n_dense; ++q) {
@@ -957,7 +959,13 @@ int launch_stage(gfn1_batch* b, int stage, cudaStream_t st) {
     const size_t smem = sizeof(double) * (16 * (size_t)b->max_nat + 32) +
                         sizeof(int) * (3 * (size_t)b->max_nat + 2 + 2 * (size_t)b->max_nsh);
     if (smem > 48 * 1024) cudaFuncSetAttribute(setup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    setup_kernel<<<b->nmol, nt, smem, st>>>(B, M, b->opt.enable_dispersion, b->max_nsh);
+    // one CTA per molecule; large molecules (the leading entries of the
+    // processing order) with their shell pairs split over many CTAs
+    const int nd = b->n_dense, ns = b->nmol - nd;
+    if (ns > 0) setup_kernel<<<dim3(ns, 1), nt, smem, st>>>(B, M, b->opt.enable_dispersion, b->max_nsh, B.order + nd);
+    if (nd > 0)
+      setup_kernel<<<dim3(nd, std::max(1, 4 * eng->num_sms / nd)), nt, smem, st>>>(B, M, b->opt.enable_dispersion,
+                                                                                 b->max_nsh, B.order);
   } else if (stage == 1) {
     SccOptions so;
     so.max_scc = b->opt.max_scc;
@@ -1023,7 +1031,12 @@ int launch_stage(gfn1_batch* b, int stage, cudaStream_t st) {
     if (!b->opt.compute_gradient) return GFN1_OK;
     const size_t smem = sizeof(double) * 7 * (size_t)b->max_nat + sizeof(int) * (3 * (size_t)b->max_nat + 2);
     if (smem > 48 * 1024) cudaFuncSetAttribute(grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    grad_kernel<<<b->nmol, kGradThreads, smem, st>>>(B, M);
+    const int nd = b->n_dense, ns = b->nmol - nd;
+    if (ns > 0) grad_kernel<<<dim3(ns, 1), kGradThreads, smem, st>>>(B, M, B.order + nd, 3);
+    if (nd > 0) {  // large molecules: atom pairs over many CTAs, then the per-atom sums
+      grad_kernel<<<dim3(nd, std::max(1, 4 * eng->num_sms / nd)), kGradThreads, smem, st>>>(B, M, B.order, 1);
+      grad_kernel<<<dim3(nd, 1), kGradThreads, smem, st>>>(B, M, B.order, 2);
+    }
   } else {
     return fail(eng, GFN1_E_INVALID_INPUT, "unknown stage");
   }
@@ -1267,9 +1280,11 @@ int gfn1_batch_info(const gfn1_batch* b, int64_t* natoms, int64_t* nshells, int6
   if (natoms) *natoms = b->natoms;
   if (nshells) *nshells = b->nshells;
   if (naos) *naos = b->naos;
-  if (launches)  // setup, one SCC launch per non-empty size class, the fallback ladder, gradient, learned guess
-    *launches = 1 + (b->cls[0].n_cta > 0) + (b->cls[1].n_cta > 0) + (b->robust.n_cta > 0) +
-                (b->opt.compute_gradient ? 1 : 0) + (b->guess && !b->has_init_q ? 3 : 0);
+  if (launches) {  // setup, one SCC launch per non-empty size class, the fallback ladder, gradient, learned guess
+    const int nd = b->n_dense, ns = b->nmol - nd;  // (the large-molecule SCC launches vary with its iterations)
+    *launches = (ns > 0) + (nd > 0) + (b->cls[0].n_cta > 0) + (b->cls[1].n_cta > 0) + (b->robust.n_cta > 0) +
+                (b->opt.compute_gradient ? (ns > 0) + 2 * (nd > 0) : 0) + (b->guess && !b->has_init_q ? 3 : 0);
+  }
   return GFN1_OK;
 }
 
@@ -1728,7 +1743,7 @@ extern "C" int gfn1_run_noalloc(gfn1_engine* eng, int nat, const uint8_t* z, con
             cudaSuccess)
       return cuda_fail(eng, e, "learned guess");
   }
-  setup_kernel<<<1, 128, sm_setup, st>>>(B, M, o.enable_dispersion, nsh);
+  setup_kernel<<<1, 128, sm_setup, st>>>(B, M, o.enable_dispersion, nsh, nullptr);
   SccLaunch SL;
   SL.q_begin = 0;
   SL.q_end = 1;
@@ -1742,7 +1757,7 @@ extern "C" int gfn1_run_noalloc(gfn1_engine* eng, int nat, const uint8_t* z, con
   SL.smem_bytes = (int)sm_scc;
   if ((e = launch_scc(n > 96 ? 512 : 256, 1, sm_scc, st, B, M, so, SL)) != cudaSuccess)
     return cuda_fail(eng, e, "scc launch");
-  if (o.compute_gradient) grad_kernel<<<1, kGradThreads, sm_grad, st>>>(B, M);
+  if (o.compute_gradient) grad_kernel<<<1, kGradThreads, sm_grad, st>>>(B, M, nullptr, 3);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(eng, e, "kernel launch");
   if ((e = cudaMemcpyAsync(hout, base + o_terms, out_end - o_terms, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
     return cuda_fail(eng, e, "device to host copy");

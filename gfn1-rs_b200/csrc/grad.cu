@@ -50,10 +50,16 @@ __device__ __forceinline__ void grad_shell_pair(const ElemTable& eb, int kb, con
     }
 }
 
-__global__ void __launch_bounds__(kGradThreads, kGradMinBlocks) grad_kernel(Batch B, Model M) {
+// Molecule blockIdx.x of `mols` (or of the batch when null).  phases: bit 0
+// the atom-pair terms (with gridDim.y > 1 every CTA of a molecule takes every
+// gridDim.y-th block of its atom pairs), bit 1 the per-atom sums and the
+// coordination-number chain (one CTA per molecule, after all pairs).
+__global__ void __launch_bounds__(kGradThreads, kGradMinBlocks) grad_kernel(Batch B, Model M, const int* mols,
+                                                                           int phases) {
   extern __shared__ double gsm[];
-  const int m = blockIdx.x;
+  const int m = mols ? mols[blockIdx.x] : blockIdx.x;
   if (B.status[m] != kOk) return;
+  const int split = blockIdx.y, nsplit = gridDim.y;
   const int tid = threadIdx.x, nt = blockDim.x;
   const int a0 = B.atom_off[m], nat = B.atom_off[m + 1] - a0;
   const int sh0 = B.shell_off[m];
@@ -88,8 +94,8 @@ __global__ void __launch_bounds__(kGradThreads, kGradMinBlocks) grad_kernel(Batc
   __syncthreads();
 
   // ---- phase 1: atom pairs
-  const int npair = nat * (nat - 1) / 2;
-  for (int p = tid; p < npair; p += nt) {
+  const int npair = (phases & 1) ? nat * (nat - 1) / 2 : 0;
+  for (int p = tid + split * nt; p < npair; p += nt * nsplit) {
     // invert the pair index: a is the smaller atom
     int a = 0, rem = p;
     while (rem >= nat - 1 - a) {
@@ -162,6 +168,7 @@ __global__ void __launch_bounds__(kGradThreads, kGradMinBlocks) grad_kernel(Batc
     slot[6] = dcnu;
     slot[7] = dcmu;
   }
+  if (!(phases & 2) || split != 0) return;
   __syncthreads();
 
   // ---- phase 2: per-atom sums in a fixed pair order

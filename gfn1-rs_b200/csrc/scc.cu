@@ -757,13 +757,15 @@ __device__ __forceinline__ double eigenvalue_k(const double* d, const double* es
   return x;
 }
 
+// nwarm: eps[0..nwarm) and eps[N-1] hold the previous SCC iteration's
+// eigenvalues, the first iterates of their searches (0: none).
 template <int NT>
 __device__ void eigenvalues(const double* d, const double* esq, int N, int nneed, double gl, double gu,
-                            double pivmin, double atol, double* eps) {
+                            double pivmin, double atol, double* eps, int nwarm = 0) {
   const int nlist = (nneed < N) ? nneed + 1 : N;
   for (int slot = threadIdx.x; slot < nlist; slot += NT) {
     const int k = (slot < nneed) ? slot : N - 1;
-    eps[k] = eigenvalue_k(d, esq, N, k, gl, gu, pivmin, atol);
+    eps[k] = eigenvalue_k(d, esq, N, k, gl, gu, pivmin, atol, eps[k], nwarm > 0 && (k < nwarm || k == N - 1));
   }
   __syncthreads();
 }
@@ -1633,8 +1635,8 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     clk.mark(kStFock);
     // (3) Householder tridiagonalisation
     if constexpr (NT == 128) {
-      if (N <= 32 * 6 + 1)
-        tridiagonalize_blocked<NT>(A, lda, N, d, e, tau, pvec, eps, w.W1, sh);
+      if (N <= 32 * 6 + 1)  // e^2 is formed after the reduction, so its slot is the reduction's scratch
+        tridiagonalize_blocked<NT>(A, lda, N, d, e, tau, pvec, esq, w.W1, sh);
       else
         tridiagonalize<NT>(A, lda, N, d, e, tau, pvec, sh);
     } else {
@@ -1665,7 +1667,9 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     }
     int nneed = nneed0;
     for (int attempt = 0; attempt < 2; ++attempt) {
-      eigenvalues<NT>(d, esq, N, nneed, gl, gu, pivmin, 4.0 * DBL_EPSILON * onenrm, eps);
+      // from the previous iteration's eigenvalues once this rung has one
+      eigenvalues<NT>(d, esq, N, nneed, gl, gu, pivmin, 4.0 * DBL_EPSILON * onenrm, eps,
+                      (iter > 1 && attempt == 0) ? nneed_last : 0);
       clk.mark(kStEigval);
       // (5) occupations (src/electronic.rs:3815-3921)
       if (spin) {

@@ -124,10 +124,17 @@ __device__ double halogen_term(const Model& M, const int* zs, const double* xyz,
 
 // 128-thread CTAs, four per SM (128 registers): the s/p pairs fit, pairs with
 // a d shell (rare) keep part of their blocks in local memory.
-__global__ void __launch_bounds__(128, 4) setup_kernel(Batch B, Model M, int enable_dispersion, int max_nsh) {
+// Molecule blockIdx.x of `mols` (or of the batch when null).  Large molecules
+// are launched with gridDim.y > 1: every CTA of a molecule computes the
+// coordination numbers and self energies (cheap, identical), then takes every
+// gridDim.y-th block of its shell pairs for S, H0 and the Coulomb matrix; the
+// classical terms (repulsion, D3, halogen bonds) stay with blockIdx.y == 0.
+__global__ void __launch_bounds__(128, 4) setup_kernel(Batch B, Model M, int enable_dispersion, int max_nsh,
+                                                        const int* mols) {
   extern __shared__ double smem[];
-  const int m = blockIdx.x;
+  const int m = mols ? mols[blockIdx.x] : blockIdx.x;
   if (B.status[m] != kOk) return;  // rejected by the host-side validation
+  const int split = blockIdx.y, nsplit = gridDim.y;
   const int tid = threadIdx.x, nt = blockDim.x;
   const int a0 = B.atom_off[m], nat = B.atom_off[m + 1] - a0;
   const int sh0 = B.shell_off[m], nsh = B.shell_off[m + 1] - sh0;
@@ -200,7 +207,7 @@ __global__ void __launch_bounds__(128, 4) setup_kernel(Batch B, Model M, int ena
   double* S = B.S + B.mat_off[m];
   double* H0 = B.H0 + B.mat_off[m];
   const long long npairs = (long long)nsh * (nsh + 1) / 2;
-  for (long long w = tid; w < npairs; w += nt) {
+  for (long long w = tid + (long long)split * nt; w < npairs; w += (long long)nt * nsplit) {
     int si, sj;
     tri_inverse(w, si, sj);
     const int a = sh_atom[si], b = sh_atom[sj];
@@ -241,7 +248,7 @@ __global__ void __launch_bounds__(128, 4) setup_kernel(Batch B, Model M, int ena
 
   // ---- Klopman-Ohno matrix
   double* G = B.gam + B.gam_off[m];
-  for (long long w = tid; w < (long long)nsh * nsh; w += nt) {
+  for (long long w = tid + (long long)split * nt; w < (long long)nsh * nsh; w += (long long)nt * nsplit) {
     const int i = (int)(w / nsh), j = (int)(w % nsh);
     const int a = sh_atom[i], b = sh_atom[j];
     const double g = harmonic_avg(M.elem[zs[a]].hard[sh_k[i]], M.elem[zs[b]].hard[sh_k[j]]);
@@ -255,6 +262,7 @@ __global__ void __launch_bounds__(128, 4) setup_kernel(Batch B, Model M, int ena
     G[w] = v;
   }
 
+  if (split != 0) return;  // the classical terms: one CTA per molecule
   // ---- repulsion (pairs within 25 bohr), one thread per atom
   double erep = 0.0;
   for (int i = tid; i < nat; i += nt) {

@@ -523,9 +523,12 @@ constexpr int kPanelCache = 8192;  // doubles of the per-CTA cache of its rows' 
 
 struct TridiagSmall {
   double vj[kMaxPanel], wj[kMaxPanel], alpha2[kMaxPanel], vtv[kMaxPanel], wtv[kMaxPanel];
+  double vr[2][kMaxPanel], wr[2][kMaxPanel];  // rows j+1 of V and corrected W (double-buffered by column)
   double tot[2 * kMaxPanel + 2];
   double red[32];
   double scal[8];
+  double p1;   // p_{j+1} of the last column (w_{j+1} = p_{j+1} + alpha)
+  double ajj;  // A[j][j] as of the panel start (CTA 0)
 };
 
 // Rows per CTA the cache holds for panel width nb.
@@ -557,7 +560,6 @@ __global__ void __launch_bounds__(kRedNT) wide_tridiag_kernel(WideCtx X, int G, 
   double* vs = sm;                                       // v by absolute row index (maxn + 8)
   double* tsm = sm + X.maxn + 8;                         // tensor-core tiles of the trailing update
   double* cache = tsm + kTileSmemBytes / sizeof(double);  // [xs | V rows | W rows] of the CTA's rows
-  const int pcap = X.maxn + 8 + (int)(kTileSmemBytes / sizeof(double));  // staging room for partial sums (vs + tsm)
   GroupSync* cs = w.sync;
   GroupSync* ps = w.sync + 1;
   unsigned long long* cflags = w.flags;
@@ -592,34 +594,57 @@ __global__ void __launch_bounds__(kRedNT) wide_tridiag_kernel(WideCtx X, int G, 
     double* Vc = cache + R;          // Vc[l * R + (i - r0)]: panel reflectors of the CTA's rows
     double* Wc = Vc + (size_t)nb * R;  // Wc[l * R + (i - r0)]: p of the CTA's rows (w = p + alpha v)
     if (active) {
+      // The values every CTA needs from a column's owners ride along with the
+      // barrier data (x_{j+1} with the first partial sums, p_{j+1} with the
+      // second), row j+1's panel vectors are fetched before the first barrier,
+      // and the next column's A entries are prefetched during the
+      // matrix-vector product, so that a column costs two barriers and the
+      // product, not a chain of dependent loads.
+      double xa[4];    // A[i][jx] for this CTA's rows i = max(r0, jx+1) + tid + 256 k
+      int xa_col = -1;
+      const int Rmax = (nr + Ga - 1) / Ga;
+      const bool fuse_x = Rmax <= 32;  // peers' x values copied in the barrier wait
+      double* pstage = cache + (size_t)(2 * nb + 1) * R;  // staging of the partial sums
+      const int pst_cap = kPanelCache - (2 * nb + 1) * R;
       for (int l = 0; l < nbc; ++l) {
         const int j = k0 + l;
-        // ---- (A) x for the CTA's rows from the cached panel vectors
-        if (tid < l) {
-          const double v = ldcg(VW + (long long)tid * ld + j);
-          ss.vj[tid] = v;
-          ss.wj[tid] = ldcg(VW + (long long)(nb + tid) * ld + j) + ss.alpha2[tid] * v;
-        }
         const int ra = max(r0, j + 1);
-        double xa[4];
-        int na_ = 0;
-        for (int i = ra + tid; i < r1 && na_ < 4; i += kRedNT) xa[na_++] = ldcg(A + (long long)i * ld + j);
-        __syncthreads();
-        na_ = 0;
-        for (int i = ra + tid; i < r1; i += kRedNT) {
-          double x = na_ < 4 ? xa[na_++] : ldcg(A + (long long)i * ld + j);
-          const int ri = i - r0;
-          for (int q = 0; q < l; ++q) {
-            const double vi = Vc[q * R + ri];
-            const double wi = Wc[q * R + ri] + ss.alpha2[q] * vi;
-            x -= vi * ss.wj[q] + wi * ss.vj[q];
-          }
-          xs[ri] = x;
-          w.xbuf[i] = x;
+        const int par = l & 1;  // ss.vr/ss.wr[par]: row j+1 of V and W (q < l); [par ^ 1]: row j
+        // ---- (A) row j's V and W from the previous column (no loads)
+        if (tid < l) {
+          ss.vj[tid] = tid < l - 1 ? ss.vr[par ^ 1][tid] : 1.0;
+          ss.wj[tid] = tid < l - 1 ? ss.wr[par ^ 1][tid] : ss.p1 + ss.alpha2[l - 1];
+        } else if (tid >= 32 && tid - 32 < l) {  // row j+1's V and W, needed after the first barrier
+          const int q = tid - 32;
+          const double v1 = ldcg(VW + (long long)q * ld + j + 1);
+          ss.vr[par][q] = v1;
+          ss.wr[par][q] = ldcg(VW + (long long)(nb + q) * ld + j + 1) + ss.alpha2[q] * v1;
+        } else if (tid == 64 && c == 0) {
+          ss.ajj = ldcg(A + (long long)j * ld + j);
+        }
+        if (xa_col != j) {
+          int k = 0;
+          for (int i = ra + tid; i < r1 && k < 4; i += kRedNT) xa[k++] = ldcg(A + (long long)i * ld + j);
         }
         __syncthreads();
+        {
+          int k = 0;
+          for (int i = ra + tid; i < r1; i += kRedNT) {
+            double x = k < 4 ? xa[k++] : ldcg(A + (long long)i * ld + j);
+            const int ri = i - r0;
+            for (int q = 0; q < l; ++q) {
+              const double vi = Vc[q * R + ri];
+              const double wi = Wc[q * R + ri] + ss.alpha2[q] * vi;
+              x -= vi * ss.wj[q] + wi * ss.vj[q];
+            }
+            xs[ri] = x;
+            w.xbuf[i] = x;
+          }
+        }
+        __syncthreads();
+        const int nq = 2 * l + 1;  // partial sums; slot nq carries x_{j+1} from the CTA that owns row j+1
         const int rs = max(r0, j + 2);  // rows of the reflector's tail
-        for (int q = wid; q < 2 * l + 1; q += NW) {
+        for (int q = wid; q < nq; q += NW) {
           double sacc = 0.0;
           if (q == 0) {
             for (int i = rs + lane; i < r1; i += 32) sacc += xs[i - r0] * xs[i - r0];
@@ -636,58 +661,67 @@ __global__ void __launch_bounds__(kRedNT) wide_tridiag_kernel(WideCtx X, int G, 
           sacc = warp_sum(sacc);
           if (lane == 0) part[(long long)c * PS + q] = sacc;
         }
+        if (tid == 0) part[(long long)c * PS + nq] = (j + 1 >= r0 && j + 1 < r1) ? xs[j + 1 - r0] : 0.0;
         mark(0);
         // ---- (B) totals of the partials: each waiting thread copies its peer's
-        // row into shared memory (vs and the tile area are free here) as soon
-        // as that peer has arrived
-        const int nq = 2 * l + 1;
-        const bool fused = Ga * nq <= pcap;
-        {
-          double* pbuf = vs;
-          ok = flag_barrier(cflags, cs, c, Ga, ++cgen, [&](int t) {
-            if (!fused) return;
+        // partials (and, for few rows per CTA, its x values into v) as soon as
+        // that peer has arrived
+        const int nq1 = nq + 1;
+        const bool fused = Ga * nq1 <= pst_cap;
+        ok = flag_barrier(cflags, cs, c, Ga, ++cgen, [&](int t) {
+          if (fused) {
             const double* src = part + (long long)t * PS;
 #pragma unroll 8
-            for (int q = 0; q < nq; ++q) pbuf[t * nq + q] = ldcg(src + q);
-          });
-          if (!ok) break;
-          if (fused && tid < nq) {
+            for (int q = 0; q < nq1; ++q) pstage[t * nq1 + q] = ldcg(src + q);
+          }
+          if (fuse_x) {
+            const int t0 = k0 + 1 + (int)(((long long)nr * t) / Ga), t1 = k0 + 1 + (int)(((long long)nr * (t + 1)) / Ga);
+            const int u0 = max(t0, j + 2);
+            if (t == c) {
+              for (int i = u0; i < t1; ++i) vs[i] = xs[i - r0];
+            } else {
+#pragma unroll 4
+              for (int i = u0; i < t1; ++i) vs[i] = ldcg(w.xbuf + i);
+            }
+          }
+        });
+        if (!ok) break;
+        if (fused) {
+          if (tid < nq1) {
             double sacc = 0.0;
-            for (int cc = 0; cc < Ga; ++cc) sacc += pbuf[cc * nq + tid];
+            for (int cc = 0; cc < Ga; ++cc) sacc += pstage[cc * nq1 + tid];
             ss.tot[tid] = sacc;
           }
           __syncthreads();
-        }
-        mark(1);
-        if (!fused) {
-          double* pbuf = vs;
-          const int per = max(1, pcap / nq);  // CTAs' partials per chunk
+        } else {  // more partials than the staging holds: read them in chunks of CTAs
+          const int per = max(1, pst_cap / nq1);
           double sacc = 0.0;
           for (int cb = 0; cb < Ga; cb += per) {
-            const int cn = min(per, Ga - cb), tot_n = cn * nq;
+            const int cn = min(per, Ga - cb), tot_n = cn * nq1;
             for (int idx0 = 0; idx0 < tot_n; idx0 += 4 * kRedNT) {
               double t4[4];
 #pragma unroll
               for (int u = 0; u < 4; ++u) {
                 const int idx = idx0 + u * kRedNT + tid;
-                t4[u] = idx < tot_n ? ldcg(part + (long long)(cb + idx / nq) * PS + idx % nq) : 0.0;
+                t4[u] = idx < tot_n ? ldcg(part + (long long)(cb + idx / nq1) * PS + idx % nq1) : 0.0;
               }
 #pragma unroll
               for (int u = 0; u < 4; ++u) {
                 const int idx = idx0 + u * kRedNT + tid;
-                if (idx < tot_n) pbuf[idx] = t4[u];
+                if (idx < tot_n) pstage[idx] = t4[u];
               }
             }
             __syncthreads();
-            if (tid < nq)
-              for (int cc = 0; cc < cn; ++cc) sacc += pbuf[cc * nq + tid];
+            if (tid < nq1)
+              for (int cc = 0; cc < cn; ++cc) sacc += pstage[cc * nq1 + tid];
             __syncthreads();
           }
-          if (tid < nq) ss.tot[tid] = sacc;
+          if (tid < nq1) ss.tot[tid] = sacc;
           __syncthreads();
         }
+        mark(1);
         if (tid == 0) {
-          const double x0 = ldcg(w.xbuf + j + 1);
+          const double x0 = ss.tot[nq];
           const double sq = ss.tot[0];
           double beta = x0, tau = 0.0, scale = 0.0;
           if (sq > 0.0) {
@@ -699,23 +733,21 @@ __global__ void __launch_bounds__(kRedNT) wide_tridiag_kernel(WideCtx X, int G, 
           ss.scal[0] = tau;
           ss.scal[1] = scale;
           if (c == 0) {
-            double dj = ldcg(A + (long long)j * ld + j);
+            double dj = ss.ajj;
             for (int q = 0; q < l; ++q) dj -= 2.0 * ss.vj[q] * ss.wj[q];
             w.d[j] = dj;
             w.e[j] = beta;
             w.tau[j] = tau;
           }
-        } else if (tid >= 32 && tid - 32 < l) {
-          const int q = tid - 32;
-          const double v1 = ldcg(VW + (long long)q * ld + j + 1);
-          ss.vtv[q] = v1;  // completed below once scale is known
-          ss.wtv[q] = ldcg(VW + (long long)(nb + q) * ld + j + 1) + ss.alpha2[q] * v1;
         }
         __syncthreads();
         mark(2);
         const double tau = ss.scal[0], scale = ss.scal[1];
         const int kal = (j + 1) & ~1;
-        {  // v over rows kal..N+1, four loads in flight per thread
+        if (fuse_x) {  // v from the x values copied during the barrier
+          for (int k = kal + tid; k < N + 2; k += kRedNT)
+            vs[k] = k == j + 1 ? 1.0 : ((k > j + 1 && k < N) ? scale * vs[k] : 0.0);
+        } else {  // v over rows kal..N+1, four loads in flight per thread
           for (int k0v = kal; k0v < N + 2; k0v += 4 * kRedNT) {
             double t4[4];
 #pragma unroll
@@ -731,14 +763,21 @@ __global__ void __launch_bounds__(kRedNT) wide_tridiag_kernel(WideCtx X, int G, 
           }
         }
         if (tid < l) {
-          ss.vtv[tid] = ss.vtv[tid] + scale * ss.tot[1 + tid];
-          ss.wtv[tid] = ss.wtv[tid] + scale * ss.tot[1 + l + tid];
+          ss.vtv[tid] = ss.vr[par][tid] + scale * ss.tot[1 + tid];
+          ss.wtv[tid] = ss.wr[par][tid] + scale * ss.tot[1 + l + tid];
         }
         __syncthreads();
         mark(3);
+        // the next column's A entries for this CTA's rows (same panel only:
+        // the trailing update changes A between panels)
+        if (l + 1 < nbc) {
+          int k = 0;
+          for (int i = max(r0, j + 2) + tid; i < r1 && k < 4; i += kRedNT) xa[k++] = ldcg(A + (long long)i * ld + j + 1);
+          xa_col = j + 1;
+        }
         // symv over the CTA's rows: each warp takes two rows at a time, lanes
         // over column pairs, eight loads in flight per lane
-        double pv = 0.0;
+        double pv = 0.0, p1 = 0.0;
         const int npair = (N - kal + 1) >> 1;
         const double2* v2 = reinterpret_cast<const double2*>(vs + kal);
         auto finish_row = [&](int i, double t) {
@@ -758,6 +797,7 @@ __global__ void __launch_bounds__(kRedNT) wide_tridiag_kernel(WideCtx X, int G, 
             Wc[l * R + ri] = p_i;
             if (i >= j + 2) A[(long long)i * ld + j] = v_i;
             pv += p_i * v_i;
+            if (i == j + 1) p1 = p_i;
           }
         };
         int i = ra + 2 * wid;
@@ -801,24 +841,41 @@ __global__ void __launch_bounds__(kRedNT) wide_tridiag_kernel(WideCtx X, int G, 
           }
           finish_row(i, sa0 + sa1);
         }
-        if (lane == 0) ss.red[wid] = pv;
+        if (lane == 0) {
+          ss.red[wid] = pv;
+          ss.red[NW + wid] = p1;
+        }
         __syncthreads();
         if (tid == 0) {
-          double sacc = 0.0;
-          for (int q = 0; q < NW; ++q) sacc += ss.red[q];
+          double sacc = 0.0, s1 = 0.0;
+          for (int q = 0; q < NW; ++q) {
+            sacc += ss.red[q];
+            s1 += ss.red[NW + q];
+          }
           part[(long long)c * PS + PS - 1] = sacc;
+          part[(long long)c * PS + PS - 2] = s1;  // p_{j+1} from the CTA that owns row j+1, 0 elsewhere
         }
         mark(4);
-        {  // ---- (C) alpha = -tau (p.v) / 2 from the Ga partial sums
+        {  // ---- (C) alpha = -tau (p.v) / 2 and p_{j+1} from the Ga CTAs' rows
           double* pbuf = tsm;  // the tile area is free here
-          ok = flag_barrier(cflags, cs, c, Ga, ++cgen, [&](int t) { pbuf[t] = ldcg(part + (long long)t * PS + PS - 1); });
+          ok = flag_barrier(cflags, cs, c, Ga, ++cgen, [&](int t) {
+            pbuf[2 * t] = ldcg(part + (long long)t * PS + PS - 1);
+            pbuf[2 * t + 1] = ldcg(part + (long long)t * PS + PS - 2);
+          });
           if (!ok) break;
           mark(5);
           if (wid == 0) {
-            double sacc = 0.0;
-            for (int cc = lane; cc < Ga; cc += 32) sacc += pbuf[cc];
+            double sacc = 0.0, s1 = 0.0;
+            for (int cc = lane; cc < Ga; cc += 32) {
+              sacc += pbuf[2 * cc];
+              s1 += pbuf[2 * cc + 1];
+            }
             sacc = warp_sum(sacc);
-            if (lane == 0) ss.alpha2[l] = -0.5 * tau * sacc;
+            s1 = warp_sum(s1);
+            if (lane == 0) {
+              ss.alpha2[l] = -0.5 * tau * sacc;
+              ss.p1 = s1;
+            }
           }
           __syncthreads();
         }
