@@ -599,27 +599,22 @@ __device__ void tridiagonalize_blocked(double* A, int lda, int N, double* d, dou
           if (jj < m) A[(long long)k * lda + k + 1 + jj] = vreg[c];
         }
       }
-      // raw A22 v (four rows per warp pass) and the panel products W^T v, V^T v
+      // raw A22 v, one thread per entry: A22 is kept symmetric, so entry t is
+      // column t of A22 dotted with v, and each row of A22 read across the
+      // threads is contiguous (no cross-lane sums); v from shared memory
       const double* a22 = A + (long long)(k + 1) * lda + (k + 1);
-      for (int i0 = wid; i0 < m; i0 += 4 * NW) {
-        double s[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-        for (int c = 0; c < kCols; ++c) {
-          const int jj = lane + 32 * c;
-          if (jj < m) {
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-              const int i = i0 + r * NW;
-              if (i < m) s[r] += a22[(long long)i * lda + jj] * vreg[c];
-            }
-          }
+      for (int t = tid; t < m; t += NT) {
+        const double* col = a22 + t;
+        double s0 = col[0] * v0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        int r = 1;
+        for (; r + 3 < m; r += 4) {
+          s0 += col[(long long)r * lda] * xs[1 + r];
+          s1 += col[(long long)(r + 1) * lda] * xs[2 + r];
+          s2 += col[(long long)(r + 2) * lda] * xs[3 + r];
+          s3 += col[(long long)(r + 3) * lda] * xs[4 + r];
         }
-        warp_sum4(s[0], s[1], s[2], s[3]);
-        if (lane == 0) {
-#pragma unroll
-          for (int r = 0; r < 4; ++r)
-            if (i0 + r * NW < m) pvec[i0 + r * NW] = s[r];
-        }
+        for (; r < m; ++r) s0 += col[(long long)r * lda] * xs[1 + r];
+        pvec[t] = (s0 + s1) + (s2 + s3);
       }
       for (int l = wid; l < j; l += NW) {
         const double* vl = A + (long long)(k0 + l) * lda + (k + 1);

@@ -20,6 +20,15 @@ def _flat(mols):
     return off, np.concatenate([z for z, _ in mols]), np.concatenate([x for _, x in mols])
 
 
+def _rungs_under_rounding(oracle_mod, z, x, shift, trials=6):
+    opts = oracle_mod.make_options(level_shift=shift, **TIGHT)
+    rng = np.random.default_rng(0)
+    rungs = {oracle_mod.run(z, x, options=opts).rung}
+    for _ in range(trials):
+        rungs.add(oracle_mod.run(z, x + 1e-12 * rng.standard_normal(x.shape), options=opts).rung)
+    return rungs
+
+
 @pytest.mark.parametrize("shift", [0.3, 0.05])
 def test_level_shift_matches_oracle(gpu_calc, oracle_mod, fixtures, shift):
     from gfn1_rs import BatchCalculator
@@ -36,8 +45,12 @@ def test_level_shift_matches_oracle(gpu_calc, oracle_mod, fixtures, shift):
         assert np.max(np.abs(r.gradient[a0:a1] - o.gradient)) <= 1e-5, NAMES[m]
         # the shift moves the path, not the fixed point
         assert abs(r.energy[m] - plain.energy[m]) <= 1e-6, NAMES[m]
-        # ferrocene at 0.3 Eh: rung 0 needs 519 iterations (oracle), so rung 1 converges it
-        assert r.rung[m] == o.rung and plain.rung[m] == 0, NAMES[m]
+        # ferrocene at 0.3 Eh: rung 0 needs 519 iterations (oracle), so rung 1
+        # converges it.  Caffeine at 0.3 Eh sits on the edge: rung 0 takes 146
+        # iterations on the oracle, and 174-245 or a failure (then rung 1) when
+        # the coordinates move by 1e-12 bohr, so the rung is checked against
+        # the rungs the oracle reaches under such rounding-level perturbations.
+        assert r.rung[m] in _rungs_under_rounding(oracle_mod, zm, xm, shift) and plain.rung[m] == 0, NAMES[m]
 
 
 def test_level_shift_on_the_large_molecule_path(gpu_calc, oracle_mod, fixtures):
