@@ -849,7 +849,7 @@ int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t*
     const int count = K.q_end - K.q_begin;
     const size_t fixed = scc_smem_bytes(K.maxnsh, K.maxn, K.maxnat, 0);
     while (K.nt < 512 && fixed > scc_max_dynamic_smem(K.nt)) K.nt *= 2;  // vectors of big molecules need room
-    K.n_cta = count == 0 ? 0 : std::max(1, std::min(count, (512 / K.nt) * eng->num_sms));
+    K.n_cta = count == 0 ? 0 : std::max(1, std::min(count, (kSccThreadsPerSm / K.nt) * eng->num_sms));
     K.ws_stride = count == 0 ? 0 : scc_workspace_doubles(std::max(K.maxn, 1), std::max(K.maxnsh, 1), b->cap,
                                                            std::max(K.maxnat, 1));
     K.ws_offset = ws_total;
@@ -874,7 +874,7 @@ int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t*
     const size_t fixed = scc_smem_bytes(R.maxnsh, R.maxn, R.maxnat, 0);
     while (R.nt < 512 && fixed > scc_max_dynamic_smem(R.nt)) R.nt *= 2;
     // a requested level shift runs every molecule on this kernel: full width
-    const int width = o.level_shift != 0.0 ? (512 / R.nt) * eng->num_sms : 64;
+    const int width = o.level_shift != 0.0 ? (kSccThreadsPerSm / R.nt) * eng->num_sms : 64;
     R.n_cta = count == 0 ? 0 : std::min(count, width);
     R.ws_stride = count == 0 ? 0 : scc_workspace_doubles(std::max(R.maxn, 1), std::max(R.maxnsh, 1), b->cap,
                                                            std::max(R.maxnat, 1));

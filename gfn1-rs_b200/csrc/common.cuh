@@ -128,10 +128,17 @@ struct Batch {
   unsigned long long* stage_cycles;  // [kStages] per-stage clock totals, or null
 };
 
+// Threads of the persistent SCC kernel resident per SM: 128-thread CTAs run
+// kSccThreadsPerSm / 128 to an SM (the register budget per thread follows).
+#ifndef GFN1_SCC_THREADS_PER_SM
+#define GFN1_SCC_THREADS_PER_SM 512
+#endif
+constexpr int kSccThreadsPerSm = GFN1_SCC_THREADS_PER_SM;
+
 // SCC stages timed when Batch::stage_cycles is set (the device counterpart of
 // the reference's GFN1_PROFILE scopes, src/electronic.rs:1448, :2089-2157).
 enum Stage : int {
-  kStPrologue = 0,  // Cholesky, L^-1, H0'
+  kStPrologue = 0,  // H0' and the SCC state (Cholesky and L^-1: kStChol, kStLinv)
   kStFock,          // shell potential + F'
   kStTridiag,       // Householder reduction
   kStEigval,        // bisection
@@ -142,6 +149,8 @@ enum Stage : int {
   kStEnergy,        // output charges, energies, convergence test
   kStMix,           // Broyden / damped mixing
   kStFinal,         // P, W and results
+  kStChol,          // Cholesky S = L L^T
+  kStLinv,          // L^-1
   kStages
 };
 

@@ -1014,24 +1014,36 @@ __device__ void back_transform(const double* A, int lda, const double* tau, int 
         __syncwarp();
       }
     }
-    // W1 = V^T Z on the FP64 tensor cores: 8x8 tiles of (reflector j,
-    // column c), k over the rows r; reflector j has entries r > kb + j
+    // W1 = V^T Z on the FP64 tensor cores: pairs of 8x8 tiles of (reflector
+    // j, column c) sharing the reflector fragment, k over the rows r;
+    // reflector j has entries r > kb + j
     {
       const int g = lane >> 2, t4 = lane & 3;
-      const int TC = (ncol + 7) >> 3, TJ = (nb + 7) >> 3;
-      for (int tile = wid; tile < TJ * TC; tile += NW) {
-        const int JT = tile / TC, CT = tile - JT * TC;
-        const int j = JT * 8 + g, cb = CT * 8 + g;
-        double d0 = 0.0, d1 = 0.0;
+      const int TC = (ncol + 7) >> 3, TJ = (nb + 7) >> 3, TC2 = (TC + 1) >> 1;
+      for (int tile = wid; tile < TJ * TC2; tile += NW) {
+        const int JT = tile / TC2, CT = 2 * (tile - JT * TC2);
+        const int j = JT * 8 + g, cb0 = CT * 8 + g, cb1 = cb0 + 8;
+        const bool jok = j < nb, ok0 = cb0 < ncol, ok1 = cb1 < ncol;
+        const double* vj = A + (long long)(kb + (jok ? j : 0)) * lda;
+        double d00 = 0.0, d01 = 0.0, d10 = 0.0, d11 = 0.0;
         for (int r0 = kb + 1; r0 < N; r0 += 4) {
           const int r = r0 + t4;
-          const double a = (j < nb && r < N && r > kb + j) ? A[(long long)(kb + j) * lda + r] : 0.0;
-          const double b = (r < N && cb < ncol) ? Z[(long long)r * ldz + cb] : 0.0;
-          dmma_m8n8k4(d0, d1, a, b);
+          const bool rin = r < N;
+          const double* zr = Z + (long long)(rin ? r : 0) * ldz;
+          const double a = (jok && rin && r > kb + j) ? vj[r] : 0.0;
+          const double b0 = (rin && ok0) ? zr[cb0] : 0.0;
+          const double b1 = (rin && ok1) ? zr[cb1] : 0.0;
+          dmma_m8n8k4(d00, d01, a, b0);
+          dmma_m8n8k4(d10, d11, a, b1);
         }
         const int cc = CT * 8 + 2 * t4;
-        if (j < nb && cc < ncol) W1[j * ncol + cc] = d0;
-        if (j < nb && cc + 1 < ncol) W1[j * ncol + cc + 1] = d1;
+        if (jok) {
+          double* w1 = W1 + j * ncol;
+          if (cc < ncol) w1[cc] = d00;
+          if (cc + 1 < ncol) w1[cc + 1] = d01;
+          if (cc + 8 < ncol) w1[cc + 8] = d10;
+          if (cc + 9 < ncol) w1[cc + 9] = d11;
+        }
       }
     }
     __syncthreads();
@@ -1042,24 +1054,37 @@ __device__ void back_transform(const double* A, int lda, const double* tau, int 
       W2[j * ncol + c] = s;
     }
     __syncthreads();
-    // Z -= V W2 on the FP64 tensor cores: 8x8 tiles of (row r, column c)
-    // starting from Z, k over the reflectors j
+    // Z -= V W2 on the FP64 tensor cores: pairs of 8x8 tiles of (row r,
+    // column c) sharing the reflector fragment, starting from Z, k over the
+    // reflectors j
     {
       const int g = lane >> 2, t4 = lane & 3;
-      const int TC = (ncol + 7) >> 3, TR = (N - kb - 1 + 7) >> 3;
-      for (int tile = wid; tile < TR * TC; tile += NW) {
-        const int RT = tile / TC, CT = tile - RT * TC;
-        const int r = kb + 1 + RT * 8 + g, cb = CT * 8 + g, cc = CT * 8 + 2 * t4;
-        double d0 = (r < N && cc < ncol) ? Z[(long long)r * ldz + cc] : 0.0;
-        double d1 = (r < N && cc + 1 < ncol) ? Z[(long long)r * ldz + cc + 1] : 0.0;
+      const int TC = (ncol + 7) >> 3, TR = (N - kb - 1 + 7) >> 3, TC2 = (TC + 1) >> 1;
+      for (int tile = wid; tile < TR * TC2; tile += NW) {
+        const int RT = tile / TC2, CT = 2 * (tile - RT * TC2);
+        const int r = kb + 1 + RT * 8 + g, cb0 = CT * 8 + g, cb1 = cb0 + 8, cc = CT * 8 + 2 * t4;
+        const bool rok = r < N, ok0 = cb0 < ncol, ok1 = cb1 < ncol;
+        double* zr = Z + (long long)(rok ? r : 0) * ldz;
+        double d00 = (rok && cc < ncol) ? zr[cc] : 0.0;
+        double d01 = (rok && cc + 1 < ncol) ? zr[cc + 1] : 0.0;
+        double d10 = (rok && cc + 8 < ncol) ? zr[cc + 8] : 0.0;
+        double d11 = (rok && cc + 9 < ncol) ? zr[cc + 9] : 0.0;
         for (int j0 = 0; j0 < nb; j0 += 4) {
           const int j = j0 + t4;
-          const double a = (r < N && j < nb && r > kb + j) ? -A[(long long)(kb + j) * lda + r] : 0.0;
-          const double b = (j < nb && cb < ncol) ? W2[j * ncol + cb] : 0.0;
-          dmma_m8n8k4(d0, d1, a, b);
+          const bool jok = j < nb;
+          const double a = (rok && jok && r > kb + j) ? -A[(long long)(kb + j) * lda + r] : 0.0;
+          const double* w2 = W2 + (jok ? j : 0) * ncol;
+          const double b0 = (jok && ok0) ? w2[cb0] : 0.0;
+          const double b1 = (jok && ok1) ? w2[cb1] : 0.0;
+          dmma_m8n8k4(d00, d01, a, b0);
+          dmma_m8n8k4(d10, d11, a, b1);
         }
-        if (r < N && cc < ncol) Z[(long long)r * ldz + cc] = d0;
-        if (r < N && cc + 1 < ncol) Z[(long long)r * ldz + cc + 1] = d1;
+        if (rok) {
+          if (cc < ncol) zr[cc] = d00;
+          if (cc + 1 < ncol) zr[cc + 1] = d01;
+          if (cc + 8 < ncol) zr[cc + 8] = d10;
+          if (cc + 9 < ncol) zr[cc + 9] = d11;
+        }
       }
     }
     __syncthreads();
@@ -1457,6 +1482,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
   for (int i = wid; i < N; i += NW)
     for (int j = i + 1 + lane; j < N; j += 32) L[(long long)i * N + j] = 0.0;
   __syncthreads();
+  clk.mark(kStChol);
   // L^-1 by forward substitution L X = I, one thread per column; all threads
   // step through the rows together, so row i of L is a broadcast and the reads
   // of X[k][c] coalesce (the entries above the diagonal come out as zeros)
@@ -1476,6 +1502,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     }
   }
   __syncthreads();
+  clk.mark(kStLinv);
   // H0' = L^-1 H0 L^-T on the FP64 tensor cores: U = L^-1 H0 in 8x8 tiles
   // (row i of L^-1 ends at the diagonal), then H0' = U (L^-1)^T for the tiles
   // on and below the diagonal, each written to both triangles so that H0' is
@@ -1581,29 +1608,45 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     stage_potential<NT>(B, M, mc, w, vao);
     // (2) F' = H0' - 1/2 (M + M^T) with M = L^-1 diag(v) L lower triangular,
     //     so F'_ij = H0'_ij - M_ij / 2 below the diagonal and H0'_ii - M_ii on
-    //     it.  M on the FP64 tensor cores, 8x8 tiles on and below the
-    //     diagonal, k from the tile's first column to its last row.
+    //     it.  M on the FP64 tensor cores: pairs of 8x8 tiles (I, J), (I, J+1)
+    //     on and below the diagonal sharing the L^-1 fragment, k from the
+    //     pair's first column to its last row (the entries of L above the
+    //     diagonal are stored zeros, so the second tile's extra k add nothing).
     {
       const int T = (N + 7) >> 3;
       const int g = lane >> 2, t4 = lane & 3;
-      for (int tile = wid; tile < T * (T + 1) / 2; tile += NW) {
-        int I = 0;
-        while ((I + 1) * (I + 2) / 2 <= tile) ++I;
-        const int J = tile - I * (I + 1) / 2;
-        const int i = I * 8 + g, jb = J * 8 + g;
+      int I = 0, base = 0;  // base: pairs of the rows of tiles before I
+      for (int task = wid;; task += NW) {
+        while (I < T && task >= base + (I >> 1) + 1) {
+          base += (I >> 1) + 1;
+          ++I;
+        }
+        if (I >= T) break;
+        const int J = 2 * (task - base);
+        const bool two = J + 1 <= I;
+        const int i = I * 8 + g, jb0 = J * 8 + g, jb1 = jb0 + 8;
+        const bool iok = i < N;
+        const double* lirow = Li + (long long)(iok ? i : 0) * N;
         const int kend = min(N, I * 8 + 8);
-        double d0 = 0.0, d1 = 0.0;
+        double d00 = 0.0, d01 = 0.0, d10 = 0.0, d11 = 0.0;
         for (int k0 = J * 8; k0 < kend; k0 += 4) {
           const int k = k0 + t4;
-          const double a = (i < N && k < N) ? Li[(long long)i * N + k] : 0.0;
-          const double b = (k < N && jb < N) ? L[(long long)k * N + jb] * vao[k] : 0.0;
-          dmma_m8n8k4(d0, d1, a, b);
+          const bool kin = k < N;
+          const double* lk = L + (long long)(kin ? k : 0) * N;
+          const double vk = kin ? vao[k] : 0.0;
+          const double a = (iok && kin) ? lirow[k] : 0.0;
+          const double b0 = (kin && jb0 < N) ? lk[jb0] * vk : 0.0;
+          dmma_m8n8k4(d00, d01, a, b0);
+          if (two) {
+            const double b1 = (kin && jb1 < N) ? lk[jb1] * vk : 0.0;
+            dmma_m8n8k4(d10, d11, a, b1);
+          }
         }
 #pragma unroll
-        for (int c = 0; c < 2; ++c) {
-          const int j = J * 8 + 2 * t4 + c;
-          if (i < N && j <= i) {
-            const double mv = c ? d1 : d0;
+        for (int c = 0; c < 4; ++c) {
+          const int j = J * 8 + 2 * t4 + (c & 1) + (c >> 1) * 8;
+          if (iok && j <= i && (c < 2 || two)) {
+            const double mv = c == 0 ? d00 : c == 1 ? d01 : c == 2 ? d10 : d11;
             const double f = Hp[(long long)i * N + j] - (i == j ? mv : 0.5 * mv);
             A[(long long)i * lda + j] = f;
             A[(long long)j * lda + i] = f;
@@ -1744,39 +1787,60 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     clk.mark(kStBackTr);
     // (8) C = L^-T Z, D = L Z (= S C) and the AO populations
     //     (S P)_mu,mu = sum_i f_i C_mu,i D_mu,i on the FP64 tensor cores: each
-    //     warp owns 8-row blocks of mu and runs over 8-column tiles of the
-    //     occupied eigenvectors.  Row mu of L ends and column mu of L^-1 starts
-    //     at the diagonal.  D only feeds the populations and is not stored.
+    //     warp owns 8-row blocks of mu and runs over pairs of 8-column tiles
+    //     of the occupied eigenvectors (the rows of L and L^-T are shared by
+    //     the pair; four independent accumulator chains where the ranges of
+    //     k overlap).  Row mu of L ends and column mu of L^-1 starts at the
+    //     diagonal.  D only feeds the populations and is not stored.
     {
       const int T = (N + 7) >> 3, Ti = (nocc + 7) >> 3;
       const int g = lane >> 2, t4 = lane & 3;
       for (int MU = wid; MU < T; MU += NW) {
         const int mu = MU * 8 + g;
+        const bool mu_ok = mu < N;
+        const double* lrow = L + (long long)(mu_ok ? mu : 0) * N;
+        const int kd = min(N, MU * 8 + 8), kc = MU * 8;  // D: k < kd; C: k >= kc
         double pp = 0.0;
-        for (int IV = 0; IV < Ti; ++IV) {
-          const int ib = IV * 8 + g;
-          double c0 = 0.0, c1 = 0.0, d0 = 0.0, d1 = 0.0;
-          const int dend = min(N, MU * 8 + 8);
-          for (int k0 = 0; k0 < dend; k0 += 4) {
+        for (int IV = 0; IV < Ti; IV += 2) {
+          const int ib0 = IV * 8 + g, ib1 = ib0 + 8;
+          const bool ok0 = ib0 < nocc, ok1 = ib1 < nocc;
+          double c00 = 0.0, c01 = 0.0, c10 = 0.0, c11 = 0.0;
+          double d00 = 0.0, d01 = 0.0, d10 = 0.0, d11 = 0.0;
+          for (int k0 = 0; k0 < N; k0 += 4) {
             const int k = k0 + t4;
-            const double a = (mu < N && k < N) ? L[(long long)mu * N + k] : 0.0;
-            const double b = (k < N && ib < nocc) ? Z[(long long)k * N + ib] : 0.0;
-            dmma_m8n8k4(d0, d1, a, b);
-          }
-          for (int k0 = MU * 8; k0 < N; k0 += 4) {
-            const int k = k0 + t4;
-            const double a = (mu < N && k < N) ? Li[(long long)k * N + mu] : 0.0;
-            const double b = (k < N && ib < nocc) ? Z[(long long)k * N + ib] : 0.0;
-            dmma_m8n8k4(c0, c1, a, b);
+            const bool kin = k < N;
+            const double* zk = Z + (long long)(kin ? k : 0) * N;
+            const double b0 = (kin && ok0) ? zk[ib0] : 0.0;
+            const double b1 = (kin && ok1) ? zk[ib1] : 0.0;
+            if (k0 < kd) {
+              const double a = (mu_ok && kin) ? lrow[k] : 0.0;
+              dmma_m8n8k4(d00, d01, a, b0);
+              dmma_m8n8k4(d10, d11, a, b1);
+            }
+            if (k0 >= kc) {
+              const double a = (mu_ok && kin) ? Li[(long long)k * N + mu] : 0.0;
+              dmma_m8n8k4(c00, c01, a, b0);
+              dmma_m8n8k4(c10, c11, a, b1);
+            }
           }
           const int ic = IV * 8 + 2 * t4;
-          if (mu < N && ic < nocc) {
-            C[(long long)mu * N + ic] = c0;
-            pp += occ[ic] * c0 * d0;
-          }
-          if (mu < N && ic + 1 < nocc) {
-            C[(long long)mu * N + ic + 1] = c1;
-            pp += occ[ic + 1] * c1 * d1;
+          if (mu_ok) {
+            if (ic < nocc) {
+              C[(long long)mu * N + ic] = c00;
+              pp += occ[ic] * c00 * d00;
+            }
+            if (ic + 1 < nocc) {
+              C[(long long)mu * N + ic + 1] = c01;
+              pp += occ[ic + 1] * c01 * d01;
+            }
+            if (ic + 8 < nocc) {
+              C[(long long)mu * N + ic + 8] = c10;
+              pp += occ[ic + 8] * c10 * d10;
+            }
+            if (ic + 9 < nocc) {
+              C[(long long)mu * N + ic + 9] = c11;
+              pp += occ[ic + 9] * c11 * d11;
+            }
           }
         }
         pp += __shfl_xor_sync(0xffffffffu, pp, 1);
@@ -1871,7 +1935,8 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
 // processing order (rung 0 of the fallback ladder); Robust = true: the
 // molecules the rung-0 launches left unconverged (rungs 1-3).
 template <int NT, bool Robust>
-__global__ void __launch_bounds__(NT, 512 / NT) scc_kernel(Batch B, Model M, SccOptions opt, SccLaunch SL) {
+__global__ void __launch_bounds__(NT, (kSccThreadsPerSm / NT) > 0 ? kSccThreadsPerSm / NT : 1)
+    scc_kernel(Batch B, Model M, SccOptions opt, SccLaunch SL) {
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ SccShared sh;
   __shared__ int next;
@@ -1936,7 +2001,7 @@ size_t scc_smem_bytes(int maxnsh, int maxn, int maxnat, int matrix_n) {
 }
 
 // Largest dynamic shared memory a CTA of the class may request: the SM's
-// 228 KB shared by its 512 / nt CTAs (1 KB of which each CTA reserves), less
+// 228 KB shared by its kSccThreadsPerSm / nt CTAs (1 KB of which each CTA reserves), less
 // the kernel's static shared memory.
 size_t scc_max_dynamic_smem(int nt) {
   cudaFuncAttributes a;
@@ -1944,7 +2009,8 @@ size_t scc_max_dynamic_smem(int nt) {
                         : nt == 256 ? cudaFuncGetAttributes(&a, scc_kernel<256, false>)
                                     : cudaFuncGetAttributes(&a, scc_kernel<128, false>);
   const size_t stat = e == cudaSuccess ? a.sharedSizeBytes : 8192;
-  const size_t per_cta = 233472 / (512 / nt) - 1024;  // the SM's 228 KB shared by 512/nt CTAs
+  const int ctas = std::max(1, kSccThreadsPerSm / nt);
+  const size_t per_cta = 233472 / ctas - 1024;  // the SM's 228 KB shared by its CTAs
   return per_cta - stat - 256;
 }
 

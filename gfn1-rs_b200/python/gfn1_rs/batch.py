@@ -271,7 +271,8 @@ class ResidentBatch:
         s = None if stream is None else ctypes.c_void_p(int(stream))
         _lib.check(_lib.load().gfn1_batch_launch_stage(self.handle, int(stage), s), self.calc.engine.handle)
 
-    STAGES = ("prologue", "fock", "tridiag", "eigval", "fermi", "inviter", "backtr", "pop", "energy", "mix", "final")
+    STAGES = ("prologue", "fock", "tridiag", "eigval", "fermi", "inviter", "backtr", "pop", "energy", "mix", "final",
+              "chol", "linv")
 
     def stage_cycles(self) -> dict:
         """Per-stage SCC clock totals (batch created with GFN1_PROFILE=1)."""

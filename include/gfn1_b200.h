@@ -152,9 +152,10 @@ int gfn1_batch_launch(gfn1_batch* b, void* stream);
  * 1 = persistent SCC, 2 = gradient; -1 = all three (same as gfn1_batch_launch).
  * Lets a caller time each kernel with events on its own stream. */
 int gfn1_batch_launch_stage(gfn1_batch* b, int stage, void* stream);
-/* Per-stage SCC clock totals (GFN1_PROFILE=1 at batch creation), n <= 11:
- * prologue, Fock, tridiagonalisation, eigenvalues, occupations, inverse
- * iteration, back-transformation, populations, energy, mixing, final. */
+/* Per-stage SCC clock totals (GFN1_PROFILE=1 at batch creation), n <= 13:
+ * prologue (H0' and the SCC state), Fock, tridiagonalisation, eigenvalues,
+ * occupations, inverse iteration, back-transformation, populations, energy,
+ * mixing, final, Cholesky, L^-1. */
 int gfn1_batch_stage_cycles(const gfn1_batch* b, uint64_t* cycles, int n);
 /* Bytes of the input blob (one host->device copy per call) and of the output
  * blob (one device->host copy per call). */
