@@ -607,11 +607,18 @@ __device__ void tridiagonalize_blocked(double* A, int lda, int N, double* d, dou
         const double* col = a22 + t;
         double s0 = col[0] * v0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
         int r = 1;
-        for (; r + 3 < m; r += 4) {
-          s0 += col[(long long)r * lda] * xs[1 + r];
-          s1 += col[(long long)(r + 1) * lda] * xs[2 + r];
-          s2 += col[(long long)(r + 2) * lda] * xs[3 + r];
-          s3 += col[(long long)(r + 3) * lda] * xs[4 + r];
+        for (; r + 7 < m; r += 8) {  // eight loads in flight per thread
+          double a[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) a[u] = col[(long long)(r + u) * lda];
+          s0 += a[0] * xs[1 + r];
+          s1 += a[1] * xs[2 + r];
+          s2 += a[2] * xs[3 + r];
+          s3 += a[3] * xs[4 + r];
+          s0 += a[4] * xs[5 + r];
+          s1 += a[5] * xs[6 + r];
+          s2 += a[6] * xs[7 + r];
+          s3 += a[7] * xs[8 + r];
         }
         for (; r < m; ++r) s0 += col[(long long)r * lda] * xs[1 + r];
         pvec[t] = (s0 + s1) + (s2 + s3);
@@ -1026,6 +1033,7 @@ __device__ void back_transform(const double* A, int lda, const double* tau, int 
         const bool jok = j < nb, ok0 = cb0 < ncol, ok1 = cb1 < ncol;
         const double* vj = A + (long long)(kb + (jok ? j : 0)) * lda;
         double d00 = 0.0, d01 = 0.0, d10 = 0.0, d11 = 0.0;
+#pragma unroll 4
         for (int r0 = kb + 1; r0 < N; r0 += 4) {
           const int r = r0 + t4;
           const bool rin = r < N;
@@ -1069,6 +1077,7 @@ __device__ void back_transform(const double* A, int lda, const double* tau, int 
         double d01 = (rok && cc + 1 < ncol) ? zr[cc + 1] : 0.0;
         double d10 = (rok && cc + 8 < ncol) ? zr[cc + 8] : 0.0;
         double d11 = (rok && cc + 9 < ncol) ? zr[cc + 9] : 0.0;
+#pragma unroll 4
         for (int j0 = 0; j0 < nb; j0 += 4) {
           const int j = j0 + t4;
           const bool jok = j < nb;
@@ -1444,33 +1453,85 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
 
   StageClock clk(B.stage_cycles);
   const MolCtx mc{m, a0, nat, sh0, nsh, N, sh_atom, sh_k, sh_ao0, ao_sh, atom_sh, G};
-  // ---- Cholesky S = L L^T (right-looking, in place on L)
-  double* colk = eps;  // current column of L (the eigenvalue slot is free until the first iteration)
+  // ---- Cholesky S = L L^T, left-looking over panels of 8 columns: the
+  // panel minus (its rows of L) x (the panel's rows of L)^T over the finished
+  // columns on the FP64 tensor cores, the 8x8 diagonal block by one thread
+  // (registers; its factor and reciprocal pivots staged in shared memory),
+  // then the rows below by a triangular solve, one thread per row.
   for (long long i = tid; i < (long long)N * N; i += NT) L[i] = S[i];
   __syncthreads();
-  for (int k = 0; k < N; ++k) {
-    if (tid == 0) {
-      const double a = L[(long long)k * N + k];
-      // the reference rejects overlaps with an eigenvalue <= eigen_tolerance (1e-12)
-      if (!(a > 1e-12)) sh.iscal[0] = kErrInvalidInput;
-      const double r = sqrt(fmax(a, 1e-300));
-      L[(long long)k * N + k] = r;
-      sh.scal[0] = r;
+  {
+    const int g = lane >> 2, t4 = lane & 3;
+    double(*Ld)[kBackNB] = sh.Tm;  // free until the first back-transformation
+    for (int c0 = 0; c0 < N; c0 += 8) {
+      const int nbc = min(8, N - c0);
+      if (c0 > 0) {
+        const int TR = (N - c0 + 7) >> 3;
+        const bool jok = g < nbc;
+        const double* lj = L + (long long)(jok ? c0 + g : 0) * N;
+        for (int RT = wid; RT < TR; RT += NW) {
+          const int i = c0 + RT * 8 + g;
+          const bool iok = i < N;
+          const double* li = L + (long long)(iok ? i : 0) * N;
+          double d0 = 0.0, d1 = 0.0;
+#pragma unroll 4
+          for (int k0 = 0; k0 < c0; k0 += 4) {
+            const int k = k0 + t4;
+            dmma_m8n8k4(d0, d1, iok ? li[k] : 0.0, jok ? lj[k] : 0.0);
+          }
+          if (iok) {
+            double* out = L + (long long)i * N + c0 + 2 * t4;
+            if (2 * t4 < nbc) out[0] -= d0;
+            if (2 * t4 + 1 < nbc) out[1] -= d1;
+          }
+        }
+        __syncthreads();
+      }
+      if (tid == 0) {
+        double D[8][8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+          for (int j = 0; j <= i; ++j) D[i][j] = (i < nbc) ? L[(long long)(c0 + i) * N + c0 + j] : (i == j ? 1.0 : 0.0);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          // the reference rejects overlaps with an eigenvalue <= eigen_tolerance (1e-12)
+          if (j < nbc && !(D[j][j] > 1e-12)) sh.iscal[0] = kErrInvalidInput;
+          const double r = sqrt(fmax(D[j][j], 1e-300));
+          const double inv = 1.0 / r;
+          D[j][j] = r;
+          Ld[j][8] = inv;
+#pragma unroll
+          for (int i = j + 1; i < 8; ++i) D[i][j] *= inv;
+#pragma unroll
+          for (int k = j + 1; k < 8; ++k)
+#pragma unroll
+            for (int i = k; i < 8; ++i) D[i][k] -= D[i][j] * D[k][j];
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+          for (int j = 0; j <= i; ++j) {
+            Ld[i][j] = D[i][j];
+            if (i < nbc) L[(long long)(c0 + i) * N + c0 + j] = D[i][j];
+          }
+      }
+      __syncthreads();
+      for (int i = c0 + 8 + tid; i < N; i += NT) {  // rows below: x L_dd^T = row
+        double* row = L + (long long)i * N + c0;
+        double x[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) x[j] = row[j];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+#pragma unroll
+          for (int k = 0; k < j; ++k) x[j] -= x[k] * Ld[j][k];
+          x[j] *= Ld[j][8];
+          row[j] = x[j];
+        }
+      }
+      __syncthreads();
     }
-    __syncthreads();
-    const double lkk = sh.scal[0];
-    for (int i = k + 1 + tid; i < N; i += NT) {  // column k, also staged in shared memory
-      const double v = L[(long long)i * N + k] / lkk;
-      L[(long long)i * N + k] = v;
-      colk[i] = v;
-    }
-    __syncthreads();
-    for (int i = k + 1 + wid; i < N; i += NW) {
-      const double lik = colk[i];
-      double* li = L + (long long)i * N;
-      for (int j = k + 1 + lane; j <= i; j += 32) li[j] -= lik * colk[j];
-    }
-    __syncthreads();
   }
   if (sh.iscal[0] != kOk) {
     if (tid == 0) {
@@ -1483,22 +1544,28 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     for (int j = i + 1 + lane; j < N; j += 32) L[(long long)i * N + j] = 0.0;
   __syncthreads();
   clk.mark(kStChol);
-  // L^-1 by forward substitution L X = I, one thread per column; all threads
-  // step through the rows together, so row i of L is a broadcast and the reads
-  // of X[k][c] coalesce (the entries above the diagonal come out as zeros)
+  // L^-1 by forward substitution L X = I, one thread per column.  The lanes
+  // of a warp step through the rows together, so row i of L is a broadcast
+  // and the reads of X[k][c] coalesce; a warp starts at its first column
+  // (rows above it are zeros in all of its columns), four partial sums.
   for (int c0 = 0; c0 < N; c0 += NT) {
     const int c = c0 + tid;
     const int cc = min(c, N - 1);
-    for (int i = 0; i < N; ++i) {
+    const int kw = min(N, c0 + (tid & ~31));  // the warp's first column
+    if (c < N)
+      for (int i = 0; i < kw; ++i) Li[(long long)i * N + c] = 0.0;
+    for (int i = kw; i < N; ++i) {
       const double* li = L + (long long)i * N;
-      double s0 = (i == c) ? 1.0 : 0.0, s1 = 0.0;
-      int k = 0;
-      for (; k + 1 < i; k += 2) {
+      double s0 = (i == c) ? 1.0 : 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+      int k = kw;
+      for (; k + 3 < i; k += 4) {
         s0 -= li[k] * Li[(long long)k * N + cc];
         s1 -= li[k + 1] * Li[(long long)(k + 1) * N + cc];
+        s2 -= li[k + 2] * Li[(long long)(k + 2) * N + cc];
+        s3 -= li[k + 3] * Li[(long long)(k + 3) * N + cc];
       }
-      if (k < i) s0 -= li[k] * Li[(long long)k * N + cc];
-      if (c < N) Li[(long long)i * N + c] = (s0 + s1) / li[i];
+      for (; k < i; ++k) s0 -= li[k] * Li[(long long)k * N + cc];
+      if (c < N) Li[(long long)i * N + c] = ((s0 + s1) + (s2 + s3)) / li[i];
     }
   }
   __syncthreads();
@@ -1517,6 +1584,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
       const int i = I * 8 + g, jb = J * 8 + g;
       const int kend = min(N, I * 8 + 8);
       double d0 = 0.0, d1 = 0.0;
+#pragma unroll 4
       for (int k0 = 0; k0 < kend; k0 += 4) {
         const int k = k0 + t4;
         const double a = (i < N && k < N) ? Li[(long long)i * N + k] : 0.0;
@@ -1535,6 +1603,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
       const int i = I * 8 + g, jb = J * 8 + g;
       const int kend = min(N, J * 8 + 8);
       double d0 = 0.0, d1 = 0.0;
+#pragma unroll 4
       for (int k0 = 0; k0 < kend; k0 += 4) {
         const int k = k0 + t4;
         const double a = (i < N && k < N) ? U[(long long)i * N + k] : 0.0;
@@ -1629,6 +1698,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
         const double* lirow = Li + (long long)(iok ? i : 0) * N;
         const int kend = min(N, I * 8 + 8);
         double d00 = 0.0, d01 = 0.0, d10 = 0.0, d11 = 0.0;
+#pragma unroll 4
         for (int k0 = J * 8; k0 < kend; k0 += 4) {
           const int k = k0 + t4;
           const bool kin = k < N;
@@ -1806,6 +1876,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
           const bool ok0 = ib0 < nocc, ok1 = ib1 < nocc;
           double c00 = 0.0, c01 = 0.0, c10 = 0.0, c11 = 0.0;
           double d00 = 0.0, d01 = 0.0, d10 = 0.0, d11 = 0.0;
+#pragma unroll 4
           for (int k0 = 0; k0 < N; k0 += 4) {
             const int k = k0 + t4;
             const bool kin = k < N;
@@ -1907,6 +1978,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
       const int J = tile - I * (I + 1) / 2;
       const int i = I * 8 + g, jb = J * 8 + g;
       double p0 = 0.0, p1 = 0.0, q0 = 0.0, q1 = 0.0;
+#pragma unroll 4
       for (int k0 = 0; k0 < nocc; k0 += 4) {
         const int k = k0 + t4;
         const double ci = (i < N && k < nocc) ? C[(long long)i * N + k] * occ[k] : 0.0;

@@ -1,7 +1,9 @@
 """256 random molecules (2-12 atoms of H, B, C, N, O, F, Si, P, S, Cl, Br, Ti,
 Fe, Zn grown atom by atom at covalent-radius distances, charges -1/0/+1, seed
 11) in one batch against the oracle at tight convergence: |dE| <= 1e-6 Eh,
-max|dg| <= 1e-5 Eh/bohr, max|dq_shell| <= 1e-5 e, and the same status."""
+max|dg| <= 1e-5 Eh/bohr, max|dq_shell| <= 1e-5 e, and the same status.  A
+molecule with two SCC fixed points may land on either (checked against the
+oracle's fixed points under 1e-12 bohr perturbations, at most 2% of them)."""
 import os
 
 import numpy as np
@@ -53,7 +55,31 @@ def test_random_molecules_match_oracle(oracle_mod):
     assert ok.sum() >= 0.95 * len(mols)
     de = np.abs(r.energy - e)[ok]
     assert de.max() <= 1e-6
+    multistable = 0
     for m in np.nonzero(ok)[0]:
         a0, a1 = off[m], off[m + 1]
-        assert np.max(np.abs(r.gradient[a0:a1] - g[a0:a1])) <= 1e-5, m
-        assert np.max(np.abs(r.shell_charges[so[m]:so[m + 1]] - q[so[m]:so[m + 1]])) <= 1e-5, m
+        rg, rq = r.gradient[a0:a1], r.shell_charges[so[m]:so[m + 1]]
+        if np.max(np.abs(rg - g[a0:a1])) <= 1e-5 and np.max(np.abs(rq - q[so[m]:so[m + 1]])) <= 1e-5:
+            continue
+        # Some molecules have two SCC fixed points a few 1e-7 Eh apart (molecule
+        # 52: 4.5e-7 Eh, 2.9e-3 Eh/bohr), and which one the iteration reaches
+        # changes when the coordinates move by 1e-12 bohr; the device result
+        # must then equal one of the fixed points the oracle reaches.
+        sols = _oracle_solutions(oracle_mod, mols[m][0], mols[m][1], ch[m])
+        assert any(np.max(np.abs(rg - sg)) <= 1e-5 and np.max(np.abs(rq - sq)) <= 1e-5
+                   and abs(r.energy[m] - se) <= 1e-6 for se, sg, sq in sols), m
+        multistable += 1
+    assert multistable <= 0.02 * len(mols)
+
+
+def _oracle_solutions(oracle_mod, z, x, charge, trials=8):
+    off = np.array([0, len(z)], np.int32)
+    opts = oracle_mod.make_options(**TIGHT)
+    rng = np.random.default_rng(0)
+    out = []
+    for t in range(trials + 1):
+        xt = x if t == 0 else x + 1e-12 * rng.standard_normal(x.shape)
+        e, g, q, _, _, st = oracle_mod.run_batch(off, z, xt, charges=np.array([charge]), options=opts, nthreads=1)
+        if st[0] == 0:
+            out.append((e[0], g, q))
+    return out
