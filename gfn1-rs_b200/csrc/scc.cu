@@ -548,6 +548,9 @@ __device__ void tridiagonalize_blocked(double* A, int lda, int N, double* d, dou
   const int g = lane >> 2, t4 = lane & 3;
   for (int k0 = 0; k0 < N - 2; k0 += kPanel) {
     const int nbp = min(kPanel, N - 2 - k0);
+    // W of the previous column at row k, which thread 0 wrote: every thread
+    // forms it itself, so that the column needs no barrier after W is stored
+    double w_last = 0.0;
     for (int j = 0; j < nbp; ++j) {
       const int k = k0 + j, m = N - k - 1;
       // x: row k (= column k) from the diagonal, with the panel's earlier updates
@@ -555,10 +558,12 @@ __device__ void tridiagonalize_blocked(double* A, int lda, int N, double* d, dou
       for (int t = tid; t <= m; t += NT) {
         const int i = k + t;
         double x = A[(long long)k * lda + i];
+#pragma unroll 4
         for (int l = 0; l < j; ++l) {
           const double* vl = A + (long long)(k0 + l) * lda;
           const double* wl = Wp + (long long)l * N;
-          x -= vl[k] * wl[i] + wl[k] * vl[i];
+          const double wk = (l == j - 1) ? w_last : wl[k];
+          x -= vl[k] * wl[i] + wk * vl[i];
         }
         xs[t] = x;
         if (t >= 1) part += x * x;
@@ -579,6 +584,7 @@ __device__ void tridiagonalize_blocked(double* A, int lda, int N, double* d, dou
           e[k] = x0;
           tau[k] = 0.0;
         }
+        w_last = 0.0;
         __syncthreads();
         continue;
       }
@@ -644,27 +650,41 @@ __device__ void tridiagonalize_blocked(double* A, int lda, int N, double* d, dou
       }
       __syncthreads();
       // p = beta (A22 v - V (W^T v) - W (V^T v)) and p.v
+      // (at most two entries per thread: N <= 32 * kCols + 1; v kept in
+      // registers, since the next column overwrites xs without a barrier)
       double pv_part = 0.0;
-      for (int t = tid; t < m; t += NT) {
-        const int i = k + 1 + t;
-        double p = pvec[t];
-        for (int l = 0; l < j; ++l)
-          p -= A[(long long)(k0 + l) * lda + i] * sh.VtV[0][l] + Wp[(long long)l * N + i] * sh.VtV[1][l];
-        p *= beta;
-        pvec[t] = p;
-        pv_part += p * (t == 0 ? v0 : xs[1 + t]);
+      double vt[2] = {0.0, 0.0};
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int t = tid + u * NT;
+        if (t < m) {
+          const int i = k + 1 + t;
+          double p = pvec[t];
+#pragma unroll 4
+          for (int l = 0; l < j; ++l)
+            p -= A[(long long)(k0 + l) * lda + i] * sh.VtV[0][l] + Wp[(long long)l * N + i] * sh.VtV[1][l];
+          p *= beta;
+          pvec[t] = p;
+          vt[u] = t == 0 ? v0 : xs[1 + t];
+          pv_part += p * vt[u];
+        }
       }
       pv_part = warp_sum(pv_part);
       if (lane == 0) sh.red[4 + wid] = pv_part;
       __syncthreads();
       const double K = 0.5 * beta * ((sh.red[4] + sh.red[5]) + (sh.red[6] + sh.red[7]));
-      for (int t = tid; t < m; t += NT)
-        Wp[(long long)j * N + k + 1 + t] = pvec[t] - K * (t == 0 ? v0 : xs[1 + t]);
+      // each thread stores W at the rows whose x it forms in the next column
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int t = tid + u * NT;
+        if (t < m) Wp[(long long)j * N + k + 1 + t] = pvec[t] - K * vt[u];
+      }
+      w_last = pvec[0] - K * v0;
       if (tid == 0) {
         e[k] = alpha;
         tau[k] = beta;
       }
-      __syncthreads();
+      if (j == nbp - 1) __syncthreads();  // the trailing update reads all of W
     }
     // trailing matrix: A22 -= V W^T + W V^T for rows and columns >= s0, as
     // 8x8 tiles starting from A, k over the panel's columns
