@@ -250,11 +250,54 @@ __device__ void tri_factor(const double* d, const double* e, int n, double lam, 
   w[(long long)(n - 1) * ldw] = 1.0 / a;
 }
 
+// Back substitution of tri_solve from the last forward-eliminated entry
+// `cur`; returns |x|^2 of the solution.
+__device__ double tri_back(const double* w, int n, int ldw, double* x, long long stride, double cur) {
+  const long long s = (long long)n * ldw;
+  double x2 = cur * w[(long long)(n - 1) * ldw];  // x[n-1]
+  x[(n - 1) * stride] = x2;
+  double nrm = x2 * x2;
+  if (n == 1) return nrm;
+  const double* w2 = w + (long long)(n - 2) * ldw;
+  double x1 = (x[(n - 2) * stride] - w2[s] * x2) * w2[0];  // x[n-2]
+  x[(n - 2) * stride] = x1;
+  nrm += x1 * x1;
+  int k = n - 3;
+  for (; k >= 3; k -= 4) {
+    double rh[4], u1[4], u2[4], rp[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double* wk = w + (long long)(k - q) * ldw;
+      rh[q] = x[(k - q) * stride];
+      u1[q] = wk[s];
+      u2[q] = wk[2 * s];
+      rp[q] = wk[0];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double x0 = (rh[q] - u1[q] * x1 - u2[q] * x2) * rp[q];
+      x[(k - q) * stride] = x0;
+      nrm += x0 * x0;
+      x2 = x1;
+      x1 = x0;
+    }
+  }
+  for (; k >= 0; --k) {
+    const double* wk = w + (long long)k * ldw;
+    const double x0 = (x[k * stride] - wk[s] * x1 - wk[2 * s] * x2) * wk[0];
+    x[k * stride] = x0;
+    nrm += x0 * x0;
+    x2 = x1;
+    x1 = x0;
+  }
+  return nrm;
+}
+
 // Solves (T - lam I) x = b in place with the factors of tri_factor.  The
 // running entries are carried in registers and the loads of x and of the
 // factors are issued four steps ahead of their use, so the serial recurrences
-// do not wait on memory at every step.
-__device__ void tri_solve(const double* w, int n, int ldw, double* x, long long stride) {
+// do not wait on memory at every step.  Returns |x|^2 of the solution.
+__device__ double tri_solve(const double* w, int n, int ldw, double* x, long long stride) {
   const long long s = (long long)n * ldw;
   double cur = x[0];
   int k = 0;
@@ -291,38 +334,57 @@ __device__ void tri_solve(const double* w, int n, int ldw, double* x, long long 
     x[k * stride] = xk;
     cur = xk1;
   }
-  double x2 = cur * w[(long long)(n - 1) * ldw];  // x[n-1]
-  x[(n - 1) * stride] = x2;
-  if (n == 1) return;
-  const double* w2 = w + (long long)(n - 2) * ldw;
-  double x1 = (x[(n - 2) * stride] - w2[s] * x2) * w2[0];  // x[n-2]
-  x[(n - 2) * stride] = x1;
-  k = n - 3;
-  for (; k >= 3; k -= 4) {
-    double rh[4], u1[4], u2[4], rp[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const double* wk = w + (long long)(k - q) * ldw;
-      rh[q] = x[(k - q) * stride];
-      u1[q] = wk[s];
-      u2[q] = wk[2 * s];
-      rp[q] = wk[0];
+  return tri_back(w, n, ldw, x, stride, cur);
+}
+
+// tri_factor for the shift lam together with the forward elimination of the
+// right-hand side b_i = hash_unit(i, col) + 1e-3 (the start vector of inverse
+// iteration), stored in x; returns the last eliminated entry, from which
+// tri_back completes the first solve.
+__device__ double tri_factor_rhs(const double* d, const double* e, int n, double lam, double tiny, double* w,
+                                 int ldw, double* x, long long stride, unsigned col) {
+  double a = d[0] - lam;
+  double c = n > 1 ? e[0] : 0.0;
+  const long long s = (long long)n * ldw;
+  double cur = hash_unit(0, col) + 1e-3;
+  for (int k = 0; k < n - 1; ++k) {
+    const double b = e[k];
+    const double an = d[k + 1] - lam;
+    const double cn = (k + 1 < n - 1) ? e[k + 1] : 0.0;
+    double* wk = w + (long long)k * ldw;
+    double xk = cur, xk1 = hash_unit(k + 1, col) + 1e-3;
+    if (fabs(a) >= fabs(b)) {
+      double piv = a;
+      if (fabs(piv) < tiny) piv = piv >= 0.0 ? tiny : -tiny;
+      const double r = 1.0 / piv;
+      wk[0] = r;
+      wk[s] = c;
+      wk[2 * s] = 0.0;
+      wk[3 * s] = b * r;
+      wk[4 * s] = 0.0;
+      xk1 -= (b * r) * xk;
+      a = an - b * r * c;
+      c = cn;
+    } else {
+      const double r = 1.0 / b;
+      const double mult = a * r;
+      wk[0] = r;
+      wk[s] = an;
+      wk[2 * s] = cn;
+      wk[3 * s] = mult;
+      wk[4 * s] = 1.0;
+      const double t = xk;
+      xk = xk1;
+      xk1 = t - mult * xk;
+      a = c - mult * an;
+      c = -mult * cn;
     }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const double x0 = (rh[q] - u1[q] * x1 - u2[q] * x2) * rp[q];
-      x[(k - q) * stride] = x0;
-      x2 = x1;
-      x1 = x0;
-    }
+    x[k * stride] = xk;
+    cur = xk1;
   }
-  for (; k >= 0; --k) {
-    const double* wk = w + (long long)k * ldw;
-    const double x0 = (x[k * stride] - wk[s] * x1 - wk[2 * s] * x2) * wk[0];
-    x[k * stride] = x0;
-    x2 = x1;
-    x1 = x0;
-  }
+  if (fabs(a) < tiny) a = a >= 0.0 ? tiny : -tiny;
+  w[(long long)(n - 1) * ldw] = 1.0 / a;
+  return cur;
 }
 
 // ---------------------------------------------------------------- stages
@@ -1849,11 +1911,23 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
         const double pert = 10.0 * DBL_EPSILON * fmax(fabs(lam), onenrm);
         if (jj > j && lam - lam_prev < pert) lam = lam_prev + pert;
         lam_prev = lam;
-        tri_factor(d, e, N, lam, tiny, ws, N);
         double* x = Z + jj;  // column jj, stride N
+        if (jend - j == 1) {
+          // isolated: the start vector's forward elimination runs with the
+          // factorisation, the two solves are not normalised in between
+          // (growth below 1e40), and the second one returns |x|^2
+          const double cur = tri_factor_rhs(d, e, N, lam, tiny, ws, N, x, N, (unsigned)jj);
+          tri_back(ws, N, N, x, N, cur);
+          const double nrm = tri_solve(ws, N, N, x, N);
+          const double inv = 1.0 / sqrt(fmax(nrm, 1e-300));
+#pragma unroll 8
+          for (int i = 0; i < N; ++i) x[(long long)i * N] *= inv;
+          continue;
+        }
+        tri_factor(d, e, N, lam, tiny, ws, N);
 #pragma unroll 4
         for (int i = 0; i < N; ++i) x[(long long)i * N] = hash_unit(i, jj) + 1e-3;
-        const int nit = (jend - j > 1) ? 4 : 2;
+        const int nit = 4;
         for (int it = 0; it < nit; ++it) {
           tri_solve(ws, N, N, x, N);
           for (int q = j; q < jj; ++q) {  // modified Gram-Schmidt inside the cluster
