@@ -1227,7 +1227,7 @@ __device__ void stage_potential(const Batch& B, const Model& M, const MolCtx& c,
   __syncthreads();
   for (int i = tid; i < nsh; i += NT) {
     double v = 0.0;
-    for (int j = 0; j < nsh; ++j) v += G[(long long)i * nsh + j] * w.qin[j];
+    for (int j = 0; j < nsh; ++j) v += G[(long long)j * nsh + i] * w.qin[j];  // G symmetric: coalesced column
     const int a = sh_atom[i];
     const double qa = w.qat[a];
     v += qa * qa * M.elem[B.z[a0 + a]].gam3;
@@ -1268,7 +1268,7 @@ __device__ void stage_charges_energy(const Batch& B, const Model& M, const MolCt
   double p2 = 0.0, p3 = 0.0, pr = 0.0;
   for (int i = tid; i < nsh; i += NT) {
     double v = 0.0;
-    for (int j = 0; j < nsh; ++j) v += G[(long long)i * nsh + j] * w.qout[j];
+    for (int j = 0; j < nsh; ++j) v += G[(long long)j * nsh + i] * w.qout[j];  // G symmetric: coalesced column
     p2 += w.qout[i] * v;
     const int a = sh_atom[i];
     const double qa = w.qat[a];

@@ -246,7 +246,8 @@ __global__ void __launch_bounds__(128, 4) setup_kernel(Batch B, Model M, int ena
     }
   }
 
-  // ---- Klopman-Ohno matrix
+  // ---- Klopman-Ohno matrix (exactly symmetric: G_ij and G_ji come from the
+  // same commutative expression, which the SCC's column reads rely on)
   double* G = B.gam + B.gam_off[m];
   for (long long w = tid + (long long)split * nt; w < (long long)nsh * nsh; w += (long long)nt * nsplit) {
     const int i = (int)(w / nsh), j = (int)(w % nsh);

@@ -1243,7 +1243,7 @@ __global__ void __launch_bounds__(kWideNT, 1) wide_fermi_kernel(WideCtx X) {
 }
 
 // (6) inverse iteration for the occupied eigenvectors of the tridiagonal (one
-// thread per cluster of eigenvalues closer than 1e-5 |T|_1, modified
+// thread per cluster of eigenvalues closer than ortol_rel |T|_1, modified
 // Gram-Schmidt inside a cluster), columns of Z with stride ld.
 __global__ void __launch_bounds__(64) wide_inviter_kernel(WideCtx X, double ortol_rel, int* stats) {
   const WideMol& w = X.mols[X.act[blockIdx.y]];
@@ -1271,11 +1271,23 @@ __global__ void __launch_bounds__(64) wide_inviter_kernel(WideCtx X, double orto
     const double pert = 10.0 * DBL_EPSILON * fmax(fabs(lam), onenrm);
     if (jj > j && lam - lam_prev < pert) lam = lam_prev + pert;
     lam_prev = lam;
-    tri_factor(w.d, w.e, N, lam, tiny, wsv, ld);
     double* x = Z + jj;
+    if (jend - j == 1) {
+      // isolated: the start vector's forward elimination runs with the
+      // factorisation, the two solves are not normalised in between (growth
+      // below 1e40), and the second one returns |x|^2
+      const double cur = tri_factor_rhs(w.d, w.e, N, lam, tiny, wsv, ld, x, ld, (unsigned)jj);
+      tri_back(wsv, N, ld, x, ld, cur);
+      const double nrm = tri_solve(wsv, N, ld, x, ld);
+      const double inv = 1.0 / sqrt(fmax(nrm, 1e-300));
+#pragma unroll 8
+      for (int i = 0; i < N; ++i) x[(long long)i * ld] *= inv;
+      continue;
+    }
+    tri_factor(w.d, w.e, N, lam, tiny, wsv, ld);
 #pragma unroll 8
     for (int i = 0; i < N; ++i) x[(long long)i * ld] = hash_unit(i, jj) + 1e-3;
-    const int nit = (jend - j > 1) ? 4 : 2;
+    const int nit = 4;
     for (int it = 0; it < nit; ++it) {
       tri_solve(wsv, N, ld, x, ld);
       for (int q = j; q < jj; ++q) {
