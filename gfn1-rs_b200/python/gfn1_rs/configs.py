@@ -49,13 +49,15 @@ def main():
     ap.add_argument("--frames", type=int, default=256)
     ap.add_argument("--batch", type=int, default=64)
     ap.add_argument("--only", choices=("all", "single", "trajectory", "hessian"), default="all")
+    ap.add_argument("--modes", default=",".join(trajectory.MODES),
+                    help="comma-separated starting-guess modes of the trajectory (the first is the dE reference)")
     a = ap.parse_args()
     if a.only in ("all", "hessian"):
         hessians(256)
     if a.only in ("all", "single"):
         singles()
     if a.only in ("all", "trajectory"):
-        trajectories(a.frames, a.batch)
+        trajectories(a.frames, a.batch, tuple(m for m in a.modes.split(",") if m))
 
 
 def hessians(nmol: int):
@@ -84,12 +86,12 @@ def singles():
                           "abs_dE": abs(plain["energy"] - learned["energy"])}), flush=True)
 
 
-def trajectories(frames: int, batch: int):
+def trajectories(frames: int, batch: int, modes=trajectory.MODES):
     z, x = workloads.water_trajectory(96, frames=frames)
     xb = x * ANGSTROM_TO_BOHR
     calc = BatchCalculator()
     ref = None
-    for mode in trajectory.MODES:
+    for mode in modes:
         trajectory.run_trajectory(z, xb[:batch], batch=batch, mode=mode, calc=calc)  # warm-up
         r = trajectory.run_trajectory(z, xb, batch=batch, mode=mode, calc=calc)
         ref = ref or r
