@@ -531,8 +531,9 @@ struct TridiagSmall {
   double ajj;  // A[j][j] as of the panel start (CTA 0)
 };
 
-// Rows per CTA the cache holds for panel width nb.
-__host__ __device__ inline int tridiag_rows_cap(int nb) { return kPanelCache / (2 * nb + 1); }
+// Rows per CTA the cache holds for panel width nb: x, V and W of each row,
+// with room left to stage one CTA's 2 nb partial sums.
+__host__ __device__ inline int tridiag_rows_cap(int nb) { return (kPanelCache - 2 * nb) / (2 * nb + 1); }
 
 __host__ __device__ inline size_t tridiag_smem_bytes(int maxn) {
   return sizeof(double) * ((size_t)maxn + 8 + kPanelCache) + kTileSmemBytes;
@@ -541,6 +542,16 @@ __host__ __device__ inline size_t tridiag_smem_bytes(int maxn) {
 __host__ __device__ inline int tridiag_min_group(int N, int nb) {
   const int cap = tridiag_rows_cap(nb);
   return (N - 1 + cap - 1) / cap;
+}
+// CTAs of a group of G that share a panel's nr trailing rows: about
+// nr / min_rows of them, but never so few that one gets more rows than its
+// cache holds (nr / min_rows rounds down, which alone would leave a CTA up to
+// 2 min_rows - 1 rows), and at most G.
+__host__ __device__ inline int tridiag_active(int nr, int G, int min_rows, int nb) {
+  const int cap = tridiag_rows_cap(nb);
+  const int need = (nr + cap - 1) / cap;
+  const int want = nr / min_rows > need ? nr / min_rows : need;
+  return want < 1 ? 1 : (want < G ? want : G);
 }
 
 __global__ void __launch_bounds__(kRedNT) wide_tridiag_kernel(WideCtx X, int G, int nb, int min_rows,
@@ -575,8 +586,8 @@ __global__ void __launch_bounds__(kRedNT) wide_tridiag_kernel(WideCtx X, int G, 
       tclk = t;
     }
   };
-  {  // the first panel has the most rows per CTA; the host sizes G so that they fit the cache
-    const int nr0 = N - 1, ga0 = max(1, min(G, nr0 / min_rows));
+  {  // the first panel needs the most CTAs to fit its rows; the host sizes G for it
+    const int nr0 = N - 1, ga0 = tridiag_active(nr0, G, min_rows, nb);
     if ((nr0 + ga0 - 1) / ga0 > tridiag_rows_cap(nb)) {
       if (tid == 0 && c == 0) w.st->status = kErrInvalidInput;
       return;
@@ -586,10 +597,10 @@ __global__ void __launch_bounds__(kRedNT) wide_tridiag_kernel(WideCtx X, int G, 
   for (int k0 = 0; k0 < N - 2 && ok; k0 += nb) {
     const int nbc = min(nb, N - 2 - k0);
     const int nr = N - k0 - 1;
-    const int Ga = max(1, min(G, nr / min_rows));
+    const int Ga = tridiag_active(nr, G, min_rows, nb);
     const bool active = c < Ga;
     const int r0 = k0 + 1 + (int)(((long long)nr * c) / Ga), r1 = k0 + 1 + (int)(((long long)nr * (c + 1)) / Ga);
-    const int R = r1 - r0;  // at most tridiag_rows_cap(nb) (checked above)
+    const int R = r1 - r0;  // at most tridiag_rows_cap(nb): Ga >= nr / cap, and G fits the first panel
     double* xs = cache;              // x of the CTA's rows
     double* Vc = cache + R;          // Vc[l * R + (i - r0)]: panel reflectors of the CTA's rows
     double* Wc = Vc + (size_t)nb * R;  // Wc[l * R + (i - r0)]: p of the CTA's rows (w = p + alpha v)
@@ -1774,7 +1785,7 @@ __global__ void wide_copy_hp_kernel(WideCtx X) {  // A = H0' (a realistic matrix
 static cudaError_t wide_autotune(const WideCtx& X, int na, int capacity, int gcap, size_t smem, int maxn,
                                  cudaStream_t st, WidePlan& plan) {
   const int nbs[] = {8, 16, 32};
-  const int mrs[] = {4, 8, 16, 32};
+  const int mrs[] = {4, 8, 16, 32, 64, 128};
   cudaEvent_t e0, e1;
   cudaError_t e = cudaEventCreate(&e0);
   if (e == cudaSuccess) e = cudaEventCreate(&e1);

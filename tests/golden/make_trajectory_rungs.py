@@ -8,8 +8,11 @@ the fallback-ladder rung that converged (src/electronic.rs:1390-1447), the
 iterations of that rung, the energy and the electronic temperature used.  The
 frames drift apart (no forces), so later frames need more SCC iterations; the
 record shows which rung the reference's ladder settles on for them.
+Frame 64 also carries a tightly converged record ("tight": 1e-10 Eh, 1e-8
+e; energy, gradient, iterations), against which the device is held to the
+parity bar.
 Run: python tests/golden/make_trajectory_rungs.py (CPU only; one thread per
-frame, about ten minutes).
+frame, about ten minutes); --tight-only recomputes only the tight record.
 """
 import json
 import os
@@ -29,6 +32,8 @@ from gfn1_rs import workloads  # noqa: E402
 
 A2B = 1.8897261246257702
 FRAMES = (64, 128, 192, 255)
+TIGHT_FRAME = 64
+TIGHT = dict(energy_tolerance=1e-10, charge_tolerance=1e-8)
 
 
 def record(z, x_ang):
@@ -39,14 +44,31 @@ def record(z, x_ang):
             "electronic_temperature": o.electronic_temperature, "seconds": round(time.time() - t0, 1)}
 
 
+def tight_record(z, x_ang):
+    t0 = time.time()
+    o = oracle.run(z, x_ang * A2B, options=oracle.make_options(**TIGHT))
+    return {"energy": o.energy, "gradient": np.asarray(o.gradient).round(14).tolist(),
+            "iterations": int(o.iterations), "rung": int(o.rung), "options": TIGHT,
+            "seconds": round(time.time() - t0, 1)}
+
+
 def main():
     z, x = workloads.water_trajectory(96, frames=max(FRAMES) + 1)
     oracle.lib()
-    with ThreadPoolExecutor(len(FRAMES)) as ex:
-        recs = list(ex.map(lambda f: record(z, x[f]), FRAMES))
-    out = {"numbers": [int(v) for v in z], "frames": dict(zip((str(f) for f in FRAMES), recs))}
-    print({f: (r["rung"], r["iterations"], r["seconds"]) for f, r in out["frames"].items()}, flush=True)
-    with open(os.path.join(HERE, "trajectory_rungs.json"), "w") as f:
+    path = os.path.join(HERE, "trajectory_rungs.json")
+    if "--tight-only" in sys.argv:
+        with open(path) as fh:
+            out = json.load(fh)
+    else:
+        with ThreadPoolExecutor(len(FRAMES)) as ex:
+            recs = list(ex.map(lambda f: record(z, x[f]), FRAMES))
+        out = {"numbers": [int(v) for v in z], "frames": dict(zip((str(f) for f in FRAMES), recs))}
+        print({f: (r["rung"], r["iterations"], r["seconds"]) for f, r in out["frames"].items()}, flush=True)
+    # from the stored (rounded) positions, the ones the device test reads
+    fr = out["frames"][str(TIGHT_FRAME)]
+    fr["tight"] = tight_record(z, np.array(fr["positions_angstrom"]))
+    print("tight", {k: v for k, v in out["frames"][str(TIGHT_FRAME)]["tight"].items() if k != "gradient"}, flush=True)
+    with open(path, "w") as f:
         json.dump(out, f)
 
 

@@ -36,24 +36,28 @@ def test_trajectory_modes_agree_and_save_iterations(gpu_calc):
 
 
 def test_late_frames_rungs_match_oracle(gpu_calc):
-    """Frame 64 of the 96-water trajectory at the default options (the
-    trajectory workload's), against tests/golden/trajectory_rungs.json: same
-    rung and, since both stop at the default thresholds (1e-6 Eh, 2e-5 e)
-    rather than at a tight fixed point, energies within 1e-5 Eh.  The later
-    frames of the fixture need 139-170 iterations of a 768-AO SCC on one SM
-    (over a minute each); the trajectory workload reports their rungs."""
+    """Frame 64 of the 96-water trajectory (768 AOs, the many-SM path) against
+    tests/golden/trajectory_rungs.json.  At the default options (the
+    trajectory workload's): the same fallback-ladder rung, and energies within
+    1e-5 Eh, since both stop at the default thresholds (1e-6 Eh, 2e-5 e)
+    rather than at a fixed point.  Converged tightly (1e-10 Eh, 1e-8 e) on
+    both sides: the parity bar, |dE| <= 1e-6 Eh and max|dg| <= 1e-5 Eh/bohr."""
     from gfn1_rs import BatchCalculator, trajectory
     with open(os.path.join(ROOT, "tests", "golden", "trajectory_rungs.json")) as fh:
         rec = json.load(fh)
     z = np.array(rec["numbers"])
-    keys = ["64"]
-    frames = [rec["frames"][k] for k in keys]
-    x = np.concatenate([np.array(f["positions_angstrom"]) * A2B for f in frames])
-    off = (np.arange(len(keys) + 1) * len(z)).astype(np.int32)
-    r = BatchCalculator().calculate_flat(off, np.tile(z, len(keys)), x, compute_gradient=False)
-    for i, f in enumerate(frames):
-        assert r.status[i] == 0, keys[i]
-        assert r.rung[i] == f["rung"], keys[i]
-        assert abs(r.energy[i] - f["energy"]) <= 1e-5, keys[i]
-    print("rungs", trajectory.rung_usage(r.rung), "iterations", r.iterations.tolist(),
-          "oracle", [f["iterations"] for f in frames])
+    f = rec["frames"]["64"]
+    x = np.array(f["positions_angstrom"]) * A2B
+    off = np.array([0, len(z)], np.int32)
+    r = BatchCalculator().calculate_flat(off, z, x, compute_gradient=False)
+    assert r.status[0] == 0
+    assert r.rung[0] == f["rung"]
+    assert abs(r.energy[0] - f["energy"]) <= 1e-5
+    print("rungs", trajectory.rung_usage(r.rung), "iterations", r.iterations.tolist(), "oracle", f["iterations"])
+    t = f["tight"]
+    rt = BatchCalculator(**t["options"]).calculate_flat(off, z, x)
+    assert rt.status[0] == 0 and rt.rung[0] == t["rung"]
+    de = abs(rt.energy[0] - t["energy"])
+    dg = np.abs(rt.gradient - np.array(t["gradient"])).max()
+    print(f"tight: dE {de:.2e} dg {dg:.2e} iterations {rt.iterations[0]} vs {t['iterations']}")
+    assert de <= 1e-6 and dg <= 1e-5
