@@ -77,7 +77,7 @@ class BatchCalculator:
         the packaged trained network, or a path to a parameter file.
         spin_multiplicity: None (the reference's default) or n >= 1 for every
         molecule of a call (spin-constrained occupations).  level_shift: the
-        reference's virtual level shift (Eh), molecules up to 1024 AOs."""
+        reference's virtual level shift (Eh), molecules of every size."""
         self.engine = _lib.Engine(param_path, device)
         self.guess = None
         if learned_guess:

@@ -53,7 +53,7 @@ typedef struct gfn1_options {
                                     (src/electronic.rs:159), spin-constrained occupations
                                     in restricted orbitals (src/electronic.rs:3930-4045) */
   double level_shift;            /* 0 Eh: ElectronicOptions::level_shift (src/electronic.rs:1413-1416,
-                                    2125-2137), up to 1024 AOs */
+                                    2125-2137), molecules of every size */
 } gfn1_options;
 
 /* Per-batch outputs; any pointer may be NULL.  For gfn1_batch_download the
@@ -113,10 +113,10 @@ int gfn1_batch_energy_gradient(gfn1_engine* eng, int nmol, const int32_t* atom_o
  * P = density, W = energy_weighted_density (N x N, row-major, AO order of
  * BasisSet::build) and orbital_energies / occupations (N).  P, W, the
  * eigenvalues and occupations are those of the last diagonalisation.  The
- * one-SM-per-molecule path solves only for the eigenvalues its occupations
- * need (the lowest ceil(nel/2)+8, the whole spectrum when the Fermi
- * distribution reaches further, and the highest); the others are NaN.  Above
- * 1024 AOs the full spectrum is returned.  Any pointer may be NULL. */
+ * eigensolver solves only for the eigenvalues the occupations need (the
+ * lowest ceil(nel/2)+8, the whole spectrum when the Fermi distribution
+ * reaches further, and the highest); the others are NaN.  Any pointer may be
+ * NULL. */
 int gfn1_last_molecule_matrices(gfn1_engine* eng, int m, double* S, double* H0, double* P, double* W, double* eps,
                                 double* occ);
 
