@@ -55,6 +55,33 @@ def test_batched_hessians_match_oracle(gpu_calc, oracle_mod, fixtures):
         assert np.max(np.abs(wg[big] - wo[big])) <= 0.05, m
 
 
+def test_five_point_hessian_matches_oracle(gpu_calc, oracle_mod, fixtures):
+    """order=4 (five-point stencil, h = 1e-2 bohr) on water and ammonia against
+    the same stencil over the oracle's gradient, and against the central
+    differences: the two stencils differ by the O(h^2) truncation only."""
+    from gfn1_rs import hessian as hs
+
+    mols = _molecules(fixtures)[:1] + _molecules(fixtures)[3:4]
+    off = np.concatenate([[0], np.cumsum([len(z) for z, _ in mols])]).astype(np.int32)
+    z = np.concatenate([z for z, _ in mols])
+    x = np.concatenate([x for _, x in mols])
+    out4 = hs.hessian_batch(gpu_calc, off, z, x, order=4)
+    out2 = hs.hessian_batch(gpu_calc, off, z, x)
+    assert np.all(out4["status"] == 0) and out4["order"] == 4
+    opt = oracle_mod.make_options(**TIGHT)
+
+    def evaluate(items):
+        return [(r.converged, r.gradient) for r in
+                (oracle_mod.run(zi, xi, options=opt, init_shell_charges=q) for _, zi, xi, q in items)]
+
+    for m, (zm, xm) in enumerate(mols):
+        r0 = oracle_mod.run(zm, xm, options=opt)
+        (ho,), _ = hs.hessian(evaluate, [(zm, xm, r0.shell_charges)], order=4)
+        h4, h2 = out4["hessians"][m], out2["hessians"][m]
+        assert np.max(np.abs(h4 - ho)) <= 1e-5, m
+        assert np.max(np.abs(h4 - h2)) <= 1e-3 * np.max(np.abs(h4)), m
+
+
 def test_ase_hessian_units(gpu_calc, fixtures):
     from gfn1_rs import hessian as hs
     from gfn1_rs.ase import _BOHR, _HARTREE, _INVCM_EV, GFN1RSCalculator

@@ -3,7 +3,8 @@
 * vibrational_analysis against the reference's own unit tests
   (src/vibrational.rs:86-129): a single harmonic H oscillator and the five
   zero modes of a two-atom Hessian with one bond constant;
-* the central-difference assembly is exact for a quadratic energy;
+* the central-difference assembly is exact for a quadratic energy, the
+  five-point stencil for a quartic one;
 * the batched driver with the oracle as the gradient source on water:
   symmetric, translation sum rule, diagonal elements equal to the second
   difference of the energy.
@@ -58,6 +59,29 @@ def test_assembly_is_exact_for_a_quadratic_energy():
     out, calls = hs.hessian(evaluate, [([1] * nat, x0, None)], step=1e-2, chunk=5)
     assert calls == (6 * nat + 4) // 5
     assert np.max(np.abs(out[0] - a)) < 1e-11
+
+
+def test_five_point_stencil_is_exact_for_a_quartic_energy():
+    """g = a x + b x^3 (a quartic energy): central differences miss the
+    Hessian a + diag(3 b x^2) by h^2 b, the five-point stencil is exact."""
+    rng = np.random.default_rng(5)
+    nat = 3
+    a = rng.normal(size=(3 * nat, 3 * nat))
+    a = a + a.T
+    b = rng.uniform(0.5, 1.5, size=3 * nat)
+    x0 = rng.normal(size=(nat, 3))
+    exact = a + np.diag(3.0 * b * x0.ravel() ** 2)
+
+    def evaluate(items):
+        return [(True, (a @ x.ravel() + b * x.ravel() ** 3).reshape(-1, 3)) for _, _, x, _ in items]
+
+    (h2,), _ = hs.hessian(evaluate, [([1] * nat, x0, None)], step=1e-2)
+    (h4,), calls = hs.hessian(evaluate, [([1] * nat, x0, None)], step=1e-2, order=4, chunk=7)
+    assert calls == (12 * nat + 6) // 7
+    assert np.max(np.abs(h4 - exact)) < 1e-10
+    assert np.max(np.abs(np.diag(h2 - exact) - b * 1e-4)) < 1e-10
+    with pytest.raises(ValueError):
+        hs.displacements(nat, 1e-2, order=3)
 
 
 def test_failed_displacement_marks_the_molecule():
