@@ -6,7 +6,8 @@
 // four CTAs per SM; shared memory holds the index tables and N-vectors, and the
 // eigensolver's working matrix lives in the CTA's global workspace slot, cached
 // by L1.  Up to 193 AOs the Householder reduction is blocked (8-column panels,
-// tensor-core trailing updates).  Wider CTAs (256/512 threads) and a working
+// tensor-core trailing updates); the prologue's Cholesky is left-looking over
+// 8-column panels.  Wider CTAs (256/512 threads) and a working
 // matrix in shared memory are used only by the allocation-free single-molecule
 // entry point, which passes the room for it in the launch's shared memory.
 //
@@ -18,8 +19,9 @@
 //    the potential term  -1/2 (M + M^T),  M = L^-1 diag(v) L  (lower triangular),
 //    because  L^-1 (S o V) L^-T = L^-1 diag(v) L + (L^-1 diag(v) L)^T  for
 //    V_mu,nu = v_mu + v_nu (src/electronic.rs:3133-3158).
-//  * eigensolver: Householder tridiagonalisation (two barriers per column),
-//    Sturm-sequence multisection for the eigenvalues the occupations need,
+//  * eigensolver: Householder tridiagonalisation (three barriers per column in
+//    the blocked form), Sturm counts plus Laguerre steps, warm-started from
+//    the previous iteration, for the eigenvalues the occupations need,
 //    inverse iteration (with modified Gram-Schmidt inside eigenvalue clusters)
 //    for the occupied eigenvectors only, and a blocked (compact-WY)
 //    back-transformation (replaces faer's self_adjoint_eigen, src/linalg.rs:153-191).
