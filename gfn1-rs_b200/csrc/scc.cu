@@ -600,7 +600,8 @@ __device__ void tridiagonalize(double* A, int lda, int N, double* d, double* e, 
 // updates (x), its reflector (stored in row k as before), p = beta (A22 v -
 // V (W^T v) - W (V^T v)) with A22 as of the panel start, and w = p - K v kept
 // in Wp (kPanel x N, row l for the panel's column l).  V is read from the
-// reflector rows of A.  xs and pvec are N-vectors of scratch.
+// reflector rows of A.  xs and pvec are N-vectors of scratch.  A is the
+// global working matrix (32-byte aligned, lda a multiple of four).
 constexpr int kPanel = 8;
 template <int NT>
 __device__ void tridiagonalize_blocked(double* A, int lda, int N, double* d, double* e, double* tau, double* pvec,
@@ -669,29 +670,45 @@ __device__ void tridiagonalize_blocked(double* A, int lda, int N, double* d, dou
           if (jj < m) A[(long long)k * lda + k + 1 + jj] = vreg[c];
         }
       }
-      // raw A22 v, one thread per entry: A22 is kept symmetric, so entry t is
-      // column t of A22 dotted with v, and each row of A22 read across the
-      // threads is contiguous (no cross-lane sums); v from shared memory
-      const double* a22 = A + (long long)(k + 1) * lda + (k + 1);
-      for (int t = tid; t < m; t += NT) {
-        const double* col = a22 + t;
-        double s0 = col[0] * v0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-        int r = 1;
-        for (; r + 7 < m; r += 8) {  // eight loads in flight per thread
-          double a[8];
+      // raw A22 v: A22 is kept symmetric, so entry t is column t of A22
+      // dotted with v, and each row of A22 read across the threads is
+      // contiguous (no cross-lane sums); v from shared memory.  Each thread
+      // takes two adjacent columns with 16-byte loads: the pair of absolute
+      // columns (c, c + 1), c even, so that every load is aligned (A starts on
+      // 32 bytes, lda is a multiple of four); a pair may reach column k (left
+      // of A22) or column N (the row's padding), whose sums are dropped.  Per
+      // column, two partial sums over odd and even rows, eight rows in
+      // flight.
+      {
+        const int u0 = (k + 1) >> 1, np = ((N - 1) >> 1) - u0 + 1, ld2 = lda >> 1;
+        const double2* rowk = reinterpret_cast<const double2*>(A + (long long)(k + 1) * lda) + u0;
+        for (int p = tid; p < np; p += NT) {
+          const double2* col = rowk + p;
+          const double2 a0 = col[0];
+          double s0 = a0.x * v0, s1 = 0.0, q0 = a0.y * v0, q1 = 0.0;
+          int r = 1;
+          for (; r + 7 < m; r += 8) {
+            double2 a[8];
 #pragma unroll
-          for (int u = 0; u < 8; ++u) a[u] = col[(long long)(r + u) * lda];
-          s0 += a[0] * xs[1 + r];
-          s1 += a[1] * xs[2 + r];
-          s2 += a[2] * xs[3 + r];
-          s3 += a[3] * xs[4 + r];
-          s0 += a[4] * xs[5 + r];
-          s1 += a[5] * xs[6 + r];
-          s2 += a[6] * xs[7 + r];
-          s3 += a[7] * xs[8 + r];
+            for (int u = 0; u < 8; ++u) a[u] = col[(long long)(r + u) * ld2];
+#pragma unroll
+            for (int u = 0; u < 8; u += 2) {
+              const double xa = xs[1 + r + u], xb = xs[2 + r + u];
+              s0 += a[u].x * xa;
+              q0 += a[u].y * xa;
+              s1 += a[u + 1].x * xb;
+              q1 += a[u + 1].y * xb;
+            }
+          }
+          for (; r < m; ++r) {
+            const double2 a = col[(long long)r * ld2];
+            s0 += a.x * xs[1 + r];
+            q0 += a.y * xs[1 + r];
+          }
+          const int t = 2 * (u0 + p) - (k + 1);  // A22 index of the pair's first column
+          if (t >= 0) pvec[t] = s0 + s1;
+          if (t + 1 < m) pvec[t + 1] = q0 + q1;
         }
-        for (; r < m; ++r) s0 += col[(long long)r * lda] * xs[1 + r];
-        pvec[t] = (s0 + s1) + (s2 + s3);
       }
       for (int l = wid; l < j; l += NW) {
         const double* vl = A + (long long)(k0 + l) * lda + (k + 1);
@@ -1827,7 +1844,7 @@ __device__ void scc_molecule(const Batch& B, const Model& M, const SccOptions& o
     clk.mark(kStFock);
     // (3) Householder tridiagonalisation
     if constexpr (NT == 128) {
-      if (N <= 32 * 6 + 1)  // e^2 is formed after the reduction, so its slot is the reduction's scratch
+      if (N <= 32 * 6 + 1 && !a_shared)  // e^2 is formed after the reduction, so its slot is the reduction's scratch
         tridiagonalize_blocked<NT>(A, lda, N, d, e, tau, pvec, esq, w.W1, sh);
       else
         tridiagonalize<NT>(A, lda, N, d, e, tau, pvec, sh);
