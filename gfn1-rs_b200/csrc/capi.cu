@@ -305,6 +305,19 @@ struct gfn1_batch {
   int n_shift = 0;
   std::string host_err;   // message of the first molecule the host validation rejected
   int host_err_mol = -1;  // that molecule, or -1
+  // inputs of the last prepare() that gfn1_batch_energy_gradient ran on this
+  // batch; a call with the same topology, charges, options, large-molecule
+  // threshold and learned guess reuses its layout and only stages the new
+  // coordinates (prepare() clears it)
+  struct TopologyKey {
+    bool valid = false;
+    std::vector<int32_t> atom_offsets;
+    std::vector<uint8_t> z;
+    std::vector<double> charge;  // empty: no charges given
+    gfn1_options opt;
+    int dense_n = 0;
+    gfn1_guess* guess = nullptr;
+  } last_topology;
   gfn1_guess* guess = nullptr;       // learned guess used when no initial charges are set
   DevBuf<float> gx, gy;              // guess features [natoms x 100] and outputs [natoms x 2]
   DevBuf<double> gq;                 // guessed initial shell charges [nshells]
@@ -629,9 +642,19 @@ namespace {
 // Fills the topology part of a batch (sizes, offsets, order, element check,
 // electron count) into the pinned input blob and grows every buffer.  Buffers
 // are never shrunk, so a reused batch allocates only when a larger batch comes.
+// Molecules above this many AOs run on groups of SMs (wide.cuh); GFN1_DENSE_N
+// overrides the default of 256.
+int dense_threshold() {
+  int n = 256;
+  if (const char* dn = std::getenv("GFN1_DENSE_N"))
+    if (*dn) n = std::max(2, std::atoi(dn));
+  return n;
+}
+
 int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t* z, const double* charge,
             const gfn1_options* opt, std::string& first_err, int& worst) {
   gfn1_engine* eng = b->eng;
+  b->last_topology.valid = false;
   gfn1_options o;
   if (opt) o = *opt;
   else fill_default(&o);
@@ -785,9 +808,7 @@ int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t*
   // above kDenseN AOs one SM per molecule is too slow: those molecules run on
   // groups of SMs (wide.cuh).  GFN1_DENSE_N overrides the threshold (the tests
   // use it to run both paths on the same molecules).
-  int kDenseN = 256;
-  if (const char* dn = std::getenv("GFN1_DENSE_N"))
-    if (*dn) kDenseN = std::max(2, std::atoi(dn));
+  const int kDenseN = dense_threshold();
   constexpr int kWideMaxN = 8192;  // the reduction keeps two N-vectors per CTA in shared memory
   int n_dense = 0;
   while (n_dense < nmol && n_m[h_order[n_dense]] > kDenseN) ++n_dense;
@@ -1105,6 +1126,51 @@ bool finite_all_f(const float* x, long long n) {
   return true;
 }
 
+bool same_bits(double x, double y) { return std::memcmp(&x, &y, sizeof(double)) == 0; }
+
+bool same_options(const gfn1_options& a, const gfn1_options& b) {
+  return a.max_scc == b.max_scc && same_bits(a.energy_tolerance, b.energy_tolerance) &&
+         same_bits(a.charge_tolerance, b.charge_tolerance) && same_bits(a.mixing, b.mixing) &&
+         a.scc_broyden == b.scc_broyden && a.scc_broyden_size == b.scc_broyden_size &&
+         same_bits(a.electronic_temperature, b.electronic_temperature) &&
+         a.enable_dispersion == b.enable_dispersion && a.compute_gradient == b.compute_gradient &&
+         a.spin_multiplicity == b.spin_multiplicity && same_bits(a.level_shift, b.level_shift);
+}
+
+// Whether a call's topology, charges and options equal those of the last
+// prepare() on the one-shot batch (and the large-molecule threshold and the
+// engine's learned guess are unchanged), so that its layout, processing order,
+// size classes and validated statuses still hold.  Values compare bitwise.
+bool same_topology(const gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t* z, const double* charge,
+                   const gfn1_options* opt) {
+  const gfn1_batch::TopologyKey& k = b->last_topology;
+  if (!k.valid || nmol != b->nmol || (int)k.atom_offsets.size() != nmol + 1) return false;
+  if (std::memcmp(k.atom_offsets.data(), atom_offsets, sizeof(int32_t) * (nmol + 1)) != 0) return false;
+  const size_t natoms = (size_t)atom_offsets[nmol];
+  if (k.z.size() != natoms || (natoms && std::memcmp(k.z.data(), z, natoms) != 0)) return false;
+  if (charge ? (k.charge.size() != (size_t)nmol || std::memcmp(k.charge.data(), charge, sizeof(double) * nmol) != 0)
+             : !k.charge.empty())
+    return false;
+  gfn1_options o;
+  if (opt) o = *opt;
+  else fill_default(&o);
+  return same_options(o, k.opt) && k.dense_n == dense_threshold() && k.guess == b->eng->guess;
+}
+
+void remember_topology(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t* z, const double* charge,
+                       const gfn1_options* opt) {
+  gfn1_batch::TopologyKey& k = b->last_topology;
+  k.atom_offsets.assign(atom_offsets, atom_offsets + nmol + 1);
+  k.z.assign(z, z + atom_offsets[nmol]);
+  if (charge) k.charge.assign(charge, charge + nmol);
+  else k.charge.clear();
+  if (opt) k.opt = *opt;
+  else fill_default(&k.opt);
+  k.dense_n = dense_threshold();
+  k.guess = b->eng->guess;
+  k.valid = true;
+}
+
 }  // namespace
 
 // ============================================================== C ABI
@@ -1336,10 +1402,16 @@ int gfn1_batch_energy_gradient(gfn1_engine* eng, int nmol, const int32_t* atom_o
   gfn1_batch* b = eng->oneshot;
   const char* prof = std::getenv("GFN1_PROFILE");
   b->profiling = prof && *prof && *prof != '0';
-  std::string first_err;
-  int worst = GFN1_OK;
-  int rc = prepare(b, nmol, atom_offsets, z, charge, opt, first_err, worst);
-  if (rc != GFN1_OK) return rc;
+  int rc = GFN1_OK;
+  if (same_topology(b, nmol, atom_offsets, z, charge, opt)) {
+    b->has_init_q = false;  // everything else prepare() sets depends only on the key
+  } else {
+    std::string first_err;
+    int worst = GFN1_OK;
+    rc = prepare(b, nmol, atom_offsets, z, charge, opt, first_err, worst);
+    if (rc != GFN1_OK) return rc;
+    remember_topology(b, nmol, atom_offsets, z, charge, opt);
+  }
   if (!finite_all(xyz_bohr, 3 * b->natoms)) return fail(eng, GFN1_E_NAN, "non-finite coordinate");
   std::memcpy(b->hin<double>(b->lay.xyz), xyz_bohr, sizeof(double) * 3 * b->natoms);
   if (init_shell_q) {

@@ -90,6 +90,7 @@ class BatchCalculator:
                          enable_dispersion=int(bool(enable_dispersion)),
                          spin_multiplicity=int(spin_multiplicity or 0), level_shift=float(level_shift))
         self._last = None  # (atom_offsets, numbers) of the last calculate_flat call
+        self._last_shoff = None  # its shell offsets (read-only), reused while the topology repeats
 
     def shell_offsets(self, atom_offsets, numbers) -> np.ndarray:
         """Prefix sums of the shell counts, laid out as the C side does (atoms of
@@ -115,7 +116,14 @@ class BatchCalculator:
         z = np.ascontiguousarray(numbers, dtype=np.uint8)
         xyz = np.ascontiguousarray(xyz_bohr, dtype=np.float64).reshape(-1, 3)
         nmol, natoms = len(off) - 1, int(off[-1])
-        shoff = self.shell_offsets(off, z)
+        if (self._last is not None and np.array_equal(self._last[0], off) and np.array_equal(self._last[1], z)):
+            off, z = self._last  # the same topology as the last call (trajectories, optimisers, repeated batches)
+            shoff = self._last_shoff
+        else:
+            off, z = off.copy(), z.copy()
+            shoff = self.shell_offsets(off, z)
+            for a in (off, z, shoff):  # shared by the results and the cache
+                a.flags.writeable = False
         nsh = int(shoff[-1])
         ch = None if charges is None else np.ascontiguousarray(charges, dtype=np.float64)
         q0 = None if initial_shell_charges is None else np.ascontiguousarray(initial_shell_charges, dtype=np.float64)
@@ -136,7 +144,7 @@ class BatchCalculator:
         rc = L.gfn1_batch_energy_gradient(self.engine.handle, nmol, _lib.ptr(off, ctypes.c_int32),
                                           _lib.ptr(z, ctypes.c_uint8), _lib.ptr(xyz), _lib.ptr(ch), _lib.ptr(q0),
                                           ctypes.byref(opt), ctypes.byref(out))
-        self._last = (off, z)
+        self._last, self._last_shoff = (off, z), shoff
         if rc != 0 and (raise_on_error or rc not in (3, 4, 8, 12)):
             _lib.check(rc, self.engine.handle)
         return BatchResult(energy, terms, grad, qsh, qat, dip, fermi, iters, status, off, shoff, rung)
