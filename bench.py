@@ -24,6 +24,11 @@ parity: both arms against the CPU oracle on its sample of the workload, at
 the bench's options and converged tightly (the FP64 answer the bars refer
 to: |dE| <= 1e-6 Eh, |dg| <= 1e-5 Eh/bohr, |dq_shell| <= 1e-5 e).
 
+other_configs (rank 0, one GPU): the 16- and 300-water clusters and the
+first 64 frames of the 96-water trajectory through the public API, each with
+its parity against the CPU oracle (live for the 16 waters, the committed
+oracle fixtures for the others) and the large-molecule path's autotuned plan.
+
 --impl reference times the CPU restatement of gfn1-rs's path (oracle/, C++ FP64,
 all host threads, zero initial guess, the same options) on a bounded sample of
 the same workload.
@@ -80,6 +85,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nmol", type=int, default=NMOL)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-other-configs", action="store_true",
+                    help="skip the 16- and 300-water clusters and the 96-water trajectory (rank 0, one GPU)")
     ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
                     help="weak: every rank evaluates its own 4096-molecule batch; strong: one global batch split "
                          "over the ranks by longest-processing-time on the SCC cost model (gfn1_rs.shard)")
@@ -249,6 +256,123 @@ def unbatched_plain(calc, off, z, xb, nsample=256):
         calc.calculate_flat([0, a1 - a0], z[a0:a1], xb[a0:a1])
     torch.cuda.synchronize()
     return nsample / (time.perf_counter() - t0)
+
+
+def _max_dev(res, m, energy, gradient, shell_q, a0, a1, s0, s1):
+    return (abs(float(res.energy[m]) - energy),
+            float(np.max(np.abs(res.gradient[a0:a1] - np.asarray(gradient)))),
+            float(np.max(np.abs(res.shell_charges[s0:s1] - np.asarray(shell_q)))))
+
+
+def other_configs(frames: int = 64):
+    """The plan's other workloads on this GPU in the same run, each after one
+    warm-up call, wall clock around synchronous calls through the public API,
+    with parity against the CPU oracle:
+      water16: the 16-water cluster (48 atoms, 128 AOs, seed 0), converged
+        tightly (1e-8 Eh, 1e-7 e), one molecule per call; the oracle runs the
+        same molecule on one host thread here (its time is the CPU figure);
+      water300: the 300-water cluster (900 atoms, 2400 AOs, seed 1), tightly
+        converged, on the large-molecule path; parity against the committed
+        oracle fixture (tests/golden/large_systems.json; its single-thread CPU
+        time comes from that fixture run, not from this host); the
+        autotuner's reduction plan;
+      water96: the first `frames` frames of the 96-water trajectory (288 atoms,
+        768 AOs each, seed 2) as one batch at the bench's options, plain and
+        learned guess; parity on the fixture's three frames, tightly converged.
+    """
+    import ctypes
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from gfn1_rs import BatchCalculator, _lib, trajectory, workloads
+
+    tight = dict(energy_tolerance=1e-8, charge_tolerance=1e-7)
+    out = {}
+    # config 0
+    z, x = workloads.water_cluster(16, 0)
+    xb = np.ascontiguousarray(x * A2B)
+    off1 = [0, len(z)]
+    rec = {"workload": "16-water cluster, 48 atoms, 128 AOs, seed 0, converged to 1e-8 Eh / 1e-7 e"}
+    for arm, kw in (("plain", {}), ("learned", {"learned_guess": True})):
+        calc = BatchCalculator(**tight, **kw)
+        r = calc.calculate_flat(off1, z, xb)
+        reps = 10
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            r = calc.calculate_flat(off1, z, xb)
+        dt = (time.perf_counter() - t0) / reps
+        rec[arm] = {"evals_per_s": 1.0 / dt, "iterations": int(r.iterations[0]), "status": int(r.status[0])}
+        rec[arm + "_result"] = r
+    t0 = time.perf_counter()
+    o = oracle.run(z, xb, options=oracle.make_options(**tight))
+    cpu_s = time.perf_counter() - t0
+    rec["cpu"] = {"evals_per_s": 1.0 / cpu_s, "cores": 1, "kind": "port", "iterations": int(o.iterations)}
+    ns = len(o.shell_charges)
+    for arm in ("plain", "learned"):
+        r = rec.pop(arm + "_result")
+        dE, dg, dq = _max_dev(r, 0, o.energy, o.gradient, o.shell_charges, 0, len(z), 0, ns)
+        rec[arm]["parity_vs_oracle"] = {"max_abs_dE": dE, "max_abs_dg": dg, "max_abs_dq": dq}
+    rec["gpu_vs_cpu"] = rec["plain"]["evals_per_s"] / rec["cpu"]["evals_per_s"]
+    out["water16"] = rec
+    # config 2
+    with open(os.path.join(ROOT, "tests", "golden", "large_systems.json")) as fh:
+        fx = json.load(fh)
+    w = fx["water300"]
+    z = np.array(w["numbers"])
+    xb = np.ascontiguousarray(np.array(w["positions_angstrom"]) * A2B)
+    off1 = [0, len(z)]
+    rec = {"workload": "300-water cluster, 900 atoms, 2400 AOs, seed 1, converged to 1e-8 Eh / 1e-7 e"}
+    for arm, kw in (("plain", {}), ("learned", {"learned_guess": True})):
+        calc = BatchCalculator(**tight, **kw)
+        r = calc.calculate_flat(off1, z, xb)  # warm-up: allocation and the autotuner
+        reps = 2
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            r = calc.calculate_flat(off1, z, xb)
+        dt = (time.perf_counter() - t0) / reps
+        dE, dg, dq = _max_dev(r, 0, w["energy"], w["gradient"], w["shell_charges"], 0, len(z), 0,
+                              len(w["shell_charges"]))
+        rec[arm] = {"evals_per_s": 1.0 / dt, "seconds": dt, "iterations": int(r.iterations[0]),
+                    "status": int(r.status[0]),
+                    "parity_vs_oracle_fixture": {"max_abs_dE": dE, "max_abs_dg": dg, "max_abs_dq": dq}}
+        if arm == "plain":
+            v = [ctypes.c_int32() for _ in range(3)] + [ctypes.c_double(), ctypes.c_int32()]
+            _lib.check(_lib.load().gfn1_last_wide_plan(calc.engine.handle, *[ctypes.byref(t) for t in v]),
+                       calc.engine.handle)
+            rec["reduction_plan"] = {"panel": v[0].value, "min_rows_per_cta": v[1].value,
+                                     "ctas_per_molecule": v[2].value, "autotuned_reduction_ms": v[3].value,
+                                     "autotuned": bool(v[4].value)}
+    rec["cpu_fixture"] = {"seconds": w["seconds"], "iterations": w["iterations"], "cores": 1, "kind": "port",
+                          "where": "oracle fixture run on one core of the build host, not this host"}
+    rec["gpu_vs_cpu_fixture"] = w["seconds"] / rec["plain"]["seconds"]
+    out["water300"] = rec
+    # config 4
+    z, xt = workloads.water_trajectory(96, frames=frames)
+    xt = xt * A2B
+    rec = {"workload": f"96-water free-flight trajectory, first {frames} frames (288 atoms, 768 AOs) in one batch, "
+                       f"converged to {ENERGY_TOL:g} Eh / {CHARGE_TOL:g} e"}
+    calc = BatchCalculator(energy_tolerance=ENERGY_TOL, charge_tolerance=CHARGE_TOL)
+    for mode in ("plain", "learned"):
+        trajectory.run_trajectory(z, xt, batch=frames, mode=mode, calc=calc)  # warm-up
+        r = trajectory.run_trajectory(z, xt, batch=frames, mode=mode, calc=calc)
+        rec[mode] = {"evals_per_s": frames / r["seconds"], "iterations_mean": float(r["iterations"].mean()),
+                     "failed": int((r["status"] != 0).sum()), "rungs": trajectory.rung_usage(r["rung"])}
+    fr = fx["water96_traj"]
+    zf = np.array(fr[0]["numbers"])
+    nat = len(zf)
+    offf = (np.arange(len(fr) + 1) * nat).astype(np.int32)
+    xf = np.concatenate([np.array(f["positions_angstrom"]) for f in fr]) * A2B
+    r = BatchCalculator(**tight).calculate_flat(offf, np.tile(zf, len(fr)), xf)
+    nsa = len(fr[0]["shell_charges"])
+    dev = [_max_dev(r, i, f["energy"], f["gradient"], f["shell_charges"], i * nat, (i + 1) * nat, i * nsa,
+                    (i + 1) * nsa) for i, f in enumerate(fr)]
+    rec["parity_vs_oracle_fixture"] = {"frames": len(fr), "max_abs_dE": max(d[0] for d in dev),
+                                       "max_abs_dg": max(d[1] for d in dev), "max_abs_dq": max(d[2] for d in dev)}
+    rec["cpu_fixture"] = {"seconds_per_frame": float(np.mean([f["seconds"] for f in fr])), "cores": 1,
+                          "kind": "port", "where": "oracle fixture run on one core of the build host, tight "
+                                                   "convergence, not this host"}
+    out["water96"] = rec
+    return out
 
 
 def run_reference(args, rank):
@@ -450,6 +574,8 @@ def main():
         cfg["parity_vs_oracle"] = parity
         cfg["scc_iterations_p95"] = {"learned": float(np.percentile(res.iterations, 95)),
                                      "plain": float(np.percentile(res_plain.iterations, 95))}
+        if world == 1 and not args.no_other_configs:
+            cfg["other_configs"] = other_configs()
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps, "higher_is_better": True,
                "scaling": args.scaling, "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded clusters)",

@@ -1375,6 +1375,21 @@ int gfn1_batch_download(gfn1_batch* b, const gfn1_outputs* out) {
   return finish(b, out, b->eng->stream);
 }
 
+int gfn1_last_wide_plan(gfn1_engine* eng, int32_t* panel, int32_t* min_rows, int32_t* ctas_per_molecule,
+                        double* reduction_ms, int32_t* tuned) {
+  if (!eng) return fail(eng, GFN1_E_INVALID_INPUT, "invalid arguments");
+  int nb = 0, mr = 0, g = 0, tu = 0;
+  float ms = 0.f;
+  const gfn1_batch* b = eng->oneshot;
+  if (b && b->wide && !b->wide_ids.empty()) wide_plan_info(b->wide, &nb, &mr, &g, &ms, &tu);
+  if (panel) *panel = nb;
+  if (min_rows) *min_rows = mr;
+  if (ctas_per_molecule) *ctas_per_molecule = g;
+  if (reduction_ms) *reduction_ms = ms;
+  if (tuned) *tuned = tu;
+  return GFN1_OK;
+}
+
 int gfn1_batch_stage_cycles(const gfn1_batch* b, uint64_t* cycles, int n) {
   if (!b || !cycles) return fail(nullptr, GFN1_E_INVALID_INPUT, "invalid arguments");
   if (!b->profiling) return fail(b->eng, GFN1_E_INVALID_INPUT, "stage profiling is off (set GFN1_PROFILE=1)");

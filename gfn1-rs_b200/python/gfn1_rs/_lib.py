@@ -116,6 +116,7 @@ def load():
         L.gfn1_batch_launch_stage.argtypes = [vp, ctypes.c_int, vp]
         L.gfn1_batch_stage_cycles.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
         L.gfn1_batch_io_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
+        L.gfn1_last_wide_plan.argtypes = [vp, _ip, _ip, _ip, _dp, _ip]
         L.gfn1_last_molecule_matrices.argtypes = [vp, ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp]
         L.gfn1_batch_molecule_matrices.argtypes = [vp, ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp]
         L.gfn1_last_molecule_fock.argtypes = [vp, ctypes.c_int, _dp, _dp, _dp]
@@ -152,7 +153,7 @@ def load():
             getattr(L, name).restype = ctypes.c_int
         for name in ("gfn1_last_molecule_matrices", "gfn1_batch_molecule_matrices", "gfn1_run_noalloc",
                      "gfn1_last_molecule_fock", "gfn1_batch_molecule_fock", "gfn1_batch_optimize",
-                     "gfn1_batch_launch_stage", "gfn1_batch_stage_cycles", "gfn1_batch_io_bytes",
+                     "gfn1_batch_launch_stage", "gfn1_batch_stage_cycles", "gfn1_batch_io_bytes", "gfn1_last_wide_plan",
                      "gfn1_engine_create", "gfn1_basis_size", "gfn1_run", "gfn1_batch_energy_gradient",
                      "gfn1_batch_create", "gfn1_batch_set_positions", "gfn1_batch_set_initial_charges",
                      "gfn1_batch_launch", "gfn1_batch_download", "gfn1_batch_outputs_device", "gfn1_batch_info"):

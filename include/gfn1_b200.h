@@ -160,6 +160,15 @@ int gfn1_batch_stage_cycles(const gfn1_batch* b, uint64_t* cycles, int n);
 /* Bytes of the input blob (one host->device copy per call) and of the output
  * blob (one device->host copy per call). */
 int gfn1_batch_io_bytes(const gfn1_batch* b, int64_t* h2d, int64_t* d2h);
+/* Plan of the large-molecule path (molecules above 256 AOs) in the last
+ * gfn1_batch_energy_gradient / gfn1_run call on this engine: the Householder
+ * reduction's panel width, its minimum rows per CTA, the CTAs per molecule,
+ * the reduction time the autotuner measured for that plan (ms) and whether the
+ * autotuner chose it (1) or GFN1_WIDE_PANEL fixed it (0).  All zero when that
+ * call had no large molecule.  No counterpart in the reference (faer chooses
+ * its own blocking inside self_adjoint_eigen, src/linalg.rs:176). */
+int gfn1_last_wide_plan(gfn1_engine* eng, int32_t* panel, int32_t* min_rows, int32_t* ctas_per_molecule,
+                        double* reduction_ms, int32_t* tuned);
 /* Synchronises and copies results to host buffers. */
 int gfn1_batch_download(gfn1_batch* b, const gfn1_outputs* out);
 /* As gfn1_last_molecule_matrices for molecule m of a resident batch after its

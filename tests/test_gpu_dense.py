@@ -138,3 +138,34 @@ def test_fallback_ladder_on_the_large_molecule_path(gpu_calc, oracle_mod, fixtur
     assert abs(r.energy[0] - o.energy) <= 1e-6
     assert np.abs(r.gradient - o.gradient).max() <= 1e-5
 
+
+
+def test_last_wide_plan_reports_the_autotuned_reduction(gpu_calc):
+    """gfn1_last_wide_plan: the autotuner's choice after a call with a
+    large molecule (a panel width and a minimum row count among its
+    candidates, at least one CTA per molecule, a measured time), all zeros
+    after a call without one."""
+    import ctypes
+
+    from gfn1_rs import BatchCalculator, _lib, workloads
+
+    def plan(calc):
+        v = [ctypes.c_int32() for _ in range(3)] + [ctypes.c_double(), ctypes.c_int32()]
+        _lib.check(_lib.load().gfn1_last_wide_plan(calc.engine.handle, *[ctypes.byref(t) for t in v]),
+                   calc.engine.handle)
+        return [t.value for t in v]
+
+    old = os.environ.pop("GFN1_WIDE_PANEL", None)
+    try:
+        calc = BatchCalculator()
+        z, x = workloads.water_cluster(40, 7)  # 320 AOs: above the 256-AO threshold
+        r = calc.calculate_flat([0, len(z)], z, x * A2B)
+        assert r.status[0] == 0
+        nb, mr, g, ms, tuned = plan(calc)
+        assert nb in (8, 16, 32) and mr in (4, 8, 16, 32, 64, 128) and g >= 1 and ms > 0.0 and tuned == 1
+        z, x = workloads.water_cluster(4, 7)  # 32 AOs: one SM
+        calc.calculate_flat([0, len(z)], z, x * A2B)
+        assert plan(calc) == [0, 0, 0, 0.0, 0]
+    finally:
+        if old is not None:
+            os.environ["GFN1_WIDE_PANEL"] = old
