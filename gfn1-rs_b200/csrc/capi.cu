@@ -25,8 +25,10 @@
 #include "model.cuh"
 
 namespace gfn1 {
-__global__ void setup_kernel(Batch B, Model M, int enable_dispersion, int max_nsh, const int* mols);
-__global__ void grad_kernel(Batch B, Model M, const int* mols, int phases);
+cudaError_t launch_setup(int max_l, dim3 grid, int nt, size_t smem, cudaStream_t st, const Batch& B, const Model& M,
+                         int enable_dispersion, int max_nsh, const int* mols);
+cudaError_t launch_grad(int max_l, dim3 grid, size_t smem, cudaStream_t st, const Batch& B, const Model& M,
+                        const int* mols, int phases);
 long long scc_workspace_doubles(int maxn, int maxnsh, int cap, int maxnat);
 size_t scc_smem_bytes(int maxnsh, int maxn, int maxnat, int matrix_n);
 size_t scc_max_dynamic_smem(int nt);
@@ -287,6 +289,7 @@ struct gfn1_batch {
   int nmol = 0;
   long long natoms = 0, nshells = 0, naos = 0, mat_total = 0, gam_total = 0, pair_total = 0;
   int max_nat = 0, max_nsh = 0, max_n = 0, cap = 0;
+  int max_l = 0;  // highest shell angular momentum of the batch (selects the s/p setup and gradient kernels)
   // SCC size classes: [0] molecules above the split size, [1] the rest
   struct SccClass {
     int q_begin = 0, q_end = 0, n_cta = 0, nt = 256, maxn = 0, maxnsh = 0, maxnat = 0;
@@ -668,6 +671,7 @@ int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t*
   const long long natoms = atom_offsets[nmol];
   b->natoms = natoms;
   b->max_nat = b->max_nsh = b->max_n = 0;
+  b->max_l = 0;
   // sizes first (for the blob layout)
   std::vector<int> nsh_m(nmol), n_m(nmol), st_m(nmol, GFN1_OK);
   std::vector<double> nref_m(nmol, 0.0);
@@ -695,6 +699,7 @@ int prepare(gfn1_batch* b, int nmol, const int32_t* atom_offsets, const uint8_t*
       n += eng->elem[zz].nao;
       s += eng->elem[zz].nsh;
       nref_m[m] += eng->refocc_total[zz];
+      for (int k = 0; k < eng->elem[zz].nsh; ++k) b->max_l = std::max(b->max_l, eng->elem[zz].l[k]);
     }
     const double ch = charge ? charge[m] : 0.0;
     const double nelec = nref_m[m] - ch;  // src/electronic.rs:491-510
@@ -979,14 +984,16 @@ int launch_stage(gfn1_batch* b, int stage, cudaStream_t st) {
     }
     const size_t smem = sizeof(double) * (16 * (size_t)b->max_nat + 32) +
                         sizeof(int) * (3 * (size_t)b->max_nat + 2 + 2 * (size_t)b->max_nsh);
-    if (smem > 48 * 1024) cudaFuncSetAttribute(setup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     // one CTA per molecule; large molecules (the leading entries of the
-    // processing order) with their shell pairs split over many CTAs
+    // processing order) with their shell pairs split over many CTAs; the s/p
+    // instantiation unless the batch has a d shell
     const int nd = b->n_dense, ns = b->nmol - nd;
-    if (ns > 0) setup_kernel<<<dim3(ns, 1), nt, smem, st>>>(B, M, b->opt.enable_dispersion, b->max_nsh, B.order + nd);
-    if (nd > 0)
-      setup_kernel<<<dim3(nd, std::max(1, 4 * eng->num_sms / nd)), nt, smem, st>>>(B, M, b->opt.enable_dispersion,
-                                                                                 b->max_nsh, B.order);
+    if (ns > 0 && (e = launch_setup(b->max_l, dim3(ns, 1), nt, smem, st, B, M, b->opt.enable_dispersion, b->max_nsh,
+                                    B.order + nd)) != cudaSuccess)
+      return cuda_fail(eng, e, "setup launch");
+    if (nd > 0 && (e = launch_setup(b->max_l, dim3(nd, std::max(1, 4 * eng->num_sms / nd)), nt, smem, st, B, M,
+                                    b->opt.enable_dispersion, b->max_nsh, B.order)) != cudaSuccess)
+      return cuda_fail(eng, e, "setup launch");
   } else if (stage == 1) {
     SccOptions so;
     so.max_scc = b->opt.max_scc;
@@ -1051,12 +1058,14 @@ int launch_stage(gfn1_batch* b, int stage, cudaStream_t st) {
   } else if (stage == 2) {
     if (!b->opt.compute_gradient) return GFN1_OK;
     const size_t smem = sizeof(double) * 7 * (size_t)b->max_nat + sizeof(int) * (3 * (size_t)b->max_nat + 2);
-    if (smem > 48 * 1024) cudaFuncSetAttribute(grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int nd = b->n_dense, ns = b->nmol - nd;
-    if (ns > 0) grad_kernel<<<dim3(ns, 1), kGradThreads, smem, st>>>(B, M, B.order + nd, 3);
+    if (ns > 0 && (e = launch_grad(b->max_l, dim3(ns, 1), smem, st, B, M, B.order + nd, 3)) != cudaSuccess)
+      return cuda_fail(eng, e, "gradient launch");
     if (nd > 0) {  // large molecules: atom pairs over many CTAs, then the per-atom sums
-      grad_kernel<<<dim3(nd, std::max(1, 4 * eng->num_sms / nd)), kGradThreads, smem, st>>>(B, M, B.order, 1);
-      grad_kernel<<<dim3(nd, 1), kGradThreads, smem, st>>>(B, M, B.order, 2);
+      if ((e = launch_grad(b->max_l, dim3(nd, std::max(1, 4 * eng->num_sms / nd)), smem, st, B, M, B.order, 1)) !=
+              cudaSuccess ||
+          (e = launch_grad(b->max_l, dim3(nd, 1), smem, st, B, M, B.order, 2)) != cudaSuccess)
+        return cuda_fail(eng, e, "gradient launch");
     }
   } else {
     return fail(eng, GFN1_E_INVALID_INPUT, "unknown stage");
@@ -1830,7 +1839,8 @@ extern "C" int gfn1_run_noalloc(gfn1_engine* eng, int nat, const uint8_t* z, con
             cudaSuccess)
       return cuda_fail(eng, e, "learned guess");
   }
-  setup_kernel<<<1, 128, sm_setup, st>>>(B, M, o.enable_dispersion, nsh, nullptr);
+  if ((e = launch_setup(2, dim3(1), 128, sm_setup, st, B, M, o.enable_dispersion, nsh, nullptr)) != cudaSuccess)
+    return cuda_fail(eng, e, "setup launch");
   SccLaunch SL;
   SL.q_begin = 0;
   SL.q_end = 1;
@@ -1844,7 +1854,8 @@ extern "C" int gfn1_run_noalloc(gfn1_engine* eng, int nat, const uint8_t* z, con
   SL.smem_bytes = (int)sm_scc;
   if ((e = launch_scc(n > 96 ? 512 : 256, 1, sm_scc, st, B, M, so, SL)) != cudaSuccess)
     return cuda_fail(eng, e, "scc launch");
-  if (o.compute_gradient) grad_kernel<<<1, kGradThreads, sm_grad, st>>>(B, M, nullptr, 3);
+  if (o.compute_gradient && (e = launch_grad(2, dim3(1), sm_grad, st, B, M, nullptr, 3)) != cudaSuccess)
+    return cuda_fail(eng, e, "gradient launch");
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(eng, e, "kernel launch");
   if ((e = cudaMemcpyAsync(hout, base + o_terms, out_end - o_terms, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
     return cuda_fail(eng, e, "device to host copy");

@@ -53,7 +53,10 @@ __device__ __forceinline__ void grad_shell_pair(const ElemTable& eb, int kb, con
 // Molecule blockIdx.x of `mols` (or of the batch when null).  phases: bit 0
 // the atom-pair terms (with gridDim.y > 1 every CTA of a molecule takes every
 // gridDim.y-th block of its atom pairs), bit 1 the per-atom sums and the
-// coordination-number chain (one CTA per molecule, after all pairs).
+// coordination-number chain (one CTA per molecule, after all pairs).  MaxL:
+// the highest shell angular momentum of the batch; the s/p instantiation
+// (MaxL = 1) leaves out the d-shell blocks and their registers.
+template <int MaxL>
 __global__ void __launch_bounds__(kGradThreads, kGradMinBlocks) grad_kernel(Batch B, Model M, const int* mols,
                                                                            int phases) {
   extern __shared__ double gsm[];
@@ -129,6 +132,14 @@ __global__ void __launch_bounds__(kGradThreads, kGradMinBlocks) grad_kernel(Batc
           if (fabs(poly) > 1e-18) dlog = (fi * ea.poly[ka] + fj * eb.poly[kb]) * 0.5 * rr / r2 / poly;
           const int mu0 = atom_ao[b] + eb.ao_first[kb], nu0 = atom_ao[a] + ea.ao_first[ka];
           const double xs[5] = {hij, vmu + vnu, dlog, -eb.kcn[kb] * hs, -ea.kcn[ka] * hs};
+          if constexpr (MaxL < 2) {
+            switch (eb.l[kb] * 2 + ea.l[ka]) {
+              case 0: grad_shell_pair<0, 0>(eb, kb, &xyz[3 * b], ea, ka, &xyz[3 * a], P, W, N, mu0, nu0, xs, rv, gmu, dcmu, dcnu); break;
+              case 1: grad_shell_pair<0, 1>(eb, kb, &xyz[3 * b], ea, ka, &xyz[3 * a], P, W, N, mu0, nu0, xs, rv, gmu, dcmu, dcnu); break;
+              case 2: grad_shell_pair<1, 0>(eb, kb, &xyz[3 * b], ea, ka, &xyz[3 * a], P, W, N, mu0, nu0, xs, rv, gmu, dcmu, dcnu); break;
+              default: grad_shell_pair<1, 1>(eb, kb, &xyz[3 * b], ea, ka, &xyz[3 * a], P, W, N, mu0, nu0, xs, rv, gmu, dcmu, dcnu); break;
+            }
+          } else
           switch (eb.l[kb] * 3 + ea.l[ka]) {
             case 0: grad_shell_pair<0, 0>(eb, kb, &xyz[3 * b], ea, ka, &xyz[3 * a], P, W, N, mu0, nu0, xs, rv, gmu, dcmu, dcnu); break;
             case 1: grad_shell_pair<0, 1>(eb, kb, &xyz[3 * b], ea, ka, &xyz[3 * a], P, W, N, mu0, nu0, xs, rv, gmu, dcmu, dcnu); break;
@@ -215,6 +226,19 @@ __global__ void __launch_bounds__(kGradThreads, kGradMinBlocks) grad_kernel(Batc
     }
     for (int c = 0; c < 3; ++c) B.grad[3 * (a0 + i) + c] = g[c] + B.grad_classic[3 * (a0 + i) + c];
   }
+}
+
+// Launches the gradient kernel for a batch whose highest shell angular
+// momentum is max_l (the s/p instantiation below 2).
+cudaError_t launch_grad(int max_l, dim3 grid, size_t smem, cudaStream_t st, const Batch& B, const Model& M,
+                        const int* mols, int phases) {
+  auto* k = max_l >= 2 ? grad_kernel<2> : grad_kernel<1>;
+  if (smem > 48 * 1024) {
+    const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  k<<<grid, kGradThreads, smem, st>>>(B, M, mols, phases);
+  return cudaGetLastError();
 }
 
 }  // namespace gfn1

@@ -129,6 +129,9 @@ __device__ double halogen_term(const Model& M, const int* zs, const double* xyz,
 // coordination numbers and self energies (cheap, identical), then takes every
 // gridDim.y-th block of its shell pairs for S, H0 and the Coulomb matrix; the
 // classical terms (repulsion, D3, halogen bonds) stay with blockIdx.y == 0.
+// MaxL: the highest shell angular momentum of the batch; the s/p
+// instantiation (MaxL = 1) leaves out the d-shell blocks and their registers.
+template <int MaxL>
 __global__ void __launch_bounds__(128, 4) setup_kernel(Batch B, Model M, int enable_dispersion, int max_nsh,
                                                         const int* mols) {
   extern __shared__ double smem[];
@@ -233,6 +236,14 @@ __global__ void __launch_bounds__(128, 4) setup_kernel(Batch B, Model M, int ena
         hij = 0.5 * (sei + sej) * hscale(M, za, ka, zb, kb) * poly;
       }
     }
+    if constexpr (MaxL < 2) {
+      switch (la * 2 + lb) {
+        case 0: shell_pair_sh0<0, 0>(ea, ka, &xyz[3 * a], eb, kb, &xyz[3 * b], zero, hij, S, H0, N, mu0, nu0); break;
+        case 1: shell_pair_sh0<0, 1>(ea, ka, &xyz[3 * a], eb, kb, &xyz[3 * b], zero, hij, S, H0, N, mu0, nu0); break;
+        case 2: shell_pair_sh0<1, 0>(ea, ka, &xyz[3 * a], eb, kb, &xyz[3 * b], zero, hij, S, H0, N, mu0, nu0); break;
+        default: shell_pair_sh0<1, 1>(ea, ka, &xyz[3 * a], eb, kb, &xyz[3 * b], zero, hij, S, H0, N, mu0, nu0); break;
+      }
+    } else
     switch (la * 3 + lb) {
       case 0: shell_pair_sh0<0, 0>(ea, ka, &xyz[3 * a], eb, kb, &xyz[3 * b], zero, hij, S, H0, N, mu0, nu0); break;
       case 1: shell_pair_sh0<0, 1>(ea, ka, &xyz[3 * a], eb, kb, &xyz[3 * b], zero, hij, S, H0, N, mu0, nu0); break;
@@ -404,6 +415,19 @@ __global__ void __launch_bounds__(128, 4) setup_kernel(Batch B, Model M, int ena
     t[7] = edisp;
     t[8] = ehal;
   }
+}
+
+// Launches the setup kernel for a batch whose highest shell angular momentum
+// is max_l (the s/p instantiation below 2).
+cudaError_t launch_setup(int max_l, dim3 grid, int nt, size_t smem, cudaStream_t st, const Batch& B, const Model& M,
+                         int enable_dispersion, int max_nsh, const int* mols) {
+  auto* k = max_l >= 2 ? setup_kernel<2> : setup_kernel<1>;
+  if (smem > 48 * 1024) {
+    const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  k<<<grid, nt, smem, st>>>(B, M, enable_dispersion, max_nsh, mols);
+  return cudaGetLastError();
 }
 
 }  // namespace gfn1
