@@ -25,8 +25,12 @@ __device__ __forceinline__ float dsilu_f(float z) {
 // ------------------------------------------------------------------ descriptors
 // One CTA per molecule, one warp per atom.  Lanes own radial features lane and
 // lane + 32 (channels 0-1 and 2-3, centre lane & 15); lanes 0..15 own the
-// angular pair (channel lane >> 2, radial function lane & 3).
-__global__ void __launch_bounds__(128) guess_features_kernel(int nmol, const int* __restrict__ atom_off,
+// angular pair (channel lane >> 2, radial function lane & 3).  The neighbour
+// geometry (distance, cutoff function, unit vector, channel) is formed once per
+// neighbour, by the lane j - j0 of a 32-neighbour chunk, and broadcast to the
+// warp in neighbour order, so every feature sums its terms in the order of
+// the neighbours.
+__global__ void __launch_bounds__(128, 4) guess_features_kernel(int nmol, const int* __restrict__ atom_off,
                                                              const int* __restrict__ z,
                                                              const double* __restrict__ xyz,
                                                              const float* __restrict__ mean,
@@ -51,31 +55,49 @@ __global__ void __launch_bounds__(128) guess_features_kernel(int nmol, const int
     const double xa = xyz[3LL * i], ya = xyz[3LL * i + 1], za = xyz[3LL * i + 2];
     double g0 = 0.0, g1 = 0.0;
     double vx = 0.0, vy = 0.0, vz = 0.0, sxx = 0.0, syy = 0.0, szz = 0.0, sxy = 0.0, sxz = 0.0, syz = 0.0, sw = 0.0;
-    for (int j = a0; j < a1; ++j) {
-      if (j == i) continue;
-      const int cj = elem_channel(z[j]);
-      if (cj < 0) continue;
-      const double dx = xyz[3LL * j] - xa, dy = xyz[3LL * j + 1] - ya, dz = xyz[3LL * j + 2] - za;
-      const double r2 = dx * dx + dy * dy + dz * dz;
-      if (!(r2 < rc * rc) || r2 == 0.0) continue;
-      const double r = sqrt(r2);
-      const double fc = 0.5 * (cos(pi * r / rc) + 1.0);
-      const double gr = exp(-4.0 * (r - mu) * (r - mu)) * fc;
-      if (cj == c0) g0 += gr;
-      if (cj == c1) g1 += gr;
-      if (lane < 16 && cj == ca) {
-        const double w = exp(-(r - nu) * (r - nu)) * fc;
-        const double ux = dx / r, uy = dy / r, uz = dz / r;
-        vx += w * ux;
-        vy += w * uy;
-        vz += w * uz;
-        sxx += w * ux * ux;
-        syy += w * uy * uy;
-        szz += w * uz * uz;
-        sxy += w * ux * uy;
-        sxz += w * ux * uz;
-        syz += w * uy * uz;
-        sw += w;
+    for (int j0 = a0; j0 < a1; j0 += 32) {
+      // neighbour j0 + lane: channel (-1: none), distance, cutoff function, unit vector
+      int cjl = -1;
+      double rl = 0.0, fcl = 0.0, uxl = 0.0, uyl = 0.0, uzl = 0.0;
+      const int jl = j0 + lane;
+      if (jl < a1 && jl != i) {
+        const int cj = elem_channel(z[jl]);
+        const double dx = xyz[3LL * jl] - xa, dy = xyz[3LL * jl + 1] - ya, dz = xyz[3LL * jl + 2] - za;
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        if (cj >= 0 && r2 < rc * rc && r2 != 0.0) {
+          cjl = cj;
+          rl = sqrt(r2);
+          fcl = 0.5 * (cos(pi * rl / rc) + 1.0);
+          uxl = dx / rl;
+          uyl = dy / rl;
+          uzl = dz / rl;
+        }
+      }
+      const int nj = min(32, a1 - j0);
+      for (int t = 0; t < nj; ++t) {
+        const int cj = __shfl_sync(0xffffffffu, cjl, t);
+        if (cj < 0) continue;
+        const double r = __shfl_sync(0xffffffffu, rl, t);
+        const double fc = __shfl_sync(0xffffffffu, fcl, t);
+        const double gr = exp(-4.0 * (r - mu) * (r - mu)) * fc;
+        if (cj == c0) g0 += gr;
+        if (cj == c1) g1 += gr;
+        const double ux = __shfl_sync(0xffffffffu, uxl, t);
+        const double uy = __shfl_sync(0xffffffffu, uyl, t);
+        const double uz = __shfl_sync(0xffffffffu, uzl, t);
+        if (lane < 16 && cj == ca) {
+          const double w = exp(-(r - nu) * (r - nu)) * fc;
+          vx += w * ux;
+          vy += w * uy;
+          vz += w * uz;
+          sxx += w * ux * ux;
+          syy += w * uy * uy;
+          szz += w * uz * uz;
+          sxy += w * ux * uy;
+          sxz += w * ux * uz;
+          syz += w * uy * uz;
+          sw += w;
+        }
       }
     }
     auto put = [&](int f, double v) {
@@ -94,56 +116,87 @@ __global__ void __launch_bounds__(128) guess_features_kernel(int nmol, const int
 }
 
 // ------------------------------------------------------------------ inference
-constexpr int kTile = 64;      // atoms per tile
-constexpr int kInferNT = 256;  // 8 warps: warp w owns rows 8w..8w+7, lane l columns 4l..4l+3
+// Tensor-core MLP on 64-atom tiles: each hidden layer is a [64 x K] x [K x 128]
+// product of BF16 activations and weights with FP32 accumulation
+// (mma.sync.m16n8k16, 8 warps: warp w takes rows 16 (w & 3).. and columns
+// 64 (w >> 2)..), then bias and SiLU in FP32, rounded to BF16 for the next
+// layer.  Weights sit transposed in shared memory ([n][k], rows padded by 8
+// elements so that the fragment loads of the 8 row groups fall in distinct
+// banks); the first layer's K = 100 is padded with zeros to 112.
+constexpr int kTile = 64;                  // atoms per tile
+constexpr int kInferNT = 256;              // 8 warps
+constexpr int kK1 = 112;                   // kGuessIn rounded up to the MMA's k = 16
+constexpr int kLd1 = kK1 + 8;              // row stride (elements) of the input tile and W1^T
+constexpr int kLdH = kGuessHid + 8;        // row stride of hidden activations, W2^T and W3^T
+static_assert(kGuessIn <= kK1 && kK1 % 16 == 0, "first-layer padding");
 
 struct InferSmem {
-  static constexpr size_t w1 = 0;
-  static constexpr size_t w2 = w1 + sizeof(uint16_t) * kGuessIn * kGuessHid;
-  static constexpr size_t w3 = w2 + sizeof(uint16_t) * kGuessHid * kGuessHid;
-  static constexpr size_t w4 = w3 + sizeof(uint16_t) * kGuessHid * kGuessHid;
-  static constexpr size_t bias = w4 + sizeof(uint16_t) * kGuessHid * kGuessOut;
-  static constexpr size_t xin = bias + sizeof(float) * (3 * kGuessHid + 4);
-  static constexpr size_t h0 = xin + sizeof(uint16_t) * kTile * kGuessIn;
-  static constexpr size_t h1 = h0 + sizeof(uint16_t) * kTile * kGuessHid;
-  static constexpr size_t total = h1 + sizeof(uint16_t) * kTile * kGuessHid;
+  static constexpr size_t w1 = 0;                                                    // W1^T [128][kLd1]
+  static constexpr size_t w2 = w1 + sizeof(uint16_t) * kGuessHid * kLd1;             // W2^T [128][kLdH]
+  static constexpr size_t w3 = w2 + sizeof(uint16_t) * kGuessHid * kLdH;             // W3^T [128][kLdH]
+  static constexpr size_t w4 = w3 + sizeof(uint16_t) * kGuessHid * kLdH;             // W4 [128][2]
+  static constexpr size_t bias = w4 + sizeof(uint16_t) * kGuessHid * kGuessOut;      // b1 b2 b3 b4 (FP32)
+  static constexpr size_t xin = bias + sizeof(float) * (3 * kGuessHid + 4);          // [64][kLd1]
+  static constexpr size_t h0 = xin + sizeof(uint16_t) * kTile * kLd1;                // [64][kLdH]
+  static constexpr size_t h1 = h0 + sizeof(uint16_t) * kTile * kLdH;                 // [64][kLdH]
+  static constexpr size_t total = h1 + sizeof(uint16_t) * kTile * kLdH;
 };
+static_assert(InferSmem::w2 % 16 == 0 && InferSmem::w3 % 16 == 0 && InferSmem::w4 % 16 == 0 &&
+                  InferSmem::bias % 16 == 0 && InferSmem::xin % 16 == 0 && InferSmem::h0 % 16 == 0 &&
+                  InferSmem::h1 % 16 == 0,
+              "16-byte aligned regions");
 
 __device__ __forceinline__ float bf2f(uint16_t h) { return __uint_as_float(((unsigned)h) << 16); }
 __device__ __forceinline__ uint16_t f2bf(float f) {
   const __nv_bfloat16 b = __float2bfloat16_rn(f);
   return *reinterpret_cast<const uint16_t*>(&b);
 }
+__device__ __forceinline__ uint32_t lds32(const uint16_t* p) { return *reinterpret_cast<const uint32_t*>(p); }
 
-// One hidden layer on a 64-atom tile: out = SiLU(in W + b), in [64][K], W [K][128].
-template <int K>
-__device__ __forceinline__ void infer_layer(const uint16_t* __restrict__ in, const uint16_t* __restrict__ W,
+// D += A B for one 16x8 tile, k = 16: A row-major (a0: rows g, k 2t..2t+1;
+// a1: rows g + 8; a2, a3: k + 8), B column-major (b0: k 2t..2t+1 of column
+// g; b1: k + 8), D (d0, d1: row g, columns 2t, 2t + 1; d2, d3: row g + 8),
+// g = lane / 4, t = lane % 4.
+__device__ __forceinline__ void mma_bf16_16x8x16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                                 uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// One hidden layer on a 64-atom tile: out = SiLU(in W + b); in [64][LDI],
+// wt = W^T [128][LDI], out [64][kLdH], K a multiple of 16.
+template <int K, int LDI>
+__device__ __forceinline__ void infer_layer(const uint16_t* __restrict__ in, const uint16_t* __restrict__ wt,
                                             const float* __restrict__ bias, uint16_t* __restrict__ out) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int r0 = (wid & 3) * 16, n0 = (wid >> 2) * 64;
   float acc[8][4];
 #pragma unroll
-  for (int r = 0; r < 8; ++r)
+  for (int q = 0; q < 8; ++q)
 #pragma unroll
-    for (int c = 0; c < 4; ++c) acc[r][c] = 0.0f;
-  const uint16_t* inr = in + (wid * 8) * K;
-#pragma unroll 4
-  for (int k = 0; k < K; ++k) {
-    const uint2 wv = *reinterpret_cast<const uint2*>(W + k * kGuessHid + 4 * lane);
-    const float w0 = bf2f(wv.x & 0xffff), w1 = bf2f(wv.x >> 16), w2 = bf2f(wv.y & 0xffff), w3 = bf2f(wv.y >> 16);
+    for (int c = 0; c < 4; ++c) acc[q][c] = 0.0f;
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-      const float h = bf2f(inr[r * K + k]);
-      acc[r][0] += h * w0;
-      acc[r][1] += h * w1;
-      acc[r][2] += h * w2;
-      acc[r][3] += h * w3;
+  for (int k0 = 0; k0 < K; k0 += 16) {
+    const uint16_t* ar = in + (r0 + g) * LDI + k0 + 2 * t;
+    const uint32_t a0 = lds32(ar), a1 = lds32(ar + 8 * LDI), a2 = lds32(ar + 8), a3 = lds32(ar + 8 * LDI + 8);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const uint16_t* br = wt + (n0 + 8 * q + g) * LDI + k0 + 2 * t;
+      mma_bf16_16x8x16(acc[q], a0, a1, a2, a3, lds32(br), lds32(br + 8));
     }
   }
 #pragma unroll
-  for (int r = 0; r < 8; ++r) {
-    uint16_t* o = out + (wid * 8 + r) * kGuessHid + 4 * lane;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) o[c] = f2bf(silu_f(acc[r][c] + bias[4 * lane + c]));
+  for (int q = 0; q < 8; ++q) {
+    const int col = n0 + 8 * q + 2 * t;
+    const float b0 = bias[col], b1 = bias[col + 1];
+    const uint32_t lo = (uint32_t)f2bf(silu_f(acc[q][0] + b0)) | ((uint32_t)f2bf(silu_f(acc[q][1] + b1)) << 16);
+    const uint32_t hi = (uint32_t)f2bf(silu_f(acc[q][2] + b0)) | ((uint32_t)f2bf(silu_f(acc[q][3] + b1)) << 16);
+    *reinterpret_cast<uint32_t*>(out + (r0 + g) * kLdH + col) = lo;
+    *reinterpret_cast<uint32_t*>(out + (r0 + g + 8) * kLdH + col) = hi;
   }
 }
 
@@ -161,8 +214,30 @@ __global__ void __launch_bounds__(kInferNT, 1) guess_infer_kernel(const float* _
   uint16_t* sh0 = reinterpret_cast<uint16_t*>(smem + InferSmem::h0);
   uint16_t* sh1 = reinterpret_cast<uint16_t*>(smem + InferSmem::h1);
   const int tid = threadIdx.x;
-  const long long nw = (long long)kGuessIn * kGuessHid + 2LL * kGuessHid * kGuessHid + kGuessHid * kGuessOut;
-  for (long long i = tid; i < nw; i += kInferNT) sw1[i] = wbf16[i];  // W1..W4 are contiguous in smem too
+  // weights: W1..W3 read in their global order [k][n] and stored transposed,
+  // the padding columns zero; W4 as it is
+  const uint16_t* gw1 = wbf16;
+  const uint16_t* gw2 = gw1 + kGuessIn * kGuessHid;
+  const uint16_t* gw3 = gw2 + kGuessHid * kGuessHid;
+  const uint16_t* gw4 = gw3 + kGuessHid * kGuessHid;
+  for (int i = tid; i < kGuessHid * kLd1; i += kInferNT) {
+    const int n = i / kLd1, k = i - n * kLd1;
+    if (k >= kGuessIn) sw1[i] = 0;
+  }
+  for (int i = tid; i < kGuessHid * kLdH; i += kInferNT) {
+    const int n = i / kLdH, k = i - n * kLdH;
+    if (k >= kGuessHid) sw2[i] = sw3[i] = 0;
+  }
+  for (int i = tid; i < kGuessIn * kGuessHid; i += kInferNT) {
+    const int k = i / kGuessHid, n = i - k * kGuessHid;
+    sw1[n * kLd1 + k] = gw1[i];
+  }
+  for (int i = tid; i < kGuessHid * kGuessHid; i += kInferNT) {
+    const int k = i / kGuessHid, n = i - k * kGuessHid;
+    sw2[n * kLdH + k] = gw2[i];
+    sw3[n * kLdH + k] = gw3[i];
+  }
+  for (int i = tid; i < kGuessHid * kGuessOut; i += kInferNT) sw4[i] = gw4[i];
   // biases from the FP32 parameter vector
   const float* pb1 = params + 2 * kGuessDesc + kGuessIn * kGuessHid;
   const float* pb2 = pb1 + kGuessHid + kGuessHid * kGuessHid;
@@ -175,24 +250,24 @@ __global__ void __launch_bounds__(kInferNT, 1) guess_infer_kernel(const float* _
   }
   if (tid < kGuessOut) sb[3 * kGuessHid + tid] = pb4[tid];
   const long long ntiles = (natoms + kTile - 1) / kTile;
-  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const long long row0 = t * kTile;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const long long row0 = tile * kTile;
     __syncthreads();
-    for (int i = tid; i < kTile * kGuessIn; i += kInferNT) {
-      const long long r = row0 + i / kGuessIn;
-      sx[i] = f2bf(r < natoms ? x[row0 * kGuessIn + i] : 0.0f);
+    for (int i = tid; i < kTile * kLd1; i += kInferNT) {
+      const int r = i / kLd1, c = i - r * kLd1;
+      sx[i] = f2bf((c < kGuessIn && row0 + r < natoms) ? x[(row0 + r) * kGuessIn + c] : 0.0f);
     }
     __syncthreads();
-    infer_layer<kGuessIn>(sx, sw1, sb, sh0);
+    infer_layer<kK1, kLd1>(sx, sw1, sb, sh0);
     __syncthreads();
-    infer_layer<kGuessHid>(sh0, sw2, sb + kGuessHid, sh1);
+    infer_layer<kGuessHid, kLdH>(sh0, sw2, sb + kGuessHid, sh1);
     __syncthreads();
-    infer_layer<kGuessHid>(sh1, sw3, sb + 2 * kGuessHid, sh0);
+    infer_layer<kGuessHid, kLdH>(sh1, sw3, sb + 2 * kGuessHid, sh0);
     __syncthreads();
     if (tid < kTile * kGuessOut) {
       const int a = tid >> 1, o = tid & 1;
       float s = sb[3 * kGuessHid + o];
-      for (int k = 0; k < kGuessHid; ++k) s += bf2f(sh0[a * kGuessHid + k]) * bf2f(sw4[k * kGuessOut + o]);
+      for (int k = 0; k < kGuessHid; ++k) s += bf2f(sh0[a * kLdH + k]) * bf2f(sw4[k * kGuessOut + o]);
       if (row0 + a < natoms) y[(row0 + a) * kGuessOut + o] = s;
     }
   }
