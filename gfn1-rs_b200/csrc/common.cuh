@@ -36,6 +36,10 @@ constexpr int kTerms = 15;     // EnergyTerms::named_values (src/electronic.rs:6
 // its register budget is sized for.
 constexpr int kGradThreads = 128;
 constexpr int kGradMinBlocks = 4;
+// The s/p instantiation of the gradient kernel runs five CTAs per SM (96
+// registers; measured on the 4096-molecule batch: 3 CTAs 7.70 ms, 4: 7.00 ms,
+// 5: 6.63 ms, the spills staying in L1)
+constexpr int kGradMinBlocksSp = 5;
 
 // Per-element data, indexed by Z.  nsh == 0 marks an element the device path
 // does not support (f shells, more than three shells).  Values are already converted to the model

@@ -57,7 +57,7 @@ __device__ __forceinline__ void grad_shell_pair(const ElemTable& eb, int kb, con
 // the highest shell angular momentum of the batch; the s/p instantiation
 // (MaxL = 1) leaves out the d-shell blocks and their registers.
 template <int MaxL>
-__global__ void __launch_bounds__(kGradThreads, kGradMinBlocks) grad_kernel(Batch B, Model M, const int* mols,
+__global__ void __launch_bounds__(kGradThreads, MaxL < 2 ? kGradMinBlocksSp : kGradMinBlocks) grad_kernel(Batch B, Model M, const int* mols,
                                                                            int phases) {
   extern __shared__ double gsm[];
   const int m = mols ? mols[blockIdx.x] : blockIdx.x;
